@@ -1,0 +1,173 @@
+/*
+ * mpmw.h -- C ABI of libmpmw.so, the B200 (sm_100a) MPM-XPBD substep library.
+ *
+ * Plain C: raw device pointers, sizes and POD structs; no C++ or torch types
+ * cross this boundary, no C++ exception escapes it.  Every entry point returns
+ * an int status (MPMW_OK or an MPMW_E_* code) and records a message readable
+ * with mpmw_last_error() (thread-local).  Entry points are stream-ordered: they
+ * enqueue work on `stream` and never synchronize the host, never allocate
+ * device memory, and write device-side faults (out-of-grid stencil, NaN) into
+ * the caller's device status word (`status`, may be NULL).
+ *
+ * Data layout (all float32 unless stated; "SoA" = component-major):
+ *   vec3 field  : float[3][n]      component c of particle p at ptr[c*n + p]
+ *   mat33 field : float[9][n]      entry (r,c) at ptr[(3r+c)*n + p]
+ *   stress      : float[6][n]      xx, yy, zz, xy, xz, yz (symmetric)
+ *   cov         : float[n][6]      reference layout (utils/mpmRoutines.py:779-802)
+ *   grid mv     : float[G][4]      (m, m*vx, m*vy, m*vz) P2G accumulators
+ *   grid v      : float[G][4]      (vx, vy, vz, 0) grid velocity
+ *   node (ix,iy,iz) -> (ix*ny + iy)*nz + iz   (C order, z fastest)
+ *
+ * Reference citations are to the MPMWarpYDW project (utils/...).
+ */
+#ifndef MPMW_H
+#define MPMW_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* return codes */
+#define MPMW_OK 0
+#define MPMW_E_ARG 1        /* invalid argument (null pointer, size, enum) */
+#define MPMW_E_LAUNCH 2     /* kernel launch failed */
+#define MPMW_E_DEVICE 3     /* CUDA runtime error */
+#define MPMW_E_WORKSPACE 4  /* workspace too small */
+
+/* device status word bits (OR-ed by kernels into *status) */
+#define MPMW_ST_OOB 1u      /* a stencil node fell outside the grid; access skipped */
+#define MPMW_ST_NAN 2u      /* a non-finite particle position was produced */
+#define MPMW_ST_TIMEOUT 4u  /* a bounded wait gave up */
+
+/* boundary condition codes (utils/simulationRoutines.py:124-228) */
+#define MPMW_BC_NONE -1
+#define MPMW_BC_FRICTION 0
+#define MPMW_BC_FRICTION_GRADUAL 1
+#define MPMW_BC_RESTITUTION 2
+#define MPMW_BC_ABSORBING 3
+#define MPMW_BC_PLANE_STRAIN_Y 4
+#define MPMW_BC_PLANE_STRAIN_Y_GLOBAL 5
+
+typedef void *mpmw_stream_t; /* a cudaStream_t; NULL = legacy default stream */
+
+/* Per-particle arrays (utils/simStates.py:10-179 SimState/MPMState/XPBDState). */
+typedef struct mpmw_particles {
+    int64_t n;
+    float *x, *v;                /* [3][n] particle_x, particle_v */
+    float *C, *F, *F_trial;      /* [9][n] particle_C, particle_F, particle_F_trial */
+    float *stress;               /* [6][n] particle_stress (symmetric) */
+    float *cov;                  /* [n][6] particle_cov, may be NULL if update_cov == 0 */
+    float *vol, *mass, *density, *radius;
+    float *mu, *lam, *ys, *alpha, *hardening, *softening, *strain_criteria;
+    float *eta_shear, *eta_bulk;
+    float *acc_strain, *damage;  /* particle_accumulated_strain, particle_damage */
+    int32_t *active, *material;  /* activeLabel, materialLabel */
+    float *x_pc, *v_pc;          /* [3][n] particle_x/v_initial_xpbd (phase-change records) */
+} mpmw_particles_t;
+
+/* One background grid. */
+typedef struct mpmw_grid {
+    int32_t dims[3];
+    float *mv;                   /* [G][4] grid_m + grid_v_in */
+    float *v;                    /* [G][4] grid_v_out */
+    float *cell_div, *cell_vol;  /* [G] cell_div_v_weighted, cell_vol_sum (VLC only) */
+} mpmw_grid_t;
+
+/* Scalars of one MPM scene (SimState/MPMState scalars + getArgs flags). */
+typedef struct mpmw_params {
+    float min_bounds[3];
+    float dx, inv_dx, dt;
+    float gravity[3];            /* already scaled by any gravity pulse */
+    float rpic_damping;
+    float grid_v_damping_scale;  /* applied only when < 1 */
+    float bound_friction, bound_restitution;
+    int32_t boundary_condition;  /* MPMW_BC_* */
+    int32_t boundary_padding;
+    float eff;                   /* phase-change energy efficiency */
+    int32_t update_cov;
+    int32_t vlc;                 /* volumetric_locking_correction */
+    int32_t constitutive_model;  /* accepted and ignored, as in the reference */
+} mpmw_params_t;
+
+/* ---- library ------------------------------------------------------------ */
+const char *mpmw_last_error(void);
+int mpmw_version(void);
+
+/* ---- set-up kernels ------------------------------------------------------ */
+/* utils/mpmRoutines.py:206-226 compute_mu_lam_bulk_from_E_nu */
+int mpmw_mu_lam_bulk(int64_t n, const float *E, const float *nu, float *mu, float *lam, float *bulk,
+                     mpmw_stream_t stream);
+/* utils/mpmRoutines.py:51-124 initialize_geostatic_F (planestrain != 0:
+ * :127-203 initialize_geostatic_F_planestrain); F is [9][n] SoA */
+int mpmw_geostatic_F(int64_t n, const float *x, float *F, const float *mu, const float *lam,
+                     const float *density, float gravity, float z_top, float K0, int planestrain,
+                     mpmw_stream_t stream);
+
+/* ---- MPM substep kernels ------------------------------------------------- */
+/* utils/mpmRoutines.py:229-312 compute_stress_from_F_trial (+ :314-453 return map,
+ * :456-471 Kirchhoff stress) */
+int mpmw_stress(const mpmw_particles_t *p, const mpmw_params_t *prm, uint32_t *status, mpmw_stream_t stream);
+/* utils/mpmRoutines.py:485-569 p2g_apic_with_stress (accumulates into grid->mv;
+ * the caller zeroes it first, utils/simulationRoutines.py:11-13) */
+int mpmw_p2g(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
+             mpmw_stream_t stream);
+/* utils/mpmRoutines.py:690-711 grid_normalization_and_gravity + add_damping_via_grid,
+ * fused with the boundary kernel selected at utils/simulationRoutines.py:124-228
+ * (mpmRoutines.py:914-1362).  Writes every node of grid->v. */
+int mpmw_grid_update(const mpmw_grid_t *g, const mpmw_params_t *prm, mpmw_stream_t stream);
+/* One reference grid kernel on its own, with its exact write set:
+ *   op 0  utils/mpmRoutines.py:690-704 grid_normalization_and_gravity (nodes with
+ *         m <= 1e-15 are left untouched)
+ *   op 1  utils/mpmRoutines.py:706-711 add_damping_via_grid (scale by
+ *         prm->grid_v_damping_scale, unconditionally)
+ *   op 2  the boundary kernel prm->boundary_condition (mpmRoutines.py:914-1362) */
+int mpmw_grid_op(const mpmw_grid_t *g, const mpmw_params_t *prm, int op, mpmw_stream_t stream);
+/* utils/mpmRoutines.py:715-802 g2p (+ update_cov) */
+int mpmw_g2p(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
+             mpmw_stream_t stream);
+/* g2p followed, per particle and in registers, by the next substep's
+ * compute_stress_from_F_trial (including Kelvin-Voigt from the new C).  Writes
+ * F (returned) and stress instead of F_trial.  Equivalent to mpmw_g2p followed
+ * by mpmw_stress when nothing runs between them (no VLC, no XPBD). */
+int mpmw_g2p_stress(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm,
+                    uint32_t *status, mpmw_stream_t stream);
+/* utils/mpmRoutines.py:817-911 accumulate_cell_divergence + apply_volumetric_locking_correction
+ * (zeroes grid->cell_div / cell_vol itself, utils/simulationRoutines.py:255-293) */
+int mpmw_vlc(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
+             mpmw_stream_t stream);
+/* One phase of the correction on its own: phase 0 = accumulate_cell_divergence
+ * (mpmRoutines.py:817-856, adds into grid->cell_div / cell_vol, no zeroing),
+ * phase 1 = apply_volumetric_locking_correction (mpmRoutines.py:859-911).
+ * Only grid->dims, cell_div and cell_vol are used. */
+int mpmw_vlc_phase(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, int phase,
+                   uint32_t *status, mpmw_stream_t stream);
+/* utils/simulationRoutines.py:6-293 mpmSimulationStep: zero grid, stress, P2G,
+ * grid update, G2P, optional VLC -- one reference substep */
+int mpmw_substep(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
+                 mpmw_stream_t stream);
+/* nsteps consecutive mpmSimulationStep calls with no XPBD between them
+ * (runMPMYDW.py:666-682 for steps where counter % mpmStepsPerXpbdStep != 0).
+ * Same result as nsteps x mpmw_substep; internally the return map of step k+1
+ * runs fused into the G2P of step k when VLC is off. */
+int mpmw_run_substeps(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, int nsteps,
+                      uint32_t *status, mpmw_stream_t stream);
+
+/* utils/mpmRoutines.py:1446-1475 deactivate_and_teleport_xpbd_below_datum */
+int mpmw_teleport(const mpmw_particles_t *p, float z_datum, float teleport_distance, mpmw_stream_t stream);
+/* utils/mpmRoutines.py:3-21 creep_by_damage_with_baseline */
+int mpmw_creep(const mpmw_particles_t *p, const float *ys_base, float dt, float base_creep, float damage_creep,
+               float damage_exponent, mpmw_stream_t stream);
+
+/* ---- per-step statistics (utils/simulationRoutines.py:538-675) ----------- */
+/* out (device, 7 doubles, overwritten): sum |v|/radius over active (velocityConvergence),
+ * active count (countActiveParticles), sum damage over active (compute_mean_gpu numerator),
+ * active MPM, active XPBD, inactive MPM, inactive XPBD (countParticlesByType). */
+int mpmw_stats(const mpmw_particles_t *p, double *out, mpmw_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPMW_H */

@@ -1,0 +1,126 @@
+"""ctypes binding of libmpmw.so (declarations in include/mpmw.h).
+
+The CUDA library is the only compute path: if it is missing or cannot be
+loaded, :func:`lib` raises.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from .build import LIB, build
+
+_P = ctypes.c_void_p
+_F = ctypes.c_float
+_I = ctypes.c_int
+_I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
+
+MPMW_OK = 0
+ST_OOB, ST_NAN, ST_TIMEOUT = 1, 2, 4
+BC_CODES = {
+    "none": -1,
+    "friction": 0,
+    "friction_gradual": 1,
+    "restitution": 2,
+    "absorbing": 3,
+    "plane_strain_y": 4,
+    "plane_strain_y_global": 5,
+}
+
+
+class Particles(ctypes.Structure):
+    _fields_ = [("n", _I64),
+                ("x", _P), ("v", _P),
+                ("C", _P), ("F", _P), ("F_trial", _P),
+                ("stress", _P), ("cov", _P),
+                ("vol", _P), ("mass", _P), ("density", _P), ("radius", _P),
+                ("mu", _P), ("lam", _P), ("ys", _P), ("alpha", _P), ("hardening", _P), ("softening", _P),
+                ("strain_criteria", _P), ("eta_shear", _P), ("eta_bulk", _P),
+                ("acc_strain", _P), ("damage", _P),
+                ("active", _P), ("material", _P),
+                ("x_pc", _P), ("v_pc", _P)]
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("dims", _I32 * 3), ("mv", _P), ("v", _P), ("cell_div", _P), ("cell_vol", _P)]
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("min_bounds", _F * 3), ("dx", _F), ("inv_dx", _F), ("dt", _F), ("gravity", _F * 3),
+                ("rpic_damping", _F), ("grid_v_damping_scale", _F), ("bound_friction", _F),
+                ("bound_restitution", _F), ("boundary_condition", _I32), ("boundary_padding", _I32),
+                ("eff", _F), ("update_cov", _I32), ("vlc", _I32), ("constitutive_model", _I32)]
+
+
+_SIGS = {
+    "mpmw_last_error": (ctypes.c_char_p, []),
+    "mpmw_version": (_I, []),
+    "mpmw_mu_lam_bulk": (_I, [_I64, _P, _P, _P, _P, _P, _P]),
+    "mpmw_geostatic_F": (_I, [_I64, _P, _P, _P, _P, _P, _F, _F, _F, _I, _P]),
+    "mpmw_stress": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Params), _P, _P]),
+    "mpmw_p2g": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _P, _P]),
+    "mpmw_grid_update": (_I, [ctypes.POINTER(Grid), ctypes.POINTER(Params), _P]),
+    "mpmw_grid_op": (_I, [ctypes.POINTER(Grid), ctypes.POINTER(Params), _I, _P]),
+    "mpmw_g2p": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _P, _P]),
+    "mpmw_g2p_stress": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _P, _P]),
+    "mpmw_vlc": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _P, _P]),
+    "mpmw_vlc_phase": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _I, _P, _P]),
+    "mpmw_substep": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _P, _P]),
+    "mpmw_run_substeps": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _I, _P,
+                               _P]),
+    "mpmw_teleport": (_I, [ctypes.POINTER(Particles), _F, _F, _P]),
+    "mpmw_creep": (_I, [ctypes.POINTER(Particles), _P, _F, _F, _F, _F, _P]),
+    "mpmw_stats": (_I, [ctypes.POINTER(Particles), _P, _P]),
+}
+
+_LIB = None
+
+
+def lib(rebuild: bool = True):
+    """Load (building first if stale) libmpmw.so; raises if it cannot be loaded."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = LIB
+    if rebuild:
+        try:
+            path = build()
+        except Exception:
+            if not os.path.exists(LIB):
+                raise
+    if not os.path.exists(path):
+        raise RuntimeError(f"libmpmw.so not found at {path}; run python -m mpmwarpydw_b200.build")
+    h = ctypes.CDLL(path)
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(h, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = h
+    return h
+
+
+class MPMWError(RuntimeError):
+    pass
+
+
+def check(rc: int, what: str = ""):
+    if rc != MPMW_OK:
+        msg = lib().mpmw_last_error().decode(errors="replace")
+        raise MPMWError(f"{what}: libmpmw error {rc}: {msg}")
+
+
+def exported_symbols(header: str | None = None):
+    """Names of every function declared in include/*.h (for symbol checks)."""
+    import glob
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    names = []
+    files = [header] if header else sorted(glob.glob(os.path.join(root, "include", "*.h")))
+    for f in files:
+        src = open(f).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names += re.findall(r"\b(mpmw_[a-z0-9_]+)\s*\(", src)
+    return sorted(set(names))

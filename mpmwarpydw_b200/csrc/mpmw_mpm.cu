@@ -1,0 +1,984 @@
+// mpmw_mpm.cu -- MPM substep kernels and their C-ABI entry points.
+//
+// Kernel map (reference = MPMWarpYDW utils/...):
+//   k_stress       mpmRoutines.py:229-312 (+ return map :314-453, Kirchhoff :456-471)
+//   k_p2g          mpmRoutines.py:485-569, CTA-tiled in shared memory
+//   k_grid_update  mpmRoutines.py:690-711 + boundary kernels :914-1362, one pass
+//   k_g2p<F>       mpmRoutines.py:715-802; F=true fuses the next step's stress
+//   k_vlc_*        mpmRoutines.py:817-911
+#include <cstdarg>
+#include <cstring>
+
+#include "mpmw_common.cuh"
+#include "mpmw_math.cuh"
+
+namespace mpmw {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+int check_launch(const char *what)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("%s: %s", what, cudaGetErrorString(e));
+        return MPMW_E_LAUNCH;
+    }
+    return MPMW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// stress: Drucker-Prager return map + Kirchhoff + Kelvin-Voigt for one particle
+// ---------------------------------------------------------------------------
+// Ft: trial deformation gradient; Cg: velocity gradient C used for the
+// viscous term; xr/vr: particle position/velocity in registers when HaveXV,
+// otherwise read from (and the velocity written back to) global memory on a
+// phase transition.  Outputs F (returned deformation gradient) and the full
+// symmetric stress (row-major 3x3).  Side effects follow the reference.
+template <bool HaveXV>
+__device__ __forceinline__ void stress_particle(const mpmw_particles_t &P, float eff, int64_t p,
+                                                const float *Ft, const float *Cg, const float *xr, float *vr,
+                                                float *Fout, float *out)
+{
+    const int64_t n = P.n;
+    float U[9], V[9], so[3];
+    svd3(Ft, U, so, V);
+    float sg0 = rmax(so[0], 0.01f), sg1 = rmax(so[1], 0.01f), sg2 = rmax(so[2], 0.01f);
+    float e[3] = {logf(sg0), logf(sg1), logf(sg2)};
+    float tr = (e[0] + e[1]) + e[2];
+    float mean_eps = tr / 3.f;
+    float ed[3] = {e[0] - mean_eps, e[1] - mean_eps, e[2] - mean_eps};
+    float mu = P.mu[p], lam = P.lam[p], ys = P.ys[p], alpha = P.alpha[p], D = P.damage[p];
+    float twomu = 2.f * mu;
+    float ltr = lam * tr;
+    float tau[3] = {twomu * e[0] + ltr, twomu * e[1] + ltr, twomu * e[2] + ltr};
+    float pst = ((tau[0] + tau[1]) + tau[2]) / 3.f;
+    float td[3] = {tau[0] - pst, tau[1] - pst, tau[2] - pst};
+    float sigma_eq = len3(td);
+    float yield_eff = (1.f - D) * (ys - alpha * pst);
+    bool reuse_svd = true;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Fout[k] = Ft[k];
+    if (sigma_eq > yield_eff || ys < 0.f || yield_eff < 0.f) {
+        float edn = len3(ed) + 1e-6f;
+        float dgamma = edn - yield_eff / (2.f * mu);
+        float dacc = sqrtf(2.f / 3.f) * dgamma;
+        P.acc_strain[p] = P.acc_strain[p] + dacc;
+        float sc = P.strain_criteria[p];
+        if (sc > 0.f) D = rmin(1.f, D + dacc / sc);
+        else D = 1.f;
+        if (ys < 0.f || yield_eff < 0.f) D = 1.f;
+        P.damage[p] = D;
+        if (D >= 1.f && P.material[p] == 1) {
+            // phase transition to an XPBD particle (mpmRoutines.py:379-408)
+            P.material[p] = 2;
+            float xx[3], vv[3];
+            if (HaveXV) { xx[0] = xr[0]; xx[1] = xr[1]; xx[2] = xr[2]; vv[0] = vr[0]; vv[1] = vr[1]; vv[2] = vr[2]; }
+            else { load3(P.x, n, p, xx); load3(P.v, n, p, vv); }
+            store3(P.x_pc, n, p, xx);
+            float rho = P.density[p];
+            float u = 0.5f * ((tau[0] * e[0] + tau[1] * e[1]) + tau[2] * e[2]);
+            float vexp = sqrtf(((2.f * eff) * u) / rho);
+            float vb[3] = {vv[0] + 1e-12f, vv[1] + 1e-12f, vv[2] + 1e-12f};
+            float vd[3];
+            normalize3(vb, vd);
+            vv[0] = vv[0] + vexp * vd[0]; vv[1] = vv[1] + vexp * vd[1]; vv[2] = vv[2] + vexp * vd[2];
+            store3(P.v_pc, n, p, vv);
+            if (HaveXV) { vr[0] = vv[0]; vr[1] = vv[1]; vr[2] = vv[2]; }
+            else store3(P.v, n, p, vv);
+            P.ys[p] = 0.f; P.mu[p] = 0.f; P.lam[p] = 0.f; P.alpha[p] = 0.f;
+            mu = 0.f; lam = 0.f;
+        } else {
+            float f = dgamma / edn;
+            float beta = 0.3f * alpha;
+            float vc = beta * dgamma;
+            float en[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) en[k] = (e[k] - f * ed[k]) + vc;
+            float dsy = ((2.f * mu) * (P.hardening[p] - P.softening[p])) * dgamma;
+            ys = rmax(0.f, ys + dsy);
+            P.ys[p] = ys;
+            float ex0 = expf(en[0]), ex1 = expf(en[1]), ex2 = expf(en[2]);
+            float UD[9];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) { UD[3 * r + 0] = U[3 * r + 0] * ex0; UD[3 * r + 1] = U[3 * r + 1] * ex1; UD[3 * r + 2] = U[3 * r + 2] * ex2; }
+            matmul3_bt(UD, V, Fout);
+            reuse_svd = false;
+        }
+    }
+    // Kirchhoff stress from the returned F (second svd3 at mpmRoutines.py:288;
+    // identical to the first when F was returned unchanged)
+    float T[9];
+    if (reuse_svd) {
+        kirchhoff(Fout, U, V, so, mu, lam, T);
+    } else {
+        float U2[9], V2[9], s2[3];
+        svd3(Fout, U2, s2, V2);
+        kirchhoff(Fout, U2, V2, s2, mu, lam, T);
+    }
+    // symmetrise, add Kelvin-Voigt (mpmRoutines.py:292-310)
+    float sr[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sr[3 * r + c] = 0.5f * (Cg[3 * r + c] + Cg[3 * c + r]);
+    float vrate = (sr[0] + sr[4]) + sr[8];
+    float vr3 = vrate / 3.f;
+    float te = 2.f * P.eta_shear[p];
+    float bv = P.eta_bulk[p] * vrate;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float sym = (T[3 * r + c] + T[3 * c + r]) / 2.f;
+            float dev = sr[3 * r + c] - (r == c ? vr3 : 0.f);
+            float visc = te * dev + (r == c ? bv : 0.f);
+            out[3 * r + c] = sym + visc;
+        }
+}
+
+__global__ void __launch_bounds__(kBlock) k_stress(mpmw_particles_t P, float eff)
+{
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.n) return;
+    if (!(P.material[p] <= 1)) return;
+    if (P.active[p] != 1) return;
+    float Ft[9], Cg[9], Fo[9], out[9];
+    load9(P.F_trial, P.n, p, Ft);
+    load9(P.C, P.n, p, Cg);
+    stress_particle<false>(P, eff, p, Ft, Cg, nullptr, nullptr, Fo, out);
+    store9(P.F, P.n, p, Fo);
+    store_sym6(P.stress, P.n, p, out);
+}
+
+// ---------------------------------------------------------------------------
+// P2G: one CTA per chunk of kBlock consecutive particles.  The chunk's stencil
+// bounding box is accumulated in a shared-memory tile (float4 m, mv), then
+// flushed to global memory with one vector atomic per touched node.  Chunks
+// whose bounding box exceeds the tile scatter straight to global memory, so
+// any particle order is correct; spatially sorted particles are fast.
+// ---------------------------------------------------------------------------
+constexpr int kTileMax = 2048;  // nodes (32 KB of float4)
+
+struct P2GConsts {
+    float Cp[9];   // rpic-blended affine matrix
+    float Sm[9];   // -vol * stress
+    float v[3];
+    float m;
+};
+
+template <typename Emit>
+__device__ __forceinline__ void p2g_scatter(const Weights &W, const P2GConsts &K, float dx, float inv_dx, float dt,
+                                            Emit &&emit)
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                float dpos[3] = {((float)i - W.fx[0]) * dx, ((float)j - W.fx[1]) * dx, ((float)k - W.fx[2]) * dx};
+                float weight = (W.w[0][i] * W.w[1][j]) * W.w[2][k];
+                float dwt[3] = {((W.dw[0][i] * W.w[1][j]) * W.w[2][k]) * inv_dx,
+                                ((W.w[0][i] * W.dw[1][j]) * W.w[2][k]) * inv_dx,
+                                ((W.w[0][i] * W.w[1][j]) * W.dw[2][k]) * inv_dx};
+                float ef0 = (K.Sm[0] * dwt[0] + K.Sm[1] * dwt[1]) + K.Sm[2] * dwt[2];
+                float ef1 = (K.Sm[3] * dwt[0] + K.Sm[4] * dwt[1]) + K.Sm[5] * dwt[2];
+                float ef2 = (K.Sm[6] * dwt[0] + K.Sm[7] * dwt[1]) + K.Sm[8] * dwt[2];
+                float cd0 = (K.Cp[0] * dpos[0] + K.Cp[1] * dpos[1]) + K.Cp[2] * dpos[2];
+                float cd1 = (K.Cp[3] * dpos[0] + K.Cp[4] * dpos[1]) + K.Cp[5] * dpos[2];
+                float cd2 = (K.Cp[6] * dpos[0] + K.Cp[7] * dpos[1]) + K.Cp[8] * dpos[2];
+                float wm = weight * K.m;
+                float4 add;
+                add.x = wm;
+                add.y = wm * (K.v[0] + cd0) + dt * ef0;
+                add.z = wm * (K.v[1] + cd1) + dt * ef1;
+                add.w = wm * (K.v[2] + cd2) + dt * ef2;
+                emit(W.base[0] + i, W.base[1] + j, W.base[2] + k, add);
+            }
+}
+
+__global__ void __launch_bounds__(kBlock) k_p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
+                                               uint32_t *status)
+{
+    __shared__ float4 tile[kTileMax];
+    __shared__ int s_lo[3], s_hi[3];
+    const int64_t n = P.n;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nx = G.dims[0], ny = G.dims[1], nz = G.dims[2];
+    float4 *__restrict__ gmv = reinterpret_cast<float4 *>(G.mv);
+
+    if (threadIdx.x < 3) { s_lo[threadIdx.x] = INT32_MAX; s_hi[threadIdx.x] = INT32_MIN; }
+    bool act = false;
+    Weights W;
+    P2GConsts K;
+    if (p < n) act = (P.active[p] == 1 && P.material[p] <= 1);
+    if (act) {
+        float xp[3];
+        load3(P.x, n, p, xp);
+        weights(xp, prm.min_bounds, prm.inv_dx, W);
+        float C0[9], st[9];
+        load9(P.C, n, p, C0);
+        load_sym6(P.stress, n, p, st);
+        const float r = prm.rpic_damping;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b)
+                K.Cp[3 * a + b] = (1.f - r) * C0[3 * a + b] + (r / 2.f) * (C0[3 * a + b] - C0[3 * b + a]);
+        if (r < -0.001f) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) K.Cp[k] = 0.f;
+        }
+        float nv = -P.vol[p];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) K.Sm[k] = nv * st[k];
+        load3(P.v, n, p, K.v);
+        K.m = P.mass[p];
+    }
+    __syncthreads();
+    // chunk bounding box of stencil bases (warp-reduce, then shared atomics)
+    {
+        int lo0 = act ? W.base[0] : INT32_MAX, lo1 = act ? W.base[1] : INT32_MAX, lo2 = act ? W.base[2] : INT32_MAX;
+        int hi0 = act ? W.base[0] : INT32_MIN, hi1 = act ? W.base[1] : INT32_MIN, hi2 = act ? W.base[2] : INT32_MIN;
+        lo0 = __reduce_min_sync(0xffffffffu, lo0); lo1 = __reduce_min_sync(0xffffffffu, lo1); lo2 = __reduce_min_sync(0xffffffffu, lo2);
+        hi0 = __reduce_max_sync(0xffffffffu, hi0); hi1 = __reduce_max_sync(0xffffffffu, hi1); hi2 = __reduce_max_sync(0xffffffffu, hi2);
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&s_lo[0], lo0); atomicMin(&s_lo[1], lo1); atomicMin(&s_lo[2], lo2);
+            atomicMax(&s_hi[0], hi0); atomicMax(&s_hi[1], hi1); atomicMax(&s_hi[2], hi2);
+        }
+    }
+    __syncthreads();
+    if (s_lo[0] == INT32_MAX) return;  // no active MPM particle in this chunk (uniform)
+    const int ox = s_lo[0], oy = s_lo[1], oz = s_lo[2];
+    const int64_t ex = (int64_t)s_hi[0] - ox + 3, ey = (int64_t)s_hi[1] - oy + 3, ez = (int64_t)s_hi[2] - oz + 3;
+    const int64_t tvol = ex * ey * ez;
+    const float dx = prm.dx, inv_dx = prm.inv_dx, dt = prm.dt;
+
+    if (tvol <= kTileMax) {
+        const int tv = (int)tvol, eyi = (int)ey, ezi = (int)ez;
+        for (int t = threadIdx.x; t < tv; t += blockDim.x) tile[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncthreads();
+        if (act) {
+            p2g_scatter(W, K, dx, inv_dx, dt, [&](int ix, int iy, int iz, float4 a) {
+                int t = ((ix - ox) * eyi + (iy - oy)) * ezi + (iz - oz);
+                atomicAdd(&tile[t].x, a.x);
+                atomicAdd(&tile[t].y, a.y);
+                atomicAdd(&tile[t].z, a.z);
+                atomicAdd(&tile[t].w, a.w);
+            });
+        }
+        __syncthreads();
+        uint32_t bad = 0;
+        for (int t = threadIdx.x; t < tv; t += blockDim.x) {
+            float4 a = tile[t];
+            if (a.x == 0.f && a.y == 0.f && a.z == 0.f && a.w == 0.f) continue;
+            int lz = t % ezi, rest = t / ezi;
+            int ly = rest % eyi, lx = rest / eyi;
+            int ix = ox + lx, iy = oy + ly, iz = oz + lz;
+            if (ix < 0 || iy < 0 || iz < 0 || ix >= nx || iy >= ny || iz >= nz) { bad = MPMW_ST_OOB; continue; }
+            atomicAdd(&gmv[((int64_t)ix * ny + iy) * nz + iz], a);
+        }
+        if (bad) raise_status(status, bad);
+    } else if (act) {
+        uint32_t bad = 0;
+        p2g_scatter(W, K, dx, inv_dx, dt, [&](int ix, int iy, int iz, float4 a) {
+            if (ix < 0 || iy < 0 || iz < 0 || ix >= nx || iy >= ny || iz >= nz) { bad = MPMW_ST_OOB; return; }
+            atomicAdd(&gmv[((int64_t)ix * ny + iy) * nz + iz], a);
+        });
+        if (bad) raise_status(status, bad);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// grid update: normalisation + gravity + damping + boundary condition
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float coulomb(float v, float mu, float dt, float g)
+{
+    if (fabsf(v) < 1e-12f) return 0.f;
+    float dvf = (mu * g) * dt;
+    float s = v < 0.f ? -1.f : 1.f;
+    return s * rmax(fabsf(v) - dvf, 0.f);
+}
+
+__device__ __forceinline__ void apply_bc(int bc, const int *idx, const int *dim, float *o, float mu, float rest,
+                                         float dt, float g, int pad)
+{
+    float v[3] = {o[0], o[1], o[2]};
+    if (bc == MPMW_BC_FRICTION || bc == MPMW_BC_RESTITUTION) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int t0 = (a + 1) % 3, t1 = (a + 2) % 3;
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                bool hit = side == 0 ? (idx[a] <= pad && v[a] < 0.f) : (idx[a] >= dim[a] - pad && v[a] > 0.f);
+                if (!hit) continue;
+                float w[3];
+                w[a] = bc == MPMW_BC_FRICTION ? 0.f : -rest * v[a];
+                w[t0] = coulomb(v[t0], mu, dt, g);
+                w[t1] = coulomb(v[t1], mu, dt, g);
+                o[0] = w[0]; o[1] = w[1]; o[2] = w[2];
+            }
+        }
+    } else if (bc == MPMW_BC_FRICTION_GRADUAL) {
+        const float padf = (float)pad;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int t0 = (a + 1) % 3, t1 = (a + 2) % 3;
+            float fade = 0.f;
+            bool hit = false;
+            if (idx[a] < pad && v[a] < 0.f) { fade = (float)idx[a] / padf; hit = true; }
+            else if (idx[a] >= dim[a] - pad && v[a] > 0.f) { fade = (float)(dim[a] - 1 - idx[a]) / padf; hit = true; }
+            if (!hit) continue;
+            float fm = mu * (1.f - fade);
+            float w[3];
+            w[t0] = coulomb(v[t0], fm, dt, g);
+            w[t1] = coulomb(v[t1], fm, dt, g);
+            w[a] = 0.f * (1.f - fade) + v[a] * fade;
+            o[0] = w[0]; o[1] = w[1]; o[2] = w[2];
+        }
+    } else if (bc == MPMW_BC_ABSORBING) {
+        const float padf = (float)pad;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                bool hit = side == 0 ? (idx[a] < 3) : (idx[a] >= dim[a] - 3);
+                if (!hit) continue;
+                float lf = side == 0 ? (padf - (float)idx[a]) / padf : (padf - (float)(dim[a] - 1 - idx[a])) / padf;
+                float damp = 0.f * lf + 1.f * (1.f - lf);
+                o[0] = v[0] * damp; o[1] = v[1] * damp; o[2] = v[2] * damp;
+            }
+        }
+    } else if (bc == MPMW_BC_PLANE_STRAIN_Y) {
+        const int ix = idx[0], iy = idx[1], iz = idx[2];
+        if (ix <= pad && v[0] < 0.f) { o[0] = 0.f; o[1] = coulomb(v[1], mu, dt, g); o[2] = coulomb(v[2], mu, dt, g); }
+        if (ix >= dim[0] - pad && v[0] > 0.f) { o[0] = 0.f; o[1] = coulomb(v[1], mu, dt, g); o[2] = coulomb(v[2], mu, dt, g); }
+        if (iy <= pad) { v[0] = o[0]; v[1] = o[1]; v[2] = o[2]; o[0] = v[0]; o[1] = 0.f; o[2] = v[2]; }
+        if (iy >= dim[1] - pad) { v[0] = o[0]; v[1] = o[1]; v[2] = o[2]; o[0] = v[0]; o[1] = 0.f; o[2] = v[2]; }
+        if (iz <= pad && v[2] < 0.f) { float a0 = coulomb(v[0], mu, dt, g), a1 = coulomb(v[1], mu, dt, g); o[0] = a0; o[1] = a1; o[2] = 0.f; }
+        if (iz >= dim[2] - pad && v[2] > 0.f) { float a0 = coulomb(v[0], mu, dt, g), a1 = coulomb(v[1], mu, dt, g); o[0] = a0; o[1] = a1; o[2] = 0.f; }
+    } else if (bc == MPMW_BC_PLANE_STRAIN_Y_GLOBAL) {
+        const int ix = idx[0], iz = idx[2];
+        o[1] = 0.f;
+        v[0] = o[0]; v[1] = o[1]; v[2] = o[2];
+        if (ix <= pad && v[0] < 0.f) { o[0] = 0.f; o[1] = 0.f; o[2] = coulomb(v[2], mu, dt, g); }
+        if (ix >= dim[0] - pad && v[0] > 0.f) { o[0] = 0.f; o[1] = 0.f; o[2] = coulomb(v[2], mu, dt, g); }
+        if (iz <= pad && v[2] < 0.f) { o[0] = coulomb(v[0], mu, dt, g); o[1] = 0.f; o[2] = 0.f; }
+        if (iz >= dim[2] - pad && v[2] > 0.f) { o[0] = coulomb(v[0], mu, dt, g); o[1] = 0.f; o[2] = 0.f; }
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_grid_update(mpmw_grid_t G, mpmw_params_t prm)
+{
+    const int nx = G.dims[0], ny = G.dims[1], nz = G.dims[2];
+    const int64_t total = (int64_t)nx * ny * nz;
+    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const float4 a = reinterpret_cast<const float4 *>(G.mv)[g];
+    float o[3] = {0.f, 0.f, 0.f};
+    if (a.x > 1e-15f) {
+        float inv = 1.f / a.x;
+        o[0] = a.y * inv + prm.dt * prm.gravity[0];
+        o[1] = a.z * inv + prm.dt * prm.gravity[1];
+        o[2] = a.w * inv + prm.dt * prm.gravity[2];
+    }
+    if (prm.grid_v_damping_scale < 1.f) {
+        o[0] = o[0] * prm.grid_v_damping_scale;
+        o[1] = o[1] * prm.grid_v_damping_scale;
+        o[2] = o[2] * prm.grid_v_damping_scale;
+    }
+    if (prm.boundary_condition >= 0) {
+        int iz = (int)(g % nz);
+        int64_t r = g / nz;
+        int iy = (int)(r % ny), ix = (int)(r / ny);
+        int idx[3] = {ix, iy, iz}, dim[3] = {nx, ny, nz};
+        float gm = fabsf(prm.gravity[2]);
+        apply_bc(prm.boundary_condition, idx, dim, o, prm.bound_friction, prm.bound_restitution, prm.dt, gm,
+                 prm.boundary_padding);
+    }
+    reinterpret_cast<float4 *>(G.v)[g] = make_float4(o[0], o[1], o[2], 0.f);
+}
+
+// single grid operations with the reference kernels' exact write sets:
+//   op 0: grid_normalization_and_gravity (writes only nodes with m > 1e-15)
+//   op 1: add_damping_via_grid (unconditional scale)
+//   op 2: the boundary kernel prm.boundary_condition on grid v
+__global__ void __launch_bounds__(kBlock) k_grid_op(mpmw_grid_t G, mpmw_params_t prm, int op)
+{
+    const int nx = G.dims[0], ny = G.dims[1], nz = G.dims[2];
+    const int64_t total = (int64_t)nx * ny * nz;
+    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    float4 *v4 = reinterpret_cast<float4 *>(G.v);
+    if (op == 0) {
+        const float4 a = reinterpret_cast<const float4 *>(G.mv)[g];
+        if (a.x > 1e-15f) {
+            float inv = 1.f / a.x;
+            v4[g] = make_float4(a.y * inv + prm.dt * prm.gravity[0], a.z * inv + prm.dt * prm.gravity[1],
+                                a.w * inv + prm.dt * prm.gravity[2], 0.f);
+        }
+    } else if (op == 1) {
+        float4 t = v4[g];
+        float s = prm.grid_v_damping_scale;
+        v4[g] = make_float4(t.x * s, t.y * s, t.z * s, t.w);
+    } else {
+        float4 t = v4[g];
+        float o[3] = {t.x, t.y, t.z};
+        int iz = (int)(g % nz);
+        int64_t r = g / nz;
+        int iy = (int)(r % ny), ix = (int)(r / ny);
+        int idx[3] = {ix, iy, iz}, dim[3] = {nx, ny, nz};
+        apply_bc(prm.boundary_condition, idx, dim, o, prm.bound_friction, prm.bound_restitution, prm.dt,
+                 fabsf(prm.gravity[2]), prm.boundary_padding);
+        v4[g] = make_float4(o[0], o[1], o[2], t.w);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// G2P (+ cov), optionally fused with the next substep's stress update
+// ---------------------------------------------------------------------------
+template <bool Fused>
+__global__ void __launch_bounds__(kBlock) k_g2p(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
+                                               uint32_t *status)
+{
+    const int64_t n = P.n;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    if (P.active[p] != 1) return;
+    if (!(P.material[p] <= 1)) return;
+    const int nx = G.dims[0], ny = G.dims[1], nz = G.dims[2];
+    const float4 *__restrict__ gv = reinterpret_cast<const float4 *>(G.v);
+    float xp[3];
+    load3(P.x, n, p, xp);
+    Weights W;
+    weights(xp, prm.min_bounds, prm.inv_dx, W);
+    const float inv_dx = prm.inv_dx, dt = prm.dt;
+    float nv[3] = {0.f, 0.f, 0.f}, nC[9], nF[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { nC[k] = 0.f; nF[k] = 0.f; }
+    uint32_t bad = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                float dpos[3] = {(float)i - W.fx[0], (float)j - W.fx[1], (float)k - W.fx[2]};
+                float weight = (W.w[0][i] * W.w[1][j]) * W.w[2][k];
+                int ix = W.base[0] + i, iy = W.base[1] + j, iz = W.base[2] + k;
+                float g3[3] = {0.f, 0.f, 0.f};
+                if (ix < 0 || iy < 0 || iz < 0 || ix >= nx || iy >= ny || iz >= nz) bad = MPMW_ST_OOB;
+                else {
+                    float4 t = __ldg(&gv[((int64_t)ix * ny + iy) * nz + iz]);
+                    g3[0] = t.x; g3[1] = t.y; g3[2] = t.z;
+                }
+#pragma unroll
+                for (int a = 0; a < 3; ++a) nv[a] = nv[a] + g3[a] * weight;
+                float sc = (weight * inv_dx) * 4.f;
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) nC[3 * r + c] = nC[3 * r + c] + (g3[r] * dpos[c]) * sc;
+                float dwt[3] = {((W.dw[0][i] * W.w[1][j]) * W.w[2][k]) * inv_dx,
+                                ((W.w[0][i] * W.dw[1][j]) * W.w[2][k]) * inv_dx,
+                                ((W.w[0][i] * W.w[1][j]) * W.dw[2][k]) * inv_dx};
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) nF[3 * r + c] = nF[3 * r + c] + g3[r] * dwt[c];
+            }
+    float xn[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) xn[a] = xp[a] + dt * nv[a];
+    if (!(isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]))) bad |= MPMW_ST_NAN;
+    float F[9], A[9], Ft[9];
+    load9(P.F, n, p, F);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) A[3 * r + c] = (r == c ? 1.f : 0.f) + nF[3 * r + c] * dt;
+    matmul3(A, F, Ft);
+    if (prm.update_cov && P.cov) {
+        float *cv = P.cov + 6 * p;
+        float cn[9] = {cv[0], cv[1], cv[2], cv[1], cv[3], cv[4], cv[2], cv[4], cv[5]};
+        float a1[9], a2[9];
+        matmul3(nF, cn, a1);
+        matmul3_bt(cn, nF, a2);
+        float c1[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) c1[k] = cn[k] + dt * (a1[k] + a2[k]);
+        cv[0] = c1[0]; cv[1] = c1[1]; cv[2] = c1[2]; cv[3] = c1[4]; cv[4] = c1[5]; cv[5] = c1[8];
+    }
+    store3(P.x, n, p, xn);
+    store9(P.C, n, p, nC);
+    if (Fused) {
+        float Fo[9], out[9];
+        stress_particle<true>(P, prm.eff, p, Ft, nC, xn, nv, Fo, out);
+        store9(P.F, n, p, Fo);
+        store_sym6(P.stress, n, p, out);
+    } else {
+        store9(P.F_trial, n, p, Ft);
+    }
+    store3(P.v, n, p, nv);
+    if (bad) raise_status(status, bad);
+}
+
+// ---------------------------------------------------------------------------
+// volumetric locking correction
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool vlc_cell(const float *xp, const mpmw_params_t &prm, const int *dims, int64_t &cell)
+{
+    int c0 = (int)((xp[0] - prm.min_bounds[0]) * prm.inv_dx);
+    int c1 = (int)((xp[1] - prm.min_bounds[1]) * prm.inv_dx);
+    int c2 = (int)((xp[2] - prm.min_bounds[2]) * prm.inv_dx);
+    if (c0 < 0 || c1 < 0 || c2 < 0 || c0 >= dims[0] || c1 >= dims[1] || c2 >= dims[2]) return false;
+    cell = ((int64_t)c0 * dims[1] + c1) * dims[2] + c2;
+    return true;
+}
+
+__global__ void __launch_bounds__(kBlock) k_vlc_acc(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
+                                                   uint32_t *status)
+{
+    const int64_t n = P.n;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    if (!(P.active[p] == 1 && P.material[p] <= 1)) return;
+    float xp[3];
+    load3(P.x, n, p, xp);
+    int64_t cell;
+    if (!vlc_cell(xp, prm, G.dims, cell)) { raise_status(status, MPMW_ST_OOB); return; }
+    float div = (P.C[p] + P.C[4 * n + p]) + P.C[8 * n + p];
+    float vp = P.vol[p];
+    atomicAdd(&G.cell_div[cell], div * vp);
+    atomicAdd(&G.cell_vol[cell], vp);
+}
+
+__global__ void __launch_bounds__(kBlock) k_vlc_apply(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
+                                                     uint32_t *status)
+{
+    const int64_t n = P.n;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    if (!(P.active[p] == 1 && P.material[p] <= 1)) return;
+    float xp[3];
+    load3(P.x, n, p, xp);
+    int64_t cell;
+    float vs = 0.f, cd = 0.f;
+    if (!vlc_cell(xp, prm, G.dims, cell)) raise_status(status, MPMW_ST_OOB);
+    else { vs = G.cell_vol[cell]; cd = G.cell_div[cell]; }
+    float dvc = vs > 1e-20f ? cd / vs : 0.f;
+    float c00 = P.C[p], c11 = P.C[4 * n + p], c22 = P.C[8 * n + p];
+    float dvp = (c00 + c11) + c22;
+    float corr = (dvc - dvp) / 3.f;
+    P.C[p] = c00 + corr;
+    P.C[4 * n + p] = c11 + corr;
+    P.C[8 * n + p] = c22 + corr;
+}
+
+// ---------------------------------------------------------------------------
+// set-up and per-bigStep kernels
+// ---------------------------------------------------------------------------
+__global__ void k_mu_lam_bulk(int64_t n, const float *E, const float *nu, float *mu, float *lam, float *bulk)
+{
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    float e = E[p], v = nu[p];
+    float m = e / (2.f * (1.f + v));
+    float l = (e * v) / ((1.f + v) * (1.f - 2.f * v));
+    mu[p] = m; lam[p] = l;
+    bulk[p] = l + (2.f / 3.f) * m;
+}
+
+__global__ void k_geostatic_F(int64_t n, const float *x, float *F, const float *mu, const float *lam,
+                              const float *density, float gravity, float z_top, float K0, int planestrain)
+{
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    float depth = z_top - x[2 * n + p];
+    float e0, e1, e2;
+    if (!planestrain) {
+        float sigma_v = (-density[p] * gravity) * depth;
+        float sigma_h = K0 * sigma_v;
+        float lv = lam[p], mv = mu[p];
+        float a11 = 2.f * lv + 2.f * mv, a12 = lv, a21 = 2.f * lv, a22 = lv + 2.f * mv;
+        float det = a11 * a22 - a12 * a21;
+        float eh = 0.f, ev = 0.f;
+        if (fabsf(det) > 1e-12f) {
+            eh = (sigma_h * a22 - sigma_v * a12) / det;
+            ev = (a11 * sigma_v - a21 * sigma_h) / det;
+        }
+        e0 = eh; e1 = eh; e2 = ev;
+    } else {
+        e0 = e1 = e2 = 0.f;
+        if (depth > 0.f) {
+            float mv = mu[p], lv = lam[p];
+            float nu = lv / (2.f * (lv + mv));
+            float E = (mv * (3.f * lv + 2.f * mv)) / (lv + mv);
+            float sv = (-density[p] * gravity) * depth;
+            float sh = K0 * sv;
+            float syy = nu * (sh + sv);
+            e0 = (sh - nu * (syy + sv)) / E;
+            e1 = 0.f;
+            e2 = (sv - nu * (sh + syy)) / E;
+        }
+    }
+    float f[9] = {expf(e0), 0.f, 0.f, 0.f, expf(e1), 0.f, 0.f, 0.f, expf(e2)};
+    store9(F, n, p, f);
+}
+
+__global__ void k_teleport(mpmw_particles_t P, float z_datum, float dist)
+{
+    const int64_t n = P.n;
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    if (P.active[p] == 1 && P.material[p] == 2 && P.x[2 * n + p] < z_datum) {
+        P.active[p] = 0;
+        P.x[2 * n + p] = P.x[2 * n + p] - dist;
+        P.v[p] = 0.f; P.v[n + p] = 0.f; P.v[2 * n + p] = 0.f;
+    }
+}
+
+__global__ void k_creep(mpmw_particles_t P, const float *ys_base, float dt, float base_creep, float damage_creep,
+                        float damage_exponent)
+{
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.n) return;
+    if (P.material[p] > 1) return;
+    float rate = base_creep + damage_creep * powf(P.damage[p], damage_exponent);
+    float decay = (rate * ys_base[p]) * dt;
+    P.ys[p] = rmax(0.f, P.ys[p] - decay);
+}
+
+// per-step statistics: block reduce in double, one atomic per block per field
+__global__ void __launch_bounds__(kBlock) k_stats(mpmw_particles_t P, double *out)
+{
+    const int64_t n = P.n;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        bool act = P.active[p] == 1, xp = P.material[p] == 2;
+        if (act) {
+            float v3[3];
+            load3(P.v, n, p, v3);
+            acc[0] += (double)(len3(v3) / P.radius[p]);
+            acc[1] += 1.0;
+            acc[2] += (double)P.damage[p];
+        }
+        if (xp) { if (act) acc[4] += 1.0; else acc[6] += 1.0; }
+        else { if (act) acc[3] += 1.0; else acc[5] += 1.0; }
+    }
+    __shared__ double red[7][kBlock / 32];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        double v = acc[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 7) {
+        double s = 0;
+        for (int w = 0; w < kBlock / 32; ++w) s += red[threadIdx.x][w];
+        atomicAdd(&out[threadIdx.x], s);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// argument checks
+// ---------------------------------------------------------------------------
+// field groups an entry point needs
+enum : unsigned { kNeedLabels = 1, kNeedXV = 2, kNeedCF = 4, kNeedStress = 8 };
+
+static int check_particles(const mpmw_particles_t *p, unsigned need)
+{
+    if (!p) { set_error("particles is NULL"); return MPMW_E_ARG; }
+    if (p->n < 0) { set_error("negative particle count"); return MPMW_E_ARG; }
+    if (p->n == 0) return MPMW_OK;
+    if ((need & kNeedLabels) && (!p->active || !p->material)) {
+        set_error("particles: active and material labels are required");
+        return MPMW_E_ARG;
+    }
+    if ((need & kNeedXV) && (!p->x || !p->v)) { set_error("particles: x and v are required"); return MPMW_E_ARG; }
+    if ((need & kNeedCF) && (!p->C || !p->F)) { set_error("particles: C and F are required"); return MPMW_E_ARG; }
+    if ((need & kNeedStress) &&
+        (!p->F_trial || !p->stress || !p->mu || !p->lam || !p->ys || !p->alpha || !p->hardening || !p->softening ||
+         !p->strain_criteria || !p->eta_shear || !p->eta_bulk || !p->acc_strain || !p->damage || !p->density ||
+         !p->x_pc || !p->v_pc)) {
+        set_error("particles: a stress/material field is NULL");
+        return MPMW_E_ARG;
+    }
+    return MPMW_OK;
+}
+
+static int check_grid(const mpmw_grid_t *g)
+{
+    if (!g) { set_error("grid is NULL"); return MPMW_E_ARG; }
+    if (g->dims[0] <= 0 || g->dims[1] <= 0 || g->dims[2] <= 0) { set_error("grid dims must be positive"); return MPMW_E_ARG; }
+    if ((int64_t)g->dims[0] * g->dims[1] * g->dims[2] > (int64_t)INT32_MAX) { set_error("grid too large"); return MPMW_E_ARG; }
+    if (!g->mv || !g->v) { set_error("grid mv and v are required"); return MPMW_E_ARG; }
+    if ((reinterpret_cast<uintptr_t>(g->mv) | reinterpret_cast<uintptr_t>(g->v)) & 15u) {
+        set_error("grid mv and v must be 16-byte aligned");
+        return MPMW_E_ARG;
+    }
+    return MPMW_OK;
+}
+
+static int check_params(const mpmw_params_t *prm)
+{
+    if (!prm) { set_error("params is NULL"); return MPMW_E_ARG; }
+    if (prm->boundary_condition < -1 || prm->boundary_condition > MPMW_BC_PLANE_STRAIN_Y_GLOBAL) {
+        set_error("unknown boundary_condition %d", prm->boundary_condition);
+        return MPMW_E_ARG;
+    }
+    return MPMW_OK;
+}
+
+#define MPMW_TRY(expr)            \
+    do {                          \
+        int _rc = (expr);         \
+        if (_rc != MPMW_OK) return _rc; \
+    } while (0)
+
+// host-side launchers (also used by the multi-step driver)
+int launch_stress(const mpmw_particles_t &p, const mpmw_params_t &prm, cudaStream_t s)
+{
+    if (p.n == 0) return MPMW_OK;
+    k_stress<<<grid_for(p.n), kBlock, 0, s>>>(p, prm.eff);
+    return check_launch("k_stress");
+}
+int launch_p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, cudaStream_t s)
+{
+    if (p.n == 0) return MPMW_OK;
+    k_p2g<<<grid_for(p.n), kBlock, 0, s>>>(p, g, prm, st);
+    return check_launch("k_p2g");
+}
+int launch_grid(const mpmw_grid_t &g, const mpmw_params_t &prm, cudaStream_t s)
+{
+    int64_t G = (int64_t)g.dims[0] * g.dims[1] * g.dims[2];
+    k_grid_update<<<grid_for(G), kBlock, 0, s>>>(g, prm);
+    return check_launch("k_grid_update");
+}
+int launch_g2p(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, bool fused,
+               cudaStream_t s)
+{
+    if (p.n == 0) return MPMW_OK;
+    if (fused) k_g2p<true><<<grid_for(p.n), kBlock, 0, s>>>(p, g, prm, st);
+    else k_g2p<false><<<grid_for(p.n), kBlock, 0, s>>>(p, g, prm, st);
+    return check_launch(fused ? "k_g2p<fused>" : "k_g2p");
+}
+int launch_vlc(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, cudaStream_t s)
+{
+    if (!g.cell_div || !g.cell_vol) { set_error("vlc requires grid cell_div and cell_vol"); return MPMW_E_ARG; }
+    size_t G = (size_t)g.dims[0] * g.dims[1] * g.dims[2];
+    if (cudaMemsetAsync(g.cell_div, 0, G * sizeof(float), s) != cudaSuccess ||
+        cudaMemsetAsync(g.cell_vol, 0, G * sizeof(float), s) != cudaSuccess) {
+        set_error("vlc: memset failed");
+        return MPMW_E_DEVICE;
+    }
+    if (p.n == 0) return MPMW_OK;
+    k_vlc_acc<<<grid_for(p.n), kBlock, 0, s>>>(p, g, prm, st);
+    MPMW_TRY(check_launch("k_vlc_acc"));
+    k_vlc_apply<<<grid_for(p.n), kBlock, 0, s>>>(p, g, prm, st);
+    return check_launch("k_vlc_apply");
+}
+int zero_grid(const mpmw_grid_t &g, cudaStream_t s)
+{
+    size_t G = (size_t)g.dims[0] * g.dims[1] * g.dims[2];
+    if (cudaMemsetAsync(g.mv, 0, G * 4 * sizeof(float), s) != cudaSuccess) {
+        set_error("grid memset failed");
+        return MPMW_E_DEVICE;
+    }
+    return MPMW_OK;
+}
+
+}  // namespace mpmw
+
+using namespace mpmw;
+
+extern "C" {
+
+const char *mpmw_last_error(void) { return mpmw::g_err; }
+int mpmw_version(void) { return 1; }
+
+int mpmw_mu_lam_bulk(int64_t n, const float *E, const float *nu, float *mu, float *lam, float *bulk,
+                     mpmw_stream_t stream)
+{
+    if (n < 0 || (n > 0 && (!E || !nu || !mu || !lam || !bulk))) { set_error("mu_lam_bulk: bad arguments"); return MPMW_E_ARG; }
+    if (n == 0) return MPMW_OK;
+    k_mu_lam_bulk<<<grid_for(n), kBlock, 0, as_stream(stream)>>>(n, E, nu, mu, lam, bulk);
+    return check_launch("k_mu_lam_bulk");
+}
+
+int mpmw_geostatic_F(int64_t n, const float *x, float *F, const float *mu, const float *lam, const float *density,
+                     float gravity, float z_top, float K0, int planestrain, mpmw_stream_t stream)
+{
+    if (n < 0 || (n > 0 && (!x || !F || !mu || !lam || !density))) { set_error("geostatic_F: bad arguments"); return MPMW_E_ARG; }
+    if (n == 0) return MPMW_OK;
+    k_geostatic_F<<<grid_for(n), kBlock, 0, as_stream(stream)>>>(n, x, F, mu, lam, density, gravity, z_top, K0, planestrain);
+    return check_launch("k_geostatic_F");
+}
+
+int mpmw_stress(const mpmw_particles_t *p, const mpmw_params_t *prm, uint32_t *status, mpmw_stream_t stream)
+{
+    (void)status;
+    MPMW_TRY(check_particles(p, kNeedLabels | kNeedCF | kNeedStress));
+    MPMW_TRY(check_params(prm));
+    return launch_stress(*p, *prm, as_stream(stream));
+}
+
+int mpmw_p2g(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
+             mpmw_stream_t stream)
+{
+    MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV | kNeedCF));
+    MPMW_TRY(check_grid(g));
+    MPMW_TRY(check_params(prm));
+    if (p->n > 0 && (!p->stress || !p->vol || !p->mass)) { set_error("p2g: stress, vol and mass are required"); return MPMW_E_ARG; }
+    return launch_p2g(*p, *g, *prm, status, as_stream(stream));
+}
+
+int mpmw_grid_update(const mpmw_grid_t *g, const mpmw_params_t *prm, mpmw_stream_t stream)
+{
+    MPMW_TRY(check_grid(g));
+    MPMW_TRY(check_params(prm));
+    return launch_grid(*g, *prm, as_stream(stream));
+}
+
+int mpmw_grid_op(const mpmw_grid_t *g, const mpmw_params_t *prm, int op, mpmw_stream_t stream)
+{
+    MPMW_TRY(check_grid(g));
+    MPMW_TRY(check_params(prm));
+    if (op < 0 || op > 2) { set_error("grid_op: unknown op %d", op); return MPMW_E_ARG; }
+    if (op == 2 && prm->boundary_condition < 0) return MPMW_OK;
+    int64_t G = (int64_t)g->dims[0] * g->dims[1] * g->dims[2];
+    k_grid_op<<<grid_for(G), kBlock, 0, as_stream(stream)>>>(*g, *prm, op);
+    return check_launch("k_grid_op");
+}
+
+int mpmw_g2p(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
+             mpmw_stream_t stream)
+{
+    MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV | kNeedCF));
+    MPMW_TRY(check_grid(g));
+    MPMW_TRY(check_params(prm));
+    if (p->n > 0 && !p->F_trial) { set_error("g2p: F_trial is required"); return MPMW_E_ARG; }
+    if (prm->update_cov && p->n > 0 && !p->cov) { set_error("g2p: update_cov needs cov"); return MPMW_E_ARG; }
+    return launch_g2p(*p, *g, *prm, status, false, as_stream(stream));
+}
+
+int mpmw_g2p_stress(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
+                    mpmw_stream_t stream)
+{
+    MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV | kNeedCF | kNeedStress));
+    MPMW_TRY(check_grid(g));
+    MPMW_TRY(check_params(prm));
+    if (prm->update_cov && p->n > 0 && !p->cov) { set_error("g2p: update_cov needs cov"); return MPMW_E_ARG; }
+    return launch_g2p(*p, *g, *prm, status, true, as_stream(stream));
+}
+
+int mpmw_vlc(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
+             mpmw_stream_t stream)
+{
+    MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV | kNeedCF));
+    MPMW_TRY(check_grid(g));
+    MPMW_TRY(check_params(prm));
+    if (p->n > 0 && !p->vol) { set_error("vlc: vol is required"); return MPMW_E_ARG; }
+    return launch_vlc(*p, *g, *prm, status, as_stream(stream));
+}
+
+int mpmw_vlc_phase(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, int phase,
+                   uint32_t *status, mpmw_stream_t stream)
+{
+    MPMW_TRY(check_particles(p, kNeedLabels));
+    MPMW_TRY(check_params(prm));
+    if (!g || g->dims[0] <= 0 || g->dims[1] <= 0 || g->dims[2] <= 0 || !g->cell_div || !g->cell_vol) {
+        set_error("vlc_phase: grid dims and cell_div/cell_vol are required");
+        return MPMW_E_ARG;
+    }
+    if (phase != 0 && phase != 1) { set_error("vlc_phase: phase must be 0 or 1"); return MPMW_E_ARG; }
+    if (p->n == 0) return MPMW_OK;
+    if (!p->x || !p->C || (phase == 0 && !p->vol)) { set_error("vlc_phase: x, C (and vol) are required"); return MPMW_E_ARG; }
+    cudaStream_t s = as_stream(stream);
+    if (phase == 0) k_vlc_acc<<<grid_for(p->n), kBlock, 0, s>>>(*p, *g, *prm, status);
+    else k_vlc_apply<<<grid_for(p->n), kBlock, 0, s>>>(*p, *g, *prm, status);
+    return check_launch(phase == 0 ? "k_vlc_acc" : "k_vlc_apply");
+}
+
+int mpmw_substep(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
+                 mpmw_stream_t stream)
+{
+    return mpmw_run_substeps(p, g, prm, 1, status, stream);
+}
+
+int mpmw_run_substeps(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, int nsteps,
+                      uint32_t *status, mpmw_stream_t stream)
+{
+    MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV | kNeedCF | kNeedStress));
+    MPMW_TRY(check_grid(g));
+    MPMW_TRY(check_params(prm));
+    if (nsteps < 0) { set_error("nsteps must be >= 0"); return MPMW_E_ARG; }
+    if (p->n > 0 && (!p->vol || !p->mass)) { set_error("substep: vol and mass are required"); return MPMW_E_ARG; }
+    if (prm->update_cov && p->n > 0 && !p->cov) { set_error("substep: update_cov needs cov"); return MPMW_E_ARG; }
+    if (prm->vlc && (!g->cell_div || !g->cell_vol)) { set_error("substep: vlc needs cell_div/cell_vol"); return MPMW_E_ARG; }
+    cudaStream_t s = as_stream(stream);
+    bool need_stress = true;
+    for (int step = 0; step < nsteps; ++step) {
+        if (need_stress) MPMW_TRY(launch_stress(*p, *prm, s));
+        MPMW_TRY(zero_grid(*g, s));
+        MPMW_TRY(launch_p2g(*p, *g, *prm, status, s));
+        MPMW_TRY(launch_grid(*g, *prm, s));
+        bool last = step == nsteps - 1;
+        if (!last && !prm->vlc) {
+            MPMW_TRY(launch_g2p(*p, *g, *prm, status, true, s));
+            need_stress = false;
+        } else {
+            MPMW_TRY(launch_g2p(*p, *g, *prm, status, false, s));
+            if (prm->vlc) MPMW_TRY(launch_vlc(*p, *g, *prm, status, s));
+            need_stress = true;
+        }
+    }
+    return MPMW_OK;
+}
+
+int mpmw_teleport(const mpmw_particles_t *p, float z_datum, float teleport_distance, mpmw_stream_t stream)
+{
+    MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV));
+    if (p->n == 0) return MPMW_OK;
+    k_teleport<<<grid_for(p->n), kBlock, 0, as_stream(stream)>>>(*p, z_datum, teleport_distance);
+    return check_launch("k_teleport");
+}
+
+int mpmw_creep(const mpmw_particles_t *p, const float *ys_base, float dt, float base_creep, float damage_creep,
+               float damage_exponent, mpmw_stream_t stream)
+{
+    if (!p || p->n < 0 || (p->n > 0 && (!p->material || !p->damage || !p->ys || !ys_base))) {
+        set_error("creep: bad arguments");
+        return MPMW_E_ARG;
+    }
+    if (p->n == 0) return MPMW_OK;
+    k_creep<<<grid_for(p->n), kBlock, 0, as_stream(stream)>>>(*p, ys_base, dt, base_creep, damage_creep, damage_exponent);
+    return check_launch("k_creep");
+}
+
+int mpmw_stats(const mpmw_particles_t *p, double *out, mpmw_stream_t stream)
+{
+    if (!p || p->n < 0 || !out) { set_error("stats: bad arguments"); return MPMW_E_ARG; }
+    if (p->n > 0 && (!p->active || !p->material || !p->v || !p->radius || !p->damage)) {
+        set_error("stats: active, material, v, radius and damage are required");
+        return MPMW_E_ARG;
+    }
+    cudaStream_t s = as_stream(stream);
+    if (cudaMemsetAsync(out, 0, 7 * sizeof(double), s) != cudaSuccess) { set_error("stats: memset failed"); return MPMW_E_DEVICE; }
+    if (p->n == 0) return MPMW_OK;
+    int64_t blocks = (p->n + kBlock - 1) / kBlock;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k_stats<<<(unsigned)blocks, kBlock, 0, s>>>(*p, out);
+    return check_launch("k_stats");
+}
+
+}  // extern "C"

@@ -1,0 +1,106 @@
+"""Multi-step execution: spatial particle ordering and CUDA-graph replay.
+
+``sort_particles`` reorders every per-particle array of the three state
+objects into 4x4x4-cell block order (a one-time set-up step; the reference's
+results do not depend on particle order).  Consecutive particles then share
+grid cells, which is what the P2G kernel's shared-memory tiles and the G2P
+kernel's cached grid reads rely on.  ``sim.particle_order`` keeps, for each
+stored particle, its index in the original input so results can be written
+back in input order (:func:`original_order`).
+
+``SubstepGraph`` captures ``k`` MPM substeps (one library call) into a CUDA
+graph and replays it; host work per replay is one launch.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import _lib
+from .bind import grid_from_state, params_from_states, particles_from_states, status_word, stream_handle
+from .state import Mat33Field, ScalarField, Sym33Field, Vec3Field
+
+
+def block_sort_key(x_n3: torch.Tensor, minBounds, inv_dx: float, dims, block: int = 4) -> torch.Tensor:
+    """int64 key: (block index in C order) * block^3 + (cell index inside the block)."""
+    mb = torch.as_tensor(minBounds, dtype=torch.float32, device=x_n3.device)
+    cell = torch.floor((x_n3 - mb) * inv_dx).to(torch.int64)
+    d = torch.as_tensor(dims, dtype=torch.int64, device=x_n3.device)
+    cell = torch.minimum(torch.clamp(cell, min=0), d - 1)
+    nb = (d + block - 1) // block
+    b = cell // block
+    r = cell % block
+    bidx = (b[:, 0] * nb[1] + b[:, 1]) * nb[2] + b[:, 2]
+    ridx = (r[:, 0] * block + r[:, 1]) * block + r[:, 2]
+    return bidx * (block ** 3) + ridx
+
+
+def _permute_state(obj, perm: torch.Tensor, n: int):
+    for cls in type(obj).__mro__:
+        for name, desc in list(vars(cls).items()):
+            if not isinstance(desc, (ScalarField, Vec3Field, Mat33Field, Sym33Field)):
+                continue
+            s = desc.storage(obj)
+            if s is None:
+                continue
+            if isinstance(desc, ScalarField):
+                if s.numel() == n:
+                    s.copy_(s[perm])
+                elif s.numel() % n == 0:
+                    k = s.numel() // n
+                    v = s.view(n, k)
+                    v.copy_(v[perm])
+            else:
+                s.copy_(s[:, perm])
+
+
+def sort_particles(sim, mpm, xpbd=None, block: int = 4):
+    """Reorder all per-particle state into block order (returns the permutation)."""
+    n = sim.nPoints
+    key = block_sort_key(sim.particle_x, sim.minBounds, sim.invdx, mpm.gridDims, block)
+    perm = torch.argsort(key, stable=True)
+    for obj in (sim, mpm, xpbd):
+        if obj is not None:
+            _permute_state(obj, perm, n)
+    prev = getattr(sim, "particle_order", None)
+    sim.particle_order = perm if prev is None else prev[perm]
+    return perm
+
+
+def original_order(sim, t: torch.Tensor) -> torch.Tensor:
+    """Return a per-particle tensor (first dim N) in the original input order."""
+    order = getattr(sim, "particle_order", None)
+    if order is None:
+        return t
+    out = torch.empty_like(t)
+    out[order] = t
+    return out
+
+
+class SubstepGraph:
+    """CUDA graph of ``k`` consecutive MPM substeps on fixed state buffers."""
+
+    def __init__(self, sim, mpm, xpbd, k: int, warmup: bool = True):
+        """With ``warmup`` the k substeps run once eagerly before capture (so
+        every kernel is loaded); that run advances the simulation."""
+        self.k = int(k)
+        self.P = particles_from_states(sim, mpm, xpbd)
+        self.G = grid_from_state(mpm)
+        self.prm = params_from_states(sim, mpm)
+        self.status = status_word(sim.device)
+        self.graph = torch.cuda.CUDAGraph()
+        self.stream = torch.cuda.Stream(device=sim.device)
+        self.stream.wait_stream(torch.cuda.current_stream())
+        if warmup:
+            with torch.cuda.stream(self.stream):
+                self._call()
+        torch.cuda.current_stream().wait_stream(self.stream)
+        torch.cuda.synchronize(sim.device)
+        with torch.cuda.graph(self.graph, stream=self.stream):
+            self._call()
+
+    def _call(self):
+        _lib.check(_lib.lib().mpmw_run_substeps(self.P, self.G, self.prm, self.k, self.status.data_ptr(),
+                                                 stream_handle()), "run_substeps")
+
+    def replay(self):
+        self.graph.replay()
