@@ -90,7 +90,21 @@ typedef struct mpmw_params {
     int32_t update_cov;
     int32_t vlc;                 /* volumetric_locking_correction */
     int32_t constitutive_model;  /* accepted and ignored, as in the reference */
+    int32_t stress_mode;         /* MPMW_STRESS_* */
 } mpmw_params_t;
+
+/* stress_mode: how the return map's trial state is decomposed.
+ *   MPMW_STRESS_AUTO (0): particles that are clearly elastic (|F F^T - I|_F <= 0.02
+ *     and sigma_eq below the yield surface by a 1 % + 16-ulp margin) take the
+ *     log strain from ln(I + X), X = G + G^T + G G^T, G = F - I (4-term series);
+ *     this equals the reference's U diag(2 mu ln s + lam sum ln s) U^T Kirchhoff
+ *     stress and is more accurate in FP32 than an SVD of F near identity.  All
+ *     other particles take the SVD path below.
+ *   MPMW_STRESS_SVD (1): every particle takes the SVD path (svd3 of F_trial,
+ *     principal log strains, radial return, second svd3 for the Kirchhoff
+ *     stress), operation for operation as the CPU oracle. */
+#define MPMW_STRESS_AUTO 0
+#define MPMW_STRESS_SVD 1
 
 /* ---- library ------------------------------------------------------------ */
 const char *mpmw_last_error(void);

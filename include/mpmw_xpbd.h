@@ -1,0 +1,89 @@
+/*
+ * mpmw_xpbd.h -- C ABI of the XPBD part of libmpmw.so (spatial hash, contact
+ * Jacobi passes, sleeping, MPM contact impulses, swelling).  Conventions as in
+ * mpmw.h: device pointers, SoA float[3][n] vec3 fields, int status returns,
+ * stream-ordered, no allocation (the hash build takes a caller workspace).
+ *
+ * Reference citations are to the MPMWarpYDW project (utils/...).
+ */
+#ifndef MPMW_XPBD_H
+#define MPMW_XPBD_H
+
+#include "mpmw.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* XPBDState temporaries and per-particle XPBD fields (utils/simStates.py:133-179). */
+typedef struct mpmw_xpbd {
+    float *x_int, *v_int;        /* [3][n] particle_x/v_integrated */
+    float *x_dI, *v_dI;          /* [3][n] particle_x/v_deltaInt (may be NULL) */
+    float *delta;                /* [3][n] particle_delta */
+    float *v_before;             /* [3][n] particle_v_before_contact (may be NULL) */
+    float *cum_dist;             /* [n] particle_cumDist_xpbd */
+    float *base_radius, *max_radius; /* [n] particleBaseRadius, particleMaxRadius */
+    int32_t *counts;             /* device [2]: numTotalXPBD, numSleepingXPBD (may be NULL) */
+} mpmw_xpbd_t;
+
+/* wp.HashGrid(dims) state after build(points, cell_width) (utils/simStates.py:174,
+ * utils/simulationRoutines.py:311). */
+typedef struct mpmw_hash {
+    int32_t dims[3];
+    float cell_width;
+    int32_t *point_ids;          /* [n] point index at each sorted position */
+    int32_t *cell_starts;        /* [dims product] first sorted position of each hash, 0 if empty */
+    int32_t *cell_ends;          /* [dims product] one past the last, 0 if empty */
+    int32_t *point_cells;        /* [n] hash of each point in input order (may be NULL) */
+} mpmw_hash_t;
+
+/* XPBDState scalars + SimState.gravity/dtxpbd (utils/simStates.py:133-179). */
+typedef struct mpmw_xpbd_params {
+    float gravity[3];
+    float dt;                    /* dtxpbd */
+    float v_max;                 /* particle_v_max */
+    int32_t iterations;          /* xpbd_iterations */
+    float relaxation;            /* xpbd_relaxation */
+    float coupling;              /* xpbd_mpm_coupling_strength */
+    int32_t lock;                /* mpm_contact_transition_lock */
+    float dyn_friction;          /* dynamicParticleFriction (k_mu / mu) */
+    float static_friction;       /* staticParticleFriction */
+    float static_thr;            /* staticVelocityThreshold */
+    float cohesion;              /* particle_cohesion (a gap length) */
+    float max_radius;            /* XPBDState.max_radius */
+    float sleep_thr;             /* sleepThreshold */
+    float bmin[3], bmax[3];      /* minBoundsXPBD, maxBoundsXPBD */
+    float swelling_ratio, swell_act, swell_max;
+    int32_t xpbd_only;
+} mpmw_xpbd_params_t;
+
+/* kernel selectors of mpmw_xpbd_kernel */
+#define MPMW_XK_INTEGRATE 0    /* xpbdRoutines.py:23-48; flag bit0: read x/v from particles (else x_int/v_int),
+                                  flag bit1: also copy non-XPBD particles (the wp.copy before it) */
+#define MPMW_XK_RESET_LABELS 1 /* xpbdRoutines.py:3-21 */
+#define MPMW_XK_BOUND 2        /* xpbdRoutines.py:49-136; flag: add into delta instead of overwriting it */
+#define MPMW_XK_PARTICLE 3     /* xpbdRoutines.py:138-219 (needs a built hash) */
+#define MPMW_XK_APPLY 4        /* xpbdRoutines.py:221-257 in place on x_int/v_int; flag: also write x_dI/v_dI */
+#define MPMW_XK_SLEEP 5        /* xpbdRoutines.py:312-334; flag: zero counts first */
+#define MPMW_XK_IMPULSES 6     /* xpbdRoutines.py:259-310 + the commit x <- x_int, v <- v_int
+                                  (simulationRoutines.py:444-470) */
+#define MPMW_XK_SWELL 7        /* xpbdRoutines.py:354-375 */
+
+/* Workspace bytes needed by mpmw_hash_build for n points. */
+size_t mpmw_hash_workspace_bytes(int64_t n);
+/* wp.HashGrid.build (simulationRoutines.py:311): x is [3][n] SoA. */
+int mpmw_hash_build(const float *x, int64_t n, const mpmw_hash_t *h, void *workspace, size_t ws_bytes,
+                    mpmw_stream_t stream);
+/* One XPBD kernel (MPMW_XK_*). */
+int mpmw_xpbd_kernel(int which, const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_hash_t *h,
+                     const mpmw_xpbd_params_t *q, int flag, mpmw_stream_t stream);
+/* utils/simulationRoutines.py:295-526 xpbdSimulationStep (hash build, integrate,
+ * label reset, iterations x (bound, particle contacts, apply), sleep,
+ * impulses + commit, swelling). */
+int mpmw_xpbd_step(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_hash_t *h,
+                   const mpmw_xpbd_params_t *q, void *workspace, size_t ws_bytes, mpmw_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPMW_XPBD_H */

@@ -50,7 +50,11 @@ class Params(ctypes.Structure):
     _fields_ = [("min_bounds", _F * 3), ("dx", _F), ("inv_dx", _F), ("dt", _F), ("gravity", _F * 3),
                 ("rpic_damping", _F), ("grid_v_damping_scale", _F), ("bound_friction", _F),
                 ("bound_restitution", _F), ("boundary_condition", _I32), ("boundary_padding", _I32),
-                ("eff", _F), ("update_cov", _I32), ("vlc", _I32), ("constitutive_model", _I32)]
+                ("eff", _F), ("update_cov", _I32), ("vlc", _I32), ("constitutive_model", _I32),
+                ("stress_mode", _I32)]
+
+
+STRESS_AUTO, STRESS_SVD = 0, 1
 
 
 _SIGS = {

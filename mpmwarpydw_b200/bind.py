@@ -203,7 +203,8 @@ def grid_from_state(mpm) -> _lib.Grid:
 
 def params_struct(*, minBounds=(0, 0, 0), dx=1.0, inv_dx=None, dt=0.0, gravity=(0, 0, 0), rpic_damping=0.0,
                   grid_v_damping_scale=1.1, bound_friction=0.0, bound_restitution=0.0, boundary_condition=-1,
-                  boundary_padding=0, eff=0.0, update_cov=0, vlc=0, constitutive_model=1) -> _lib.Params:
+                  boundary_padding=0, eff=0.0, update_cov=0, vlc=0, constitutive_model=1,
+                  stress_mode=0) -> _lib.Params:
     P = _lib.Params()
     for i in range(3):
         P.min_bounds[i] = float(minBounds[i])
@@ -222,6 +223,7 @@ def params_struct(*, minBounds=(0, 0, 0), dx=1.0, inv_dx=None, dt=0.0, gravity=(
     P.update_cov = int(bool(update_cov))
     P.vlc = int(bool(vlc))
     P.constitutive_model = int(constitutive_model)
+    P.stress_mode = int(stress_mode)
     return P
 
 
@@ -233,7 +235,8 @@ def params_from_states(sim, mpm) -> _lib.Params:
                          bound_friction=mpm.boundFriction, bound_restitution=mpm.boundRestitution,
                          boundary_condition=code, boundary_padding=mpm.boundaryPadding or 0, eff=mpm.eff,
                          update_cov=mpm.update_cov, vlc=mpm.volumetric_locking_correction,
-                         constitutive_model=mpm.constitutive_model)
+                         constitutive_model=mpm.constitutive_model,
+                         stress_mode=getattr(mpm, "stress_mode", 0))
 
 
 def byref(x):

@@ -19,6 +19,12 @@ int check_launch(const char *what);
 
 inline cudaStream_t as_stream(mpmw_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 
+#define MPMW_TRY_LAUNCH(what)                 \
+    do {                                      \
+        int _rc = ::mpmw::check_launch(what); \
+        if (_rc != MPMW_OK) return _rc;       \
+    } while (0)
+
 inline unsigned grid_for(int64_t n, int block = kBlock)
 {
     int64_t b = (n + block - 1) / block;

@@ -1,0 +1,15 @@
+// mpmw_internal.cuh -- host-side launchers shared between the library's
+// translation units (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/mpmw.h"
+
+namespace mpmw {
+
+int launch_stress(const mpmw_particles_t &p, const mpmw_params_t &prm, cudaStream_t s);
+int launch_p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, cudaStream_t s);
+int launch_g2p(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, bool fused,
+               cudaStream_t s);
+
+}  // namespace mpmw

@@ -52,35 +52,42 @@ __device__ __forceinline__ void matmul3_bt(const float *A, const float *B, float
 // 3x3 SVD: F = U diag(s) V^T, U and V proper rotations, s0 >= s1 >= |s2|,
 // sign(s2) = sign(det F).
 // ---------------------------------------------------------------------------
-constexpr int kSvdSweeps = 4;
+constexpr int kSvdMaxSweeps = 6;
 
+__device__ __forceinline__ float fma_(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+// One Jacobi rotation zeroing S[P][Q] (Golub & Van Loan sec. 8.5, with
+// t = 2 a_pq sgn(d) / (|d| + sqrt(d^2 + 4 a_pq^2)), d = a_qq - a_pp, sgn(0) = +1).
+// A pair counts as converged when a_pq^2 <= 1e-16 |a_pp a_qq|; returns whether
+// it rotated.
 template <int P, int Q>
-__device__ __forceinline__ void jacobi_rot(float *S, float *V)
+__device__ __forceinline__ bool jacobi_rot(float *S, float *V)
 {
     float apq = S[3 * P + Q];
-    if (apq == 0.f) return;
     float app = S[3 * P + P], aqq = S[3 * Q + Q];
-    float theta = (aqq - app) / (2.f * apq);
-    float t = 1.f / (fabsf(theta) + sqrtf(theta * theta + 1.f));
-    if (theta < 0.f) t = -t;
-    float c = 1.f / sqrtf(t * t + 1.f);
+    if (apq * apq <= 1e-16f * fabsf(app * aqq)) return false;
+    float d = aqq - app;
+    float two_apq = 2.f * apq;
+    float t = (d < 0.f ? -two_apq : two_apq) / (fabsf(d) + sqrtf(fma_(d, d, two_apq * two_apq)));
+    float c = 1.f / sqrtf(fma_(t, t, 1.f));
     float s = t * c;
-    S[3 * P + P] = app - t * apq;
-    S[3 * Q + Q] = aqq + t * apq;
+    S[3 * P + P] = fma_(-t, apq, app);
+    S[3 * Q + Q] = fma_(t, apq, aqq);
     S[3 * P + Q] = 0.f;
     S[3 * Q + P] = 0.f;
     constexpr int Rr = 3 - P - Q;
     float srp = S[3 * Rr + P], srq = S[3 * Rr + Q];
-    float nrp = c * srp - s * srq;
-    float nrq = s * srp + c * srq;
+    float nrp = fma_(c, srp, -s * srq);
+    float nrq = fma_(s, srp, c * srq);
     S[3 * Rr + P] = nrp; S[3 * P + Rr] = nrp;
     S[3 * Rr + Q] = nrq; S[3 * Q + Rr] = nrq;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         float vkp = V[3 * k + P], vkq = V[3 * k + Q];
-        V[3 * k + P] = c * vkp - s * vkq;
-        V[3 * k + Q] = s * vkp + c * vkq;
+        V[3 * k + P] = fma_(c, vkp, -s * vkq);
+        V[3 * k + Q] = fma_(s, vkp, c * vkq);
     }
+    return true;
 }
 
 template <int A, int B>
@@ -107,10 +114,11 @@ __device__ __forceinline__ void svd3(const float *F, float *U, float *sig, float
     for (int k = 0; k < 9; ++k) V[k] = 0.f;
     V[0] = V[4] = V[8] = 1.f;
 #pragma unroll 1
-    for (int sw = 0; sw < kSvdSweeps; ++sw) {
-        jacobi_rot<0, 1>(S, V);
-        jacobi_rot<0, 2>(S, V);
-        jacobi_rot<1, 2>(S, V);
+    for (int sw = 0; sw < kSvdMaxSweeps; ++sw) {
+        bool r0 = jacobi_rot<0, 1>(S, V);
+        bool r1 = jacobi_rot<0, 2>(S, V);
+        bool r2 = jacobi_rot<1, 2>(S, V);
+        if (!(r0 || r1 || r2)) break;
     }
     float lam[3] = {S[0], S[4], S[8]};
     sort_cols<0, 1>(lam, V);

@@ -1,15 +1,14 @@
 // mpmw_mpm.cu -- MPM substep kernels and their C-ABI entry points.
 //
 // Kernel map (reference = MPMWarpYDW utils/...):
-//   k_stress       mpmRoutines.py:229-312 (+ return map :314-453, Kirchhoff :456-471)
-//   k_p2g          mpmRoutines.py:485-569, CTA-tiled in shared memory
+//   (k_stress, k_g2p: mpmw_g2p.cu; k_p2g: mpmw_p2g.cu)
 //   k_grid_update  mpmRoutines.py:690-711 + boundary kernels :914-1362, one pass
-//   k_g2p<F>       mpmRoutines.py:715-802; F=true fuses the next step's stress
 //   k_vlc_*        mpmRoutines.py:817-911
 #include <cstdarg>
 #include <cstring>
 
 #include "mpmw_common.cuh"
+#include "mpmw_internal.cuh"
 #include "mpmw_math.cuh"
 
 namespace mpmw {
@@ -32,269 +31,6 @@ int check_launch(const char *what)
         return MPMW_E_LAUNCH;
     }
     return MPMW_OK;
-}
-
-// ---------------------------------------------------------------------------
-// stress: Drucker-Prager return map + Kirchhoff + Kelvin-Voigt for one particle
-// ---------------------------------------------------------------------------
-// Ft: trial deformation gradient; Cg: velocity gradient C used for the
-// viscous term; xr/vr: particle position/velocity in registers when HaveXV,
-// otherwise read from (and the velocity written back to) global memory on a
-// phase transition.  Outputs F (returned deformation gradient) and the full
-// symmetric stress (row-major 3x3).  Side effects follow the reference.
-template <bool HaveXV>
-__device__ __forceinline__ void stress_particle(const mpmw_particles_t &P, float eff, int64_t p,
-                                                const float *Ft, const float *Cg, const float *xr, float *vr,
-                                                float *Fout, float *out)
-{
-    const int64_t n = P.n;
-    float U[9], V[9], so[3];
-    svd3(Ft, U, so, V);
-    float sg0 = rmax(so[0], 0.01f), sg1 = rmax(so[1], 0.01f), sg2 = rmax(so[2], 0.01f);
-    float e[3] = {logf(sg0), logf(sg1), logf(sg2)};
-    float tr = (e[0] + e[1]) + e[2];
-    float mean_eps = tr / 3.f;
-    float ed[3] = {e[0] - mean_eps, e[1] - mean_eps, e[2] - mean_eps};
-    float mu = P.mu[p], lam = P.lam[p], ys = P.ys[p], alpha = P.alpha[p], D = P.damage[p];
-    float twomu = 2.f * mu;
-    float ltr = lam * tr;
-    float tau[3] = {twomu * e[0] + ltr, twomu * e[1] + ltr, twomu * e[2] + ltr};
-    float pst = ((tau[0] + tau[1]) + tau[2]) / 3.f;
-    float td[3] = {tau[0] - pst, tau[1] - pst, tau[2] - pst};
-    float sigma_eq = len3(td);
-    float yield_eff = (1.f - D) * (ys - alpha * pst);
-    bool reuse_svd = true;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) Fout[k] = Ft[k];
-    if (sigma_eq > yield_eff || ys < 0.f || yield_eff < 0.f) {
-        float edn = len3(ed) + 1e-6f;
-        float dgamma = edn - yield_eff / (2.f * mu);
-        float dacc = sqrtf(2.f / 3.f) * dgamma;
-        P.acc_strain[p] = P.acc_strain[p] + dacc;
-        float sc = P.strain_criteria[p];
-        if (sc > 0.f) D = rmin(1.f, D + dacc / sc);
-        else D = 1.f;
-        if (ys < 0.f || yield_eff < 0.f) D = 1.f;
-        P.damage[p] = D;
-        if (D >= 1.f && P.material[p] == 1) {
-            // phase transition to an XPBD particle (mpmRoutines.py:379-408)
-            P.material[p] = 2;
-            float xx[3], vv[3];
-            if (HaveXV) { xx[0] = xr[0]; xx[1] = xr[1]; xx[2] = xr[2]; vv[0] = vr[0]; vv[1] = vr[1]; vv[2] = vr[2]; }
-            else { load3(P.x, n, p, xx); load3(P.v, n, p, vv); }
-            store3(P.x_pc, n, p, xx);
-            float rho = P.density[p];
-            float u = 0.5f * ((tau[0] * e[0] + tau[1] * e[1]) + tau[2] * e[2]);
-            float vexp = sqrtf(((2.f * eff) * u) / rho);
-            float vb[3] = {vv[0] + 1e-12f, vv[1] + 1e-12f, vv[2] + 1e-12f};
-            float vd[3];
-            normalize3(vb, vd);
-            vv[0] = vv[0] + vexp * vd[0]; vv[1] = vv[1] + vexp * vd[1]; vv[2] = vv[2] + vexp * vd[2];
-            store3(P.v_pc, n, p, vv);
-            if (HaveXV) { vr[0] = vv[0]; vr[1] = vv[1]; vr[2] = vv[2]; }
-            else store3(P.v, n, p, vv);
-            P.ys[p] = 0.f; P.mu[p] = 0.f; P.lam[p] = 0.f; P.alpha[p] = 0.f;
-            mu = 0.f; lam = 0.f;
-        } else {
-            float f = dgamma / edn;
-            float beta = 0.3f * alpha;
-            float vc = beta * dgamma;
-            float en[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) en[k] = (e[k] - f * ed[k]) + vc;
-            float dsy = ((2.f * mu) * (P.hardening[p] - P.softening[p])) * dgamma;
-            ys = rmax(0.f, ys + dsy);
-            P.ys[p] = ys;
-            float ex0 = expf(en[0]), ex1 = expf(en[1]), ex2 = expf(en[2]);
-            float UD[9];
-#pragma unroll
-            for (int r = 0; r < 3; ++r) { UD[3 * r + 0] = U[3 * r + 0] * ex0; UD[3 * r + 1] = U[3 * r + 1] * ex1; UD[3 * r + 2] = U[3 * r + 2] * ex2; }
-            matmul3_bt(UD, V, Fout);
-            reuse_svd = false;
-        }
-    }
-    // Kirchhoff stress from the returned F (second svd3 at mpmRoutines.py:288;
-    // identical to the first when F was returned unchanged)
-    float T[9];
-    if (reuse_svd) {
-        kirchhoff(Fout, U, V, so, mu, lam, T);
-    } else {
-        float U2[9], V2[9], s2[3];
-        svd3(Fout, U2, s2, V2);
-        kirchhoff(Fout, U2, V2, s2, mu, lam, T);
-    }
-    // symmetrise, add Kelvin-Voigt (mpmRoutines.py:292-310)
-    float sr[9];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) sr[3 * r + c] = 0.5f * (Cg[3 * r + c] + Cg[3 * c + r]);
-    float vrate = (sr[0] + sr[4]) + sr[8];
-    float vr3 = vrate / 3.f;
-    float te = 2.f * P.eta_shear[p];
-    float bv = P.eta_bulk[p] * vrate;
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            float sym = (T[3 * r + c] + T[3 * c + r]) / 2.f;
-            float dev = sr[3 * r + c] - (r == c ? vr3 : 0.f);
-            float visc = te * dev + (r == c ? bv : 0.f);
-            out[3 * r + c] = sym + visc;
-        }
-}
-
-__global__ void __launch_bounds__(kBlock) k_stress(mpmw_particles_t P, float eff)
-{
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= P.n) return;
-    if (!(P.material[p] <= 1)) return;
-    if (P.active[p] != 1) return;
-    float Ft[9], Cg[9], Fo[9], out[9];
-    load9(P.F_trial, P.n, p, Ft);
-    load9(P.C, P.n, p, Cg);
-    stress_particle<false>(P, eff, p, Ft, Cg, nullptr, nullptr, Fo, out);
-    store9(P.F, P.n, p, Fo);
-    store_sym6(P.stress, P.n, p, out);
-}
-
-// ---------------------------------------------------------------------------
-// P2G: one CTA per chunk of kBlock consecutive particles.  The chunk's stencil
-// bounding box is accumulated in a shared-memory tile (float4 m, mv), then
-// flushed to global memory with one vector atomic per touched node.  Chunks
-// whose bounding box exceeds the tile scatter straight to global memory, so
-// any particle order is correct; spatially sorted particles are fast.
-// ---------------------------------------------------------------------------
-constexpr int kTileMax = 2048;  // nodes (32 KB of float4)
-
-struct P2GConsts {
-    float Cp[9];   // rpic-blended affine matrix
-    float Sm[9];   // -vol * stress
-    float v[3];
-    float m;
-};
-
-template <typename Emit>
-__device__ __forceinline__ void p2g_scatter(const Weights &W, const P2GConsts &K, float dx, float inv_dx, float dt,
-                                            Emit &&emit)
-{
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                float dpos[3] = {((float)i - W.fx[0]) * dx, ((float)j - W.fx[1]) * dx, ((float)k - W.fx[2]) * dx};
-                float weight = (W.w[0][i] * W.w[1][j]) * W.w[2][k];
-                float dwt[3] = {((W.dw[0][i] * W.w[1][j]) * W.w[2][k]) * inv_dx,
-                                ((W.w[0][i] * W.dw[1][j]) * W.w[2][k]) * inv_dx,
-                                ((W.w[0][i] * W.w[1][j]) * W.dw[2][k]) * inv_dx};
-                float ef0 = (K.Sm[0] * dwt[0] + K.Sm[1] * dwt[1]) + K.Sm[2] * dwt[2];
-                float ef1 = (K.Sm[3] * dwt[0] + K.Sm[4] * dwt[1]) + K.Sm[5] * dwt[2];
-                float ef2 = (K.Sm[6] * dwt[0] + K.Sm[7] * dwt[1]) + K.Sm[8] * dwt[2];
-                float cd0 = (K.Cp[0] * dpos[0] + K.Cp[1] * dpos[1]) + K.Cp[2] * dpos[2];
-                float cd1 = (K.Cp[3] * dpos[0] + K.Cp[4] * dpos[1]) + K.Cp[5] * dpos[2];
-                float cd2 = (K.Cp[6] * dpos[0] + K.Cp[7] * dpos[1]) + K.Cp[8] * dpos[2];
-                float wm = weight * K.m;
-                float4 add;
-                add.x = wm;
-                add.y = wm * (K.v[0] + cd0) + dt * ef0;
-                add.z = wm * (K.v[1] + cd1) + dt * ef1;
-                add.w = wm * (K.v[2] + cd2) + dt * ef2;
-                emit(W.base[0] + i, W.base[1] + j, W.base[2] + k, add);
-            }
-}
-
-__global__ void __launch_bounds__(kBlock) k_p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
-                                               uint32_t *status)
-{
-    __shared__ float4 tile[kTileMax];
-    __shared__ int s_lo[3], s_hi[3];
-    const int64_t n = P.n;
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int nx = G.dims[0], ny = G.dims[1], nz = G.dims[2];
-    float4 *__restrict__ gmv = reinterpret_cast<float4 *>(G.mv);
-
-    if (threadIdx.x < 3) { s_lo[threadIdx.x] = INT32_MAX; s_hi[threadIdx.x] = INT32_MIN; }
-    bool act = false;
-    Weights W;
-    P2GConsts K;
-    if (p < n) act = (P.active[p] == 1 && P.material[p] <= 1);
-    if (act) {
-        float xp[3];
-        load3(P.x, n, p, xp);
-        weights(xp, prm.min_bounds, prm.inv_dx, W);
-        float C0[9], st[9];
-        load9(P.C, n, p, C0);
-        load_sym6(P.stress, n, p, st);
-        const float r = prm.rpic_damping;
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b)
-                K.Cp[3 * a + b] = (1.f - r) * C0[3 * a + b] + (r / 2.f) * (C0[3 * a + b] - C0[3 * b + a]);
-        if (r < -0.001f) {
-#pragma unroll
-            for (int k = 0; k < 9; ++k) K.Cp[k] = 0.f;
-        }
-        float nv = -P.vol[p];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) K.Sm[k] = nv * st[k];
-        load3(P.v, n, p, K.v);
-        K.m = P.mass[p];
-    }
-    __syncthreads();
-    // chunk bounding box of stencil bases (warp-reduce, then shared atomics)
-    {
-        int lo0 = act ? W.base[0] : INT32_MAX, lo1 = act ? W.base[1] : INT32_MAX, lo2 = act ? W.base[2] : INT32_MAX;
-        int hi0 = act ? W.base[0] : INT32_MIN, hi1 = act ? W.base[1] : INT32_MIN, hi2 = act ? W.base[2] : INT32_MIN;
-        lo0 = __reduce_min_sync(0xffffffffu, lo0); lo1 = __reduce_min_sync(0xffffffffu, lo1); lo2 = __reduce_min_sync(0xffffffffu, lo2);
-        hi0 = __reduce_max_sync(0xffffffffu, hi0); hi1 = __reduce_max_sync(0xffffffffu, hi1); hi2 = __reduce_max_sync(0xffffffffu, hi2);
-        if ((threadIdx.x & 31) == 0) {
-            atomicMin(&s_lo[0], lo0); atomicMin(&s_lo[1], lo1); atomicMin(&s_lo[2], lo2);
-            atomicMax(&s_hi[0], hi0); atomicMax(&s_hi[1], hi1); atomicMax(&s_hi[2], hi2);
-        }
-    }
-    __syncthreads();
-    if (s_lo[0] == INT32_MAX) return;  // no active MPM particle in this chunk (uniform)
-    const int ox = s_lo[0], oy = s_lo[1], oz = s_lo[2];
-    const int64_t ex = (int64_t)s_hi[0] - ox + 3, ey = (int64_t)s_hi[1] - oy + 3, ez = (int64_t)s_hi[2] - oz + 3;
-    const int64_t tvol = ex * ey * ez;
-    const float dx = prm.dx, inv_dx = prm.inv_dx, dt = prm.dt;
-
-    if (tvol <= kTileMax) {
-        const int tv = (int)tvol, eyi = (int)ey, ezi = (int)ez;
-        for (int t = threadIdx.x; t < tv; t += blockDim.x) tile[t] = make_float4(0.f, 0.f, 0.f, 0.f);
-        __syncthreads();
-        if (act) {
-            p2g_scatter(W, K, dx, inv_dx, dt, [&](int ix, int iy, int iz, float4 a) {
-                int t = ((ix - ox) * eyi + (iy - oy)) * ezi + (iz - oz);
-                atomicAdd(&tile[t].x, a.x);
-                atomicAdd(&tile[t].y, a.y);
-                atomicAdd(&tile[t].z, a.z);
-                atomicAdd(&tile[t].w, a.w);
-            });
-        }
-        __syncthreads();
-        uint32_t bad = 0;
-        for (int t = threadIdx.x; t < tv; t += blockDim.x) {
-            float4 a = tile[t];
-            if (a.x == 0.f && a.y == 0.f && a.z == 0.f && a.w == 0.f) continue;
-            int lz = t % ezi, rest = t / ezi;
-            int ly = rest % eyi, lx = rest / eyi;
-            int ix = ox + lx, iy = oy + ly, iz = oz + lz;
-            if (ix < 0 || iy < 0 || iz < 0 || ix >= nx || iy >= ny || iz >= nz) { bad = MPMW_ST_OOB; continue; }
-            atomicAdd(&gmv[((int64_t)ix * ny + iy) * nz + iz], a);
-        }
-        if (bad) raise_status(status, bad);
-    } else if (act) {
-        uint32_t bad = 0;
-        p2g_scatter(W, K, dx, inv_dx, dt, [&](int ix, int iy, int iz, float4 a) {
-            if (ix < 0 || iy < 0 || iz < 0 || ix >= nx || iy >= ny || iz >= nz) { bad = MPMW_ST_OOB; return; }
-            atomicAdd(&gmv[((int64_t)ix * ny + iy) * nz + iz], a);
-        });
-        if (bad) raise_status(status, bad);
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -440,95 +176,6 @@ __global__ void __launch_bounds__(kBlock) k_grid_op(mpmw_grid_t G, mpmw_params_t
                  fabsf(prm.gravity[2]), prm.boundary_padding);
         v4[g] = make_float4(o[0], o[1], o[2], t.w);
     }
-}
-
-// ---------------------------------------------------------------------------
-// G2P (+ cov), optionally fused with the next substep's stress update
-// ---------------------------------------------------------------------------
-template <bool Fused>
-__global__ void __launch_bounds__(kBlock) k_g2p(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
-                                               uint32_t *status)
-{
-    const int64_t n = P.n;
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    if (P.active[p] != 1) return;
-    if (!(P.material[p] <= 1)) return;
-    const int nx = G.dims[0], ny = G.dims[1], nz = G.dims[2];
-    const float4 *__restrict__ gv = reinterpret_cast<const float4 *>(G.v);
-    float xp[3];
-    load3(P.x, n, p, xp);
-    Weights W;
-    weights(xp, prm.min_bounds, prm.inv_dx, W);
-    const float inv_dx = prm.inv_dx, dt = prm.dt;
-    float nv[3] = {0.f, 0.f, 0.f}, nC[9], nF[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) { nC[k] = 0.f; nF[k] = 0.f; }
-    uint32_t bad = 0;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                float dpos[3] = {(float)i - W.fx[0], (float)j - W.fx[1], (float)k - W.fx[2]};
-                float weight = (W.w[0][i] * W.w[1][j]) * W.w[2][k];
-                int ix = W.base[0] + i, iy = W.base[1] + j, iz = W.base[2] + k;
-                float g3[3] = {0.f, 0.f, 0.f};
-                if (ix < 0 || iy < 0 || iz < 0 || ix >= nx || iy >= ny || iz >= nz) bad = MPMW_ST_OOB;
-                else {
-                    float4 t = __ldg(&gv[((int64_t)ix * ny + iy) * nz + iz]);
-                    g3[0] = t.x; g3[1] = t.y; g3[2] = t.z;
-                }
-#pragma unroll
-                for (int a = 0; a < 3; ++a) nv[a] = nv[a] + g3[a] * weight;
-                float sc = (weight * inv_dx) * 4.f;
-#pragma unroll
-                for (int r = 0; r < 3; ++r)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) nC[3 * r + c] = nC[3 * r + c] + (g3[r] * dpos[c]) * sc;
-                float dwt[3] = {((W.dw[0][i] * W.w[1][j]) * W.w[2][k]) * inv_dx,
-                                ((W.w[0][i] * W.dw[1][j]) * W.w[2][k]) * inv_dx,
-                                ((W.w[0][i] * W.w[1][j]) * W.dw[2][k]) * inv_dx};
-#pragma unroll
-                for (int r = 0; r < 3; ++r)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) nF[3 * r + c] = nF[3 * r + c] + g3[r] * dwt[c];
-            }
-    float xn[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) xn[a] = xp[a] + dt * nv[a];
-    if (!(isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]))) bad |= MPMW_ST_NAN;
-    float F[9], A[9], Ft[9];
-    load9(P.F, n, p, F);
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) A[3 * r + c] = (r == c ? 1.f : 0.f) + nF[3 * r + c] * dt;
-    matmul3(A, F, Ft);
-    if (prm.update_cov && P.cov) {
-        float *cv = P.cov + 6 * p;
-        float cn[9] = {cv[0], cv[1], cv[2], cv[1], cv[3], cv[4], cv[2], cv[4], cv[5]};
-        float a1[9], a2[9];
-        matmul3(nF, cn, a1);
-        matmul3_bt(cn, nF, a2);
-        float c1[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) c1[k] = cn[k] + dt * (a1[k] + a2[k]);
-        cv[0] = c1[0]; cv[1] = c1[1]; cv[2] = c1[2]; cv[3] = c1[4]; cv[4] = c1[5]; cv[5] = c1[8];
-    }
-    store3(P.x, n, p, xn);
-    store9(P.C, n, p, nC);
-    if (Fused) {
-        float Fo[9], out[9];
-        stress_particle<true>(P, prm.eff, p, Ft, nC, xn, nv, Fo, out);
-        store9(P.F, n, p, Fo);
-        store_sym6(P.stress, n, p, out);
-    } else {
-        store9(P.F_trial, n, p, Ft);
-    }
-    store3(P.v, n, p, nv);
-    if (bad) raise_status(status, bad);
 }
 
 // ---------------------------------------------------------------------------
@@ -746,31 +393,11 @@ static int check_params(const mpmw_params_t *prm)
     } while (0)
 
 // host-side launchers (also used by the multi-step driver)
-int launch_stress(const mpmw_particles_t &p, const mpmw_params_t &prm, cudaStream_t s)
-{
-    if (p.n == 0) return MPMW_OK;
-    k_stress<<<grid_for(p.n), kBlock, 0, s>>>(p, prm.eff);
-    return check_launch("k_stress");
-}
-int launch_p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, cudaStream_t s)
-{
-    if (p.n == 0) return MPMW_OK;
-    k_p2g<<<grid_for(p.n), kBlock, 0, s>>>(p, g, prm, st);
-    return check_launch("k_p2g");
-}
 int launch_grid(const mpmw_grid_t &g, const mpmw_params_t &prm, cudaStream_t s)
 {
     int64_t G = (int64_t)g.dims[0] * g.dims[1] * g.dims[2];
     k_grid_update<<<grid_for(G), kBlock, 0, s>>>(g, prm);
     return check_launch("k_grid_update");
-}
-int launch_g2p(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, bool fused,
-               cudaStream_t s)
-{
-    if (p.n == 0) return MPMW_OK;
-    if (fused) k_g2p<true><<<grid_for(p.n), kBlock, 0, s>>>(p, g, prm, st);
-    else k_g2p<false><<<grid_for(p.n), kBlock, 0, s>>>(p, g, prm, st);
-    return check_launch(fused ? "k_g2p<fused>" : "k_g2p");
 }
 int launch_vlc(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, cudaStream_t s)
 {

@@ -1,0 +1,566 @@
+// mpmw_xpbd.cu -- XPBD substep kernels and the spatial hash (C-ABI entry points).
+//
+// Reference (MPMWarpYDW): utils/xpbdRoutines.py, launch order
+// utils/simulationRoutines.py:295-526, hash grid wp.HashGrid (simStates.py:174).
+//
+// Spatial hash (restates wp.HashGrid's documented behaviour):
+//   cell of a point  = truncating casts of p * (1/cell_width) per axis, offset by
+//                      2^20, clamped at 0, reduced modulo the hash dims;
+//                      hash = cz*(dx*dy) + cy*dx + cx
+//   point order      = stable sort of point indices by hash (LSD radix sort,
+//                      7-bit digits, rank within a tile taken in index order)
+//   cell ranges      = [start, end) of each hash in the sorted order, 0/0 if empty
+//   query            = cells from trunc((p - r)/w) to trunc((p + r)/w) per axis
+//                      (at most dims cells per axis), x fastest, then y, then z;
+//                      within a cell, sorted order
+#include "mpmw_common.cuh"
+#include "mpmw_math.cuh"
+#include "mpmw_scan.cuh"
+#include "../../include/mpmw_xpbd.h"
+
+namespace mpmw {
+
+// ---------------------------------------------------------------------------
+// hash cells
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int hash_index(const int *hd, int x, int y, int z)
+{
+    const int origin = 1 << 20;
+    x += origin; y += origin; z += origin;
+    x = x < 0 ? 0 : x;
+    y = y < 0 ? 0 : y;
+    z = z < 0 ? 0 : z;
+    int cx = x % hd[0], cy = y % hd[1], cz = z % hd[2];
+    return cz * (hd[0] * hd[1]) + cy * hd[0] + cx;
+}
+
+struct HashDims { int d[3]; };
+
+__global__ void k_hash_cells(const float *__restrict__ x, int64_t n, float inv, HashDims hd, int *__restrict__ keys,
+                             int *__restrict__ ids, int *__restrict__ point_cells)
+{
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    int cx = (int)(x[p] * inv), cy = (int)(x[n + p] * inv), cz = (int)(x[2 * n + p] * inv);
+    int h = hash_index(hd.d, cx, cy, cz);
+    keys[p] = h;
+    ids[p] = (int)p;
+    if (point_cells) point_cells[p] = h;
+}
+
+// ---------------------------------------------------------------------------
+// stable LSD radix sort of (key, id) pairs, 7-bit digits
+// ---------------------------------------------------------------------------
+constexpr int kRadixBits = 7;
+constexpr int kRadix = 1 << kRadixBits;
+constexpr int kSortThreads = 256;
+constexpr int kSortRounds = 16;
+constexpr int kSortTile = kSortThreads * kSortRounds;  // 4096 items per tile
+
+// per-tile digit histogram, stored digit-major: hist[d * ntiles + tile]
+__global__ void __launch_bounds__(kSortThreads) k_radix_hist(const int *__restrict__ keys, int64_t n, int shift,
+                                                            int ntiles, int *__restrict__ hist)
+{
+    __shared__ int h[kRadix];
+    for (int i = threadIdx.x; i < kRadix; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    int64_t base = (int64_t)blockIdx.x * kSortTile;
+    for (int r = 0; r < kSortRounds; ++r) {
+        int64_t i = base + (int64_t)r * kSortThreads + threadIdx.x;
+        if (i < n) atomicAdd(&h[(keys[i] >> shift) & (kRadix - 1)], 1);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) hist[(int64_t)d * ntiles + blockIdx.x] = h[d];
+}
+
+// stable scatter: offsets[d * ntiles + tile] is the exclusive prefix of hist
+__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const int *__restrict__ kin, const int *__restrict__ vin,
+                                                               int64_t n, int shift, int ntiles,
+                                                               const int *__restrict__ offsets, int *__restrict__ kout,
+                                                               int *__restrict__ vout)
+{
+    constexpr int kWarps = kSortThreads / 32;
+    __shared__ int run[kRadix];            // items of each digit placed by earlier rounds
+    __shared__ int wcnt[kWarps][kRadix];   // per-warp digit counts of the current round
+    __shared__ int tile_off[kRadix];
+    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+        run[d] = 0;
+        tile_off[d] = offsets[(int64_t)d * ntiles + blockIdx.x];
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    int64_t base = (int64_t)blockIdx.x * kSortTile;
+    for (int r = 0; r < kSortRounds; ++r) {
+        for (int d = threadIdx.x; d < kWarps * kRadix; d += blockDim.x) (&wcnt[0][0])[d] = 0;
+        __syncthreads();
+        int64_t i = base + (int64_t)r * kSortThreads + threadIdx.x;
+        bool valid = i < n;
+        int key = valid ? kin[i] : 0;
+        int val = valid ? vin[i] : 0;
+        int dig = valid ? ((key >> shift) & (kRadix - 1)) : kRadix;  // invalid items in their own class
+        unsigned peers = __match_any_sync(0xffffffffu, dig);
+        int rank = __popc(peers & lt);
+        int leader = __ffs(peers) - 1;
+        if (valid && lane == leader) wcnt[wid][dig] = __popc(peers);
+        __syncthreads();
+        if (valid) {
+            int before = 0;
+            for (int w = 0; w < wid; ++w) before += wcnt[w][dig];
+            int pos = tile_off[dig] + run[dig] + before + rank;
+            kout[pos] = key;
+            vout[pos] = val;
+        }
+        __syncthreads();
+        for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+            int s = 0;
+            for (int w = 0; w < kWarps; ++w) s += wcnt[w][d];
+            run[d] += s;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_cell_ranges(const int *__restrict__ skeys, int64_t n, int *__restrict__ starts, int *__restrict__ ends)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c = skeys[i];
+    if (i == 0 || skeys[i - 1] != c) starts[c] = (int)i;
+    if (i == n - 1 || skeys[i + 1] != c) ends[c] = (int)(i + 1);
+}
+
+static int64_t sort_tiles(int64_t n) { return (n + kSortTile - 1) / kSortTile; }
+
+size_t hash_workspace_bytes(int64_t n)
+{
+    int64_t nt = sort_tiles(n);
+    int64_t hist = (int64_t)kRadix * nt;
+    int64_t scan_scratch = scan_blocks(hist > 0 ? hist : 1) + 1;
+    // keys_a, keys_b, ids_b, hist, offsets, scan scratch (ints), 256-byte aligned pieces
+    auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
+    return (size_t)(al(4 * n) * 3 + al(4 * hist) * 2 + al(4 * scan_scratch));
+}
+
+int hash_build(const float *x, int64_t n, const mpmw_hash_t &h, void *ws, size_t ws_bytes, cudaStream_t s)
+{
+    if (ws_bytes < hash_workspace_bytes(n)) {
+        set_error("hash_build: workspace of %zu bytes is smaller than the %zu required", ws_bytes,
+                  hash_workspace_bytes(n));
+        return MPMW_E_WORKSPACE;
+    }
+    const int64_t ncell = (int64_t)h.dims[0] * h.dims[1] * h.dims[2];
+    if (cudaMemsetAsync(h.cell_starts, 0, ncell * sizeof(int), s) != cudaSuccess ||
+        cudaMemsetAsync(h.cell_ends, 0, ncell * sizeof(int), s) != cudaSuccess) {
+        set_error("hash_build: memset failed");
+        return MPMW_E_DEVICE;
+    }
+    if (n == 0) return MPMW_OK;
+    auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
+    const int64_t nt = sort_tiles(n), hist_n = (int64_t)kRadix * nt;
+    char *w = static_cast<char *>(ws);
+    int *keys_a = reinterpret_cast<int *>(w); w += al(4 * n);
+    int *keys_b = reinterpret_cast<int *>(w); w += al(4 * n);
+    int *ids_b = reinterpret_cast<int *>(w); w += al(4 * n);
+    int *hist = reinterpret_cast<int *>(w); w += al(4 * hist_n);
+    int *offs = reinterpret_cast<int *>(w); w += al(4 * hist_n);
+    int *scr = reinterpret_cast<int *>(w);
+    int *ids_a = h.point_ids;  // the sorted ids end up here (3 passes: a->b->a->b, then copy)
+    HashDims hd{{h.dims[0], h.dims[1], h.dims[2]}};
+    float inv = 1.0f / h.cell_width;
+    k_hash_cells<<<grid_for(n), kBlock, 0, s>>>(x, n, inv, hd, keys_a, ids_a, h.point_cells);
+    MPMW_TRY_LAUNCH("k_hash_cells");
+    int bits = 0;
+    for (int64_t c = ncell - 1; c > 0; c >>= 1) ++bits;
+    int *ki = keys_a, *vi = ids_a, *ko = keys_b, *vo = ids_b;
+    for (int shift = 0; shift < bits; shift += kRadixBits) {
+        k_radix_hist<<<(unsigned)nt, kSortThreads, 0, s>>>(ki, n, shift, (int)nt, hist);
+        MPMW_TRY_LAUNCH("k_radix_hist");
+        if (!exclusive_scan(hist, offs, hist_n, scr, s)) { set_error("hash_build: too many points"); return MPMW_E_ARG; }
+        MPMW_TRY_LAUNCH("scan");
+        k_radix_scatter<<<(unsigned)nt, kSortThreads, 0, s>>>(ki, vi, n, shift, (int)nt, offs, ko, vo);
+        MPMW_TRY_LAUNCH("k_radix_scatter");
+        int *t = ki; ki = ko; ko = t;
+        t = vi; vi = vo; vo = t;
+    }
+    if (vi != h.point_ids) {
+        if (cudaMemcpyAsync(h.point_ids, vi, n * sizeof(int), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+            set_error("hash_build: copy failed");
+            return MPMW_E_DEVICE;
+        }
+    }
+    k_cell_ranges<<<grid_for(n), kBlock, 0, s>>>(ki, n, h.cell_starts, h.cell_ends);
+    MPMW_TRY_LAUNCH("k_cell_ranges");
+    return MPMW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// XPBD kernels
+// ---------------------------------------------------------------------------
+// copies (x, v) into the integrated buffers and integrates XPBD particles
+// (simulationRoutines.py:314-331 + xpbdRoutines.py:23-48)
+// flag bit0: read from the particle x/v (else from x_int/v_int);
+// flag bit1: write every particle (the wp.copy), else only integrated ones
+__global__ void k_xpbd_integrate(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int flag)
+{
+    const int64_t n = P.n;
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    float x0[3], v0[3];
+    load3((flag & 1) ? P.x : X.x_int, n, p, x0);
+    load3((flag & 1) ? P.v : X.v_int, n, p, v0);
+    bool integ = P.active[p] == 1 && P.material[p] == 2;
+    if (integ) {
+        float v1[3] = {v0[0] + q.gravity[0] * q.dt, v0[1] + q.gravity[1] * q.dt, v0[2] + q.gravity[2] * q.dt};
+        float m = len3(v1);
+        if (m > q.v_max) { float s = q.v_max / m; v1[0] = v1[0] * s; v1[1] = v1[1] * s; v1[2] = v1[2] * s; }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { x0[a] = x0[a] + v1[a] * q.dt; v0[a] = v1[a]; }
+    }
+    if (integ || (flag & 2)) {
+        store3(X.x_int, n, p, x0);
+        store3(X.v_int, n, p, v0);
+    }
+}
+
+// xpbdRoutines.py:3-21
+__global__ void k_reset_labels(mpmw_particles_t P)
+{
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.n) return;
+    if (P.active[p] == 1 && P.material[p] == 0) P.material[p] = 1;
+}
+
+// xpbdRoutines.py:49-136; writes delta (the reference zeroes it first, then adds)
+__global__ void k_bound_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int accumulate)
+{
+    const int64_t n = P.n;
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    float acc[3] = {0.f, 0.f, 0.f};
+    if (accumulate) load3(X.delta, n, p, acc);
+    if (P.active[p] == 1 && P.material[p] == 2 && P.mass[p] != 0.f) {
+        float wi = 1.f / P.mass[p];
+        float xp[3], vp[3];
+        load3(X.x_int, n, p, xp);
+        load3(X.v_int, n, p, vp);
+        float r = P.radius[p];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                float nrm[3] = {0.f, 0.f, 0.f};
+                nrm[i] = side == 0 ? 1.f : -1.f;
+                const float *b = side == 0 ? q.bmin : q.bmax;
+                float d[3] = {xp[0] - b[0], xp[1] - b[1], xp[2] - b[2]};
+                float c = rmin(dot3(nrm, d) - r, 0.f);
+                if (!(c < 0.f)) continue;
+                float ln = c;
+                float dn[3] = {nrm[0] * ln, nrm[1] * ln, nrm[2] * ln};
+                float vn = dot3(nrm, vp);
+                float fmu = q.dyn_friction;
+                if (fabsf(vn) < q.static_thr * r) fmu = q.static_friction;
+                float vt[3] = {vp[0] - nrm[0] * vn, vp[1] - nrm[1] * vn, vp[2] - nrm[2] * vn};
+                float vtl = len3(vt);
+                float lf = rmax(fmu * ln, -vtl * q.dt);
+                float df[3] = {0.f, 0.f, 0.f};
+                if (vtl > 1e-8f) { float nv[3]; normalize3(vt, nv); df[0] = nv[0] * lf; df[1] = nv[1] * lf; df[2] = nv[2] * lf; }
+#pragma unroll
+                for (int a = 0; a < 3; ++a) acc[a] = acc[a] + (((df[a] - dn[a]) / wi) * q.relaxation) * wi;
+            }
+        }
+    }
+    store3(X.delta, n, p, acc);
+}
+
+// xpbdRoutines.py:138-219.  One thread per sorted position tid; the outer
+// checks use tid, the work uses the sorted point i (reference behaviour).
+// Each deltas[i] is owned by exactly one thread, so it is read-modify-written
+// without atomics; the contact-lock label writes only ever store 0 over a
+// label <= 1, which no test in this kernel distinguishes from 1.
+__global__ void k_particle_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash_t H, mpmw_xpbd_params_t q)
+{
+    const int64_t n = P.n;
+    int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= n) return;
+    if (P.active[tid] != 1) return;
+    if (!(P.material[tid] >= 0)) return;
+    int i = H.point_ids[tid];
+    if (i == -1) return;
+    float xi[3], vi[3];
+    load3(X.x_int, n, i, xi);
+    load3(X.v_int, n, i, vi);
+    float rad = P.radius[i];
+    if (P.mass[tid] == 0.f) return;
+    float w1 = 1.f / P.mass[i];
+    const float inv = 1.0f / H.cell_width;
+    const float qr = (rad + q.max_radius) + q.cohesion * rad;
+    const int hd[3] = {H.dims[0], H.dims[1], H.dims[2]};
+    int xs = (int)((xi[0] - qr) * inv), ys = (int)((xi[1] - qr) * inv), zs = (int)((xi[2] - qr) * inv);
+    int xe = (int)((xi[0] + qr) * inv), ye = (int)((xi[1] + qr) * inv), ze = (int)((xi[2] + qr) * inv);
+    xe = xe < xs + hd[0] - 1 ? xe : xs + hd[0] - 1;
+    ye = ye < ys + hd[1] - 1 ? ye : ys + hd[1] - 1;
+    ze = ze < zs + hd[2] - 1 ? ze : zs + hd[2] - 1;
+    float dl[3] = {0.f, 0.f, 0.f};
+    const float alpha = 0.f;
+    float k_mu = q.dyn_friction;
+    int mat_i = P.material[i];
+    for (int cz = zs; cz <= ze; ++cz)
+        for (int cy = ys; cy <= ye; ++cy)
+            for (int cx = xs; cx <= xe; ++cx) {
+                int c = hash_index(hd, cx, cy, cz);
+                int b = H.cell_starts[c], e = H.cell_ends[c];
+                for (int s = b; s < e; ++s) {
+                    int index = H.point_ids[s];
+                    if (!(P.active[index] == 1 && index != i && P.mass[index] > 0.f)) continue;
+                    int mat_j = P.material[index];
+                    if (mat_i <= 1 && mat_j <= 1) continue;
+                    float xj[3];
+                    load3(X.x_int, n, index, xj);
+                    float nn[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
+                    float d = len3(nn);
+                    float err = (d - rad) - P.radius[index];
+                    float w2 = 1.f / P.mass[index];
+                    float denom = w1 + w2;
+                    if (err <= q.cohesion && denom > 0.f) {
+                        if (q.lock == 1) {
+                            if (mat_i <= 1 && mat_j == 2) P.material[i] = 0;
+                            if (mat_i == 2 && mat_j <= 1) P.material[index] = 0;
+                        }
+                        float nu[3] = {nn[0] / d, nn[1] / d, nn[2] / d};
+                        float vj[3];
+                        load3(X.v_int, n, index, vj);
+                        float vrel[3] = {vi[0] - vj[0], vi[1] - vj[1], vi[2] - vj[2]};
+                        float ln = err / (1.f + (alpha * q.dt) * q.dt);
+                        float dn[3] = {nu[0] * ln, nu[1] * ln, nu[2] * ln};
+                        float vn = dot3(nu, vrel);
+                        if (fabsf(vn) < q.static_thr * rad) k_mu = q.static_friction;
+                        float vt[3] = {vrel[0] - nu[0] * vn, vrel[1] - nu[1] * vn, vrel[2] - nu[2] * vn};
+                        float lf = rmax(k_mu * ln, -len3(vt) * q.dt);
+                        float nv[3];
+                        normalize3(vt, nv);
+                        float df[3] = {nv[0] * lf, nv[1] * lf, nv[2] * lf};
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) dl[a] = dl[a] + ((df[a] - dn[a]) / denom) * w1;
+                    }
+                }
+            }
+    float cur[3];
+    load3(X.delta, n, i, cur);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) cur[a] = cur[a] + dl[a] * q.relaxation;
+    store3(X.delta, n, i, cur);
+}
+
+// xpbdRoutines.py:221-257 my_apply_particle_deltas, with the surrounding copies
+// (simulationRoutines.py:398-421) folded in: x_int/v_int are updated in place;
+// with write_tmp the deltaInt buffers receive the same values.
+__global__ void k_apply_deltas(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int write_tmp)
+{
+    const int64_t n = P.n;
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    float xn[3], vn[3];
+    load3(X.x_int, n, p, xn);
+    load3(X.v_int, n, p, vn);
+    if (P.active[p] == 1) {
+        float d[3];
+        load3(X.delta, n, p, d);
+        if (isnan(d[0]) || isnan(d[1]) || isnan(d[2])) d[0] = d[1] = d[2] = 0.f;
+        float x0[3];
+        load3(P.x, n, p, x0);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { xn[a] = xn[a] + d[a]; vn[a] = (xn[a] - x0[a]) / q.dt; }
+        float m = len3(vn);
+        if (m > q.v_max) { float s = q.v_max / m; vn[0] = vn[0] * s; vn[1] = vn[1] * s; vn[2] = vn[2] * s; }
+        store3(X.x_int, n, p, xn);
+        store3(X.v_int, n, p, vn);
+    }
+    if (write_tmp) {
+        store3(X.x_dI, n, p, xn);
+        store3(X.v_dI, n, p, vn);
+    }
+}
+
+// xpbdRoutines.py:312-334 sleepParticles (counts[0] total, counts[1] sleeping)
+__global__ void k_sleep(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q)
+{
+    const int64_t n = P.n;
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool is = p < n && P.active[p] == 1 && P.material[p] == 2;
+    bool slept = false;
+    if (is) {
+        float a[3], b[3];
+        load3(P.x, n, p, b);
+        load3(X.x_int, n, p, a);
+        float dd[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]};
+        float d = len3(dd);
+        if (d / q.dt < q.sleep_thr * P.radius[p]) {
+            store3(X.x_int, n, p, b);
+            slept = true;
+        }
+        X.cum_dist[p] = X.cum_dist[p] + d;
+    }
+    // warp-aggregated counters
+    unsigned m_all = __ballot_sync(0xffffffffu, is), m_sl = __ballot_sync(0xffffffffu, slept);
+    if ((threadIdx.x & 31) == 0 && X.counts) {
+        if (m_all) atomicAdd(&X.counts[0], __popc(m_all));
+        if (m_sl) atomicAdd(&X.counts[1], __popc(m_sl));
+    }
+}
+
+// simulationRoutines.py:444-470: v_before_contact <- v, apply_mpm_contact_impulses
+// (xpbdRoutines.py:259-310), then commit x <- x_int, v <- v_int
+__global__ void k_impulses_commit(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q)
+{
+    const int64_t n = P.n;
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    float x0[3], v0[3], xf[3], vf[3];
+    load3(P.x, n, p, x0);
+    load3(P.v, n, p, v0);
+    load3(X.x_int, n, p, xf);
+    load3(X.v_int, n, p, vf);
+    if (X.v_before) store3(X.v_before, n, p, v0);
+    if (P.active[p] == 1 && P.material[p] <= 1) {
+        xf[0] = x0[0]; xf[1] = x0[1]; xf[2] = x0[2];
+        if (q.xpbd_only == 0) {
+            float vc[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) vc[a] = v0[a] + ((xf[a] - x0[a]) / q.dt) * q.coupling;
+            float m = len3(vc);
+            if (m > q.v_max) { float s = q.v_max / m; vc[0] = vc[0] * s; vc[1] = vc[1] * s; vc[2] = vc[2] * s; }
+            vf[0] = vc[0]; vf[1] = vc[1]; vf[2] = vc[2];
+        }
+        store3(X.x_int, n, p, xf);
+        store3(X.v_int, n, p, vf);
+    }
+    store3(P.x, n, p, xf);
+    store3(P.v, n, p, vf);
+}
+
+// xpbdRoutines.py:354-375 swellParticlesType2
+__global__ void k_swell(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q)
+{
+    const int64_t n = P.n;
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    if (P.active[p] != 1 || P.material[p] != 2) return;
+    float x[3], x0[3];
+    load3(P.x, n, p, x);
+    load3(P.x_pc, n, p, x0);
+    float dd[3] = {x[0] - x0[0], x[1] - x0[1], x[2] - x0[2]};
+    float br = X.base_radius[p];
+    float dxv = len3(dd) * br;
+    float factor = q.swell_act * br;
+    float fmax = q.swell_max * br;
+    if (dxv > factor) {
+        float sr = X.max_radius[p];
+        float nr = br + ((sr - br) * (dxv - factor)) / (fmax - factor);
+        nr = rmin(rmax(nr, P.radius[p]), sr);
+        P.radius[p] = nr;
+    }
+}
+
+}  // namespace mpmw
+
+using namespace mpmw;
+
+static int check_xpbd_args(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_xpbd_params_t *q)
+{
+    if (!p || !x || !q) { set_error("xpbd: NULL argument"); return MPMW_E_ARG; }
+    if (p->n < 0) { set_error("xpbd: negative particle count"); return MPMW_E_ARG; }
+    if (p->n == 0) return MPMW_OK;
+    if (!p->x || !p->v || !p->active || !p->material || !p->mass || !p->radius) {
+        set_error("xpbd: x, v, active, material, mass and radius are required");
+        return MPMW_E_ARG;
+    }
+    if (!x->x_int || !x->v_int || !x->delta) { set_error("xpbd: x_int, v_int and delta are required"); return MPMW_E_ARG; }
+    if (q->dt == 0.f) { set_error("xpbd: dt must be nonzero"); return MPMW_E_ARG; }
+    return MPMW_OK;
+}
+
+static int check_hash(const mpmw_hash_t *h, int64_t n)
+{
+    if (!h) { set_error("hash: NULL"); return MPMW_E_ARG; }
+    if (h->dims[0] <= 0 || h->dims[1] <= 0 || h->dims[2] <= 0 ||
+        (int64_t)h->dims[0] * h->dims[1] * h->dims[2] > (int64_t)INT32_MAX) {
+        set_error("hash: bad dims"); return MPMW_E_ARG;
+    }
+    if (!(h->cell_width > 0.f)) { set_error("hash: cell_width must be positive"); return MPMW_E_ARG; }
+    if (n > 0 && (!h->point_ids || !h->cell_starts || !h->cell_ends)) { set_error("hash: arrays are required"); return MPMW_E_ARG; }
+    if (n > (int64_t)INT32_MAX) { set_error("hash: too many points"); return MPMW_E_ARG; }
+    return MPMW_OK;
+}
+
+#define TRY(expr) do { int _rc = (expr); if (_rc != MPMW_OK) return _rc; } while (0)
+
+extern "C" {
+
+size_t mpmw_hash_workspace_bytes(int64_t n) { return mpmw::hash_workspace_bytes(n < 0 ? 0 : n); }
+
+int mpmw_hash_build(const float *x, int64_t n, const mpmw_hash_t *h, void *workspace, size_t ws_bytes,
+                    mpmw_stream_t stream)
+{
+    TRY(check_hash(h, n));
+    if (n < 0 || (n > 0 && (!x || !workspace))) { set_error("hash_build: bad arguments"); return MPMW_E_ARG; }
+    return mpmw::hash_build(x, n, *h, workspace, ws_bytes, as_stream(stream));
+}
+
+int mpmw_xpbd_kernel(int which, const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_hash_t *h,
+                     const mpmw_xpbd_params_t *q, int flag, mpmw_stream_t stream)
+{
+    TRY(check_xpbd_args(p, x, q));
+    if (p->n == 0) return MPMW_OK;
+    cudaStream_t s = as_stream(stream);
+    unsigned g = grid_for(p->n);
+    switch (which) {
+    case MPMW_XK_INTEGRATE: k_xpbd_integrate<<<g, kBlock, 0, s>>>(*p, *x, *q, flag); break;
+    case MPMW_XK_RESET_LABELS: k_reset_labels<<<g, kBlock, 0, s>>>(*p); break;
+    case MPMW_XK_BOUND: k_bound_contacts<<<g, kBlock, 0, s>>>(*p, *x, *q, flag); break;
+    case MPMW_XK_PARTICLE:
+        TRY(check_hash(h, p->n));
+        k_particle_contacts<<<g, kBlock, 0, s>>>(*p, *x, *h, *q);
+        break;
+    case MPMW_XK_APPLY: k_apply_deltas<<<g, kBlock, 0, s>>>(*p, *x, *q, flag); break;
+    case MPMW_XK_SLEEP:
+        if (x->counts && flag && cudaMemsetAsync(x->counts, 0, 2 * sizeof(int), s) != cudaSuccess) {
+            set_error("sleep: memset failed"); return MPMW_E_DEVICE;
+        }
+        if (!x->cum_dist) { set_error("sleep: cum_dist is required"); return MPMW_E_ARG; }
+        k_sleep<<<g, kBlock, 0, s>>>(*p, *x, *q);
+        break;
+    case MPMW_XK_IMPULSES: k_impulses_commit<<<g, kBlock, 0, s>>>(*p, *x, *q); break;
+    case MPMW_XK_SWELL:
+        if (!x->base_radius || !x->max_radius || !p->x_pc) { set_error("swell: radii and x_pc are required"); return MPMW_E_ARG; }
+        k_swell<<<g, kBlock, 0, s>>>(*p, *x, *q);
+        break;
+    default: set_error("xpbd_kernel: unknown kernel %d", which); return MPMW_E_ARG;
+    }
+    return check_launch("xpbd kernel");
+}
+
+int mpmw_xpbd_step(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_hash_t *h,
+                   const mpmw_xpbd_params_t *q, void *workspace, size_t ws_bytes, mpmw_stream_t stream)
+{
+    TRY(check_xpbd_args(p, x, q));
+    TRY(check_hash(h, p->n));
+    if (p->n == 0) return MPMW_OK;
+    cudaStream_t s = as_stream(stream);
+    TRY(mpmw_hash_build(p->x, p->n, h, workspace, ws_bytes, stream));
+    TRY(mpmw_xpbd_kernel(MPMW_XK_INTEGRATE, p, x, h, q, 1, stream));
+    if (q->lock && !q->xpbd_only) TRY(mpmw_xpbd_kernel(MPMW_XK_RESET_LABELS, p, x, h, q, 0, stream));
+    mpmw_xpbd_params_t qi = *q;
+    if (q->xpbd_only) qi.lock = 0;
+    for (int it = 0; it < q->iterations; ++it) {
+        TRY(mpmw_xpbd_kernel(MPMW_XK_BOUND, p, x, h, &qi, 0, stream));
+        TRY(mpmw_xpbd_kernel(MPMW_XK_PARTICLE, p, x, h, &qi, 0, stream));
+        TRY(mpmw_xpbd_kernel(MPMW_XK_APPLY, p, x, h, &qi, it == q->iterations - 1, stream));
+    }
+    TRY(mpmw_xpbd_kernel(MPMW_XK_SLEEP, p, x, h, q, 1, stream));
+    TRY(mpmw_xpbd_kernel(MPMW_XK_IMPULSES, p, x, h, q, 0, stream));
+    if (q->swelling_ratio > 0.f) TRY(mpmw_xpbd_kernel(MPMW_XK_SWELL, p, x, h, q, 0, stream));
+    (void)s;
+    return MPMW_OK;
+}
+
+}  // extern "C"

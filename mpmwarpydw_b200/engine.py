@@ -21,9 +21,15 @@ from .state import Mat33Field, ScalarField, Sym33Field, Vec3Field
 
 
 def block_sort_key(x_n3: torch.Tensor, minBounds, inv_dx: float, dims, block: int = 4) -> torch.Tensor:
-    """int64 key: (block index in C order) * block^3 + (cell index inside the block)."""
+    """int64 key: (block index in C order) * block^3 + (cell index inside the block).
+
+    The cell is the particle's stencil base, int((x - minBounds) * inv_dx - 0.5)
+    in FP32 with truncation (utils/mpmRoutines.py:514-517), so particles sharing
+    a key scatter to the same 27 nodes."""
     mb = torch.as_tensor(minBounds, dtype=torch.float32, device=x_n3.device)
-    cell = torch.floor((x_n3 - mb) * inv_dx).to(torch.int64)
+    inv = torch.tensor(inv_dx, dtype=torch.float32, device=x_n3.device)
+    gp = (x_n3.to(torch.float32) - mb) * inv
+    cell = (gp - 0.5).to(torch.int64)  # truncation toward zero, as the kernels
     d = torch.as_tensor(dims, dtype=torch.int64, device=x_n3.device)
     cell = torch.minimum(torch.clamp(cell, min=0), d - 1)
     nb = (d + block - 1) // block

@@ -94,8 +94,13 @@ def compute_stress_from_F_trial(activeLabel, materialLabel, particlePosition, pa
                                 initialPhaseChangePosition, initialPhaseChangeVelocity, particle_F,
                                 particle_F_trial, mu, lam, yield_stress, hardening, softening, particle_density,
                                 strainCriteria, efficiency, eta_shear, eta_bulk, particle_C, particle_stress,
-                                particle_accumulated_strain, particle_damage, constitutive_model, alpha):
-    """utils/mpmRoutines.py:229-312 (return map :314-453, Kirchhoff :456-471)."""
+                                particle_accumulated_strain, particle_damage, constitutive_model, alpha,
+                                stress_mode=0):
+    """utils/mpmRoutines.py:229-312 (return map :314-453, Kirchhoff :456-471).
+
+    ``stress_mode`` (not in the reference): 0 lets clearly elastic particles
+    take the SVD-free log-strain path (same stress, less FP32 rounding), 1
+    runs the SVD return map for every particle."""
     m = Marshal()
     P = particles_struct(
         activeLabel.numel(), active=m.labels(activeLabel), material=m.labels(materialLabel, out=True),
@@ -107,7 +112,7 @@ def compute_stress_from_F_trial(activeLabel, materialLabel, particlePosition, pa
         eta_shear=m.scalar(eta_shear), eta_bulk=m.scalar(eta_bulk), C=m.mat33(particle_C),
         stress=m.sym33(particle_stress, out=True), acc_strain=m.scalar(particle_accumulated_strain, out=True),
         damage=m.scalar(particle_damage, out=True), alpha=m.scalar(alpha, out=True))
-    prm = params_struct(eff=efficiency, constitutive_model=constitutive_model)
+    prm = params_struct(eff=efficiency, constitutive_model=constitutive_model, stress_mode=stress_mode)
     dev = _dev(activeLabel)
     _call(_lib.lib().mpmw_stress, P, prm, status_word(dev).data_ptr(), stream_handle(),
           what="compute_stress_from_F_trial")

@@ -151,6 +151,9 @@ class MPMState:
         self.cell_vol_sum = torch.zeros(self.gridDims, dtype=F32, device=d)
         self.particle_x_initial = torch.zeros(n, 3, dtype=F32, device=d)
         self.eff = args.eff
+        # 0 (default): clearly elastic particles take the SVD-free log-strain path,
+        # all others the SVD return map; 1: SVD return map for every particle
+        self.stress_mode = int(getattr(args, "stress_mode", 0))
 
     @property
     def grid_m(self):

@@ -103,43 +103,57 @@ static inline void matvec3(const REAL *M, const REAL *v, REAL *o)
 /* F = U diag(s) V^T with U, V proper rotations, s0 >= s1 >= |s2| and        */
 /* sign(s2) = sign(det F).  Algorithm:                                      */
 /*  1. S = F^T F;                                                           */
-/*  2. four cyclic Jacobi sweeps over (0,1),(0,2),(1,2) with the exact      */
-/*     rotation (t = sgn(th)/(|th|+sqrt(th^2+1)), c = 1/sqrt(t^2+1)),       */
-/*     skipping pairs whose off-diagonal is exactly zero; V accumulates J;  */
+/*  2. cyclic Jacobi sweeps over (0,1),(0,2),(1,2) (jacobi_rot), at most 6, */
+/*     ending after a sweep in which every pair was converged; V            */
+/*     accumulates the rotations;                                           */
 /*  3. sort eigenvalues descending (compare-swap network (0,1),(0,2),(1,2)),*/
 /*     then flip V's last column if det V < 0;                              */
 /*  4. B = F V; u0 = b0/|b0|; u1 = Gram-Schmidt(b1)/|.|; u2 = u0 x u1;       */
 /*     s0 = |b0|, s1 = |b1 - (u0.b1)u0|, s2 = u2.b2.                          */
 /* The CUDA kernels implement the same steps in the same order.             */
 /* ------------------------------------------------------------------------ */
-#define SVD_SWEEPS 4
+#define SVD_MAX_SWEEPS 6
 
-static inline void jacobi_rot(REAL *S, REAL *V, int p, int q)
+/* fused multiply-add with one rounding (the CUDA kernels use __fmaf_rn at the
+ * same places) */
+#if defined(ORACLE_F64)
+#define FMA(a, b, c) fma((a), (b), (c))
+#define JACOBI_TOL2 1e-32   /* converge to double precision */
+#else
+#define FMA(a, b, c) fmaf((a), (b), (c))
+#define JACOBI_TOL2 1e-16f  /* the CUDA kernels' threshold */
+#endif
+
+/* one Jacobi rotation zeroing S[p][q]; t = 2 a_pq sgn(d) / (|d| + sqrt(d^2 + 4 a_pq^2)),
+ * d = a_qq - a_pp, sgn(0) = +1; converged pair (a_pq^2 <= 1e-16 |a_pp a_qq|)
+ * is skipped.  Returns whether it rotated. */
+static inline int jacobi_rot(REAL *S, REAL *V, int p, int q)
 {
     /* S holds the symmetric matrix in full row-major form */
     REAL apq = S[3 * p + q];
-    if (apq == R(0)) return;
     REAL app = S[3 * p + p], aqq = S[3 * q + q];
-    REAL theta = (aqq - app) / (R(2) * apq);
-    REAL t = R(1) / (FABS(theta) + SQRT(theta * theta + R(1)));
-    if (theta < R(0)) t = -t;
-    REAL c = R(1) / SQRT(t * t + R(1));
+    if (apq * apq <= JACOBI_TOL2 * FABS(app * aqq)) return 0;
+    REAL d = aqq - app;
+    REAL two_apq = R(2) * apq;
+    REAL t = (d < R(0) ? -two_apq : two_apq) / (FABS(d) + SQRT(FMA(d, d, two_apq * two_apq)));
+    REAL c = R(1) / SQRT(FMA(t, t, R(1)));
     REAL s = t * c;
-    S[3 * p + p] = app - t * apq;
-    S[3 * q + q] = aqq + t * apq;
+    S[3 * p + p] = FMA(-t, apq, app);
+    S[3 * q + q] = FMA(t, apq, aqq);
     S[3 * p + q] = R(0);
     S[3 * q + p] = R(0);
     int r = 3 - p - q;
     REAL srp = S[3 * r + p], srq = S[3 * r + q];
-    REAL nrp = c * srp - s * srq;
-    REAL nrq = s * srp + c * srq;
+    REAL nrp = FMA(c, srp, -s * srq);
+    REAL nrq = FMA(s, srp, c * srq);
     S[3 * r + p] = nrp; S[3 * p + r] = nrp;
     S[3 * r + q] = nrq; S[3 * q + r] = nrq;
     for (int k = 0; k < 3; ++k) {
         REAL vkp = V[3 * k + p], vkq = V[3 * k + q];
-        V[3 * k + p] = c * vkp - s * vkq;
-        V[3 * k + q] = s * vkp + c * vkq;
+        V[3 * k + p] = FMA(c, vkp, -s * vkq);
+        V[3 * k + q] = FMA(s, vkp, c * vkq);
     }
+    return 1;
 }
 
 static inline void swap_cols(REAL *lam, REAL *V, int a, int b)
@@ -160,10 +174,11 @@ void orc_svd3(const REAL *F, REAL *U, REAL *sig, REAL *V)
         }
     for (int k = 0; k < 9; ++k) V[k] = R(0);
     V[0] = V[4] = V[8] = R(1);
-    for (int sw = 0; sw < SVD_SWEEPS; ++sw) {
-        jacobi_rot(S, V, 0, 1);
-        jacobi_rot(S, V, 0, 2);
-        jacobi_rot(S, V, 1, 2);
+    for (int sw = 0; sw < SVD_MAX_SWEEPS; ++sw) {
+        int r0 = jacobi_rot(S, V, 0, 1);
+        int r1 = jacobi_rot(S, V, 0, 2);
+        int r2 = jacobi_rot(S, V, 1, 2);
+        if (!(r0 || r1 || r2)) break;
     }
     REAL lam[3] = {S[0], S[4], S[8]};
     swap_cols(lam, V, 0, 1);

@@ -105,6 +105,21 @@ def gpu_fields(sim, mpm, xpbd):
                 particle_v_initial_xpbd=c(xpbd.particle_v_initial_xpbd))
 
 
+def stress_either_err(g, s32, s64, floor_frac=1e-4):
+    """Per-particle stress error of the AUTO stress mode: each particle must
+    match the FP32 oracle (SVD path, same operations) or the FP64 oracle (the
+    SVD-free elastic path, which is closer to FP64 than an FP32 SVD).  Returns
+    the largest min(err32, err64) / scale over particles, scale = max(|s64_p|,
+    floor_frac * max|s64|)."""
+    g = np.asarray(g, np.float64).reshape(len(g), -1)
+    a = np.asarray(s32, np.float64).reshape(len(g), -1)
+    b = np.asarray(s64, np.float64).reshape(len(g), -1)
+    scale = np.maximum(np.abs(b).max(1), floor_frac * np.abs(b).max())
+    scale = np.where(scale > 0, scale, 1.0)
+    e = np.minimum(np.abs(g - a).max(1), np.abs(g - b).max(1)) / scale
+    return float(e.max()) if e.size else 0.0
+
+
 ORACLES = {}
 
 

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as orc
-from tests.harness import gpu_fields, oracle, rel_err, small_scene, to_oracle
+from tests.harness import gpu_fields, oracle, rel_err, small_scene, stress_either_err, to_oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -24,18 +24,29 @@ def _torch():
     return torch
 
 
-def test_stress_kernel_matches_oracle():
+@pytest.mark.parametrize("mode", [1, 0])
+def test_stress_kernel_matches_oracle(mode):
+    """mode 1 (SVD for every particle) agrees with the FP32 oracle operation by
+    operation; mode 0 (default) sends clearly elastic particles through the
+    SVD-free log strain, whose stress matches the FP64 oracle instead."""
     torch = _torch()
     from mpmwarpydw_b200.utils import mpmRoutines as M
     sim, mpm, xpbd = small_scene(seed=1)
     o = oracle("f32")
     s = to_oracle(sim, mpm, xpbd)
+    s64 = to_oracle(sim, mpm, xpbd, np.float64)
     M.launch(M.compute_stress_from_F_trial, sim.nPoints, inputs=[
         sim.activeLabel, sim.materialLabel, sim.particle_x, sim.particle_v, xpbd.particle_x_initial_xpbd,
         xpbd.particle_v_initial_xpbd, mpm.particle_F, mpm.particle_F_trial, mpm.mu, mpm.lam, mpm.ys, mpm.hardening,
         mpm.softening, sim.particle_density, mpm.strainCriteria, mpm.eff, mpm.eta_shear, mpm.eta_bulk, mpm.particle_C,
-        mpm.particle_stress, mpm.particle_accumulated_strain, mpm.particle_damage, mpm.constitutive_model, mpm.alpha])
+        mpm.particle_stress, mpm.particle_accumulated_strain, mpm.particle_damage, mpm.constitutive_model, mpm.alpha,
+        mode])
     torch.cuda.synchronize()
+    oracle("f64").compute_stress_from_F_trial(
+        s64.activeLabel, s64.materialLabel, s64.particle_x, s64.particle_v, s64.particle_x_initial_xpbd,
+        s64.particle_v_initial_xpbd, s64.particle_F, s64.particle_F_trial, s64.mu, s64.lam, s64.ys, s64.hardening,
+        s64.softening, s64.particle_density, s64.strainCriteria, s64.eff, s64.eta_shear, s64.eta_bulk, s64.particle_C,
+        s64.particle_stress, s64.particle_accumulated_strain, s64.particle_damage, s64.constitutive_model, s64.alpha)
     o.compute_stress_from_F_trial(
         s.activeLabel, s.materialLabel, s.particle_x, s.particle_v, s.particle_x_initial_xpbd,
         s.particle_v_initial_xpbd, s.particle_F, s.particle_F_trial, s.mu, s.lam, s.ys, s.hardening, s.softening,
@@ -44,10 +55,21 @@ def test_stress_kernel_matches_oracle():
     g = gpu_fields(sim, mpm, xpbd)
     assert np.array_equal(g["materialLabel"], s.materialLabel)
     assert (s.materialLabel == 2).sum() > 0, "scene should contain phase transitions"
-    for k in ("particle_F", "particle_stress", "particle_accumulated_strain", "particle_damage", "ys", "mu", "lam",
+    for k in ("particle_F", "particle_accumulated_strain", "particle_damage", "ys", "mu", "lam",
               "alpha", "particle_v", "particle_x_initial_xpbd", "particle_v_initial_xpbd"):
         e = rel_err(g[k], getattr(s, k))
         assert e <= TOL, (k, e)
+    if mode == 1:
+        assert rel_err(g["particle_stress"], s.particle_stress) <= TOL
+    else:
+        e = stress_either_err(g["particle_stress"], s.particle_stress, s64.particle_stress)
+        assert e <= TOL, e
+        # the elastic particles' stress is within 1e-5 of FP64 (the FP32 SVD path is not)
+        el = (s.particle_accumulated_strain == 0) & (s.materialLabel <= 1)
+        e64 = rel_err(g["particle_stress"][el], s64.particle_stress[el])
+        e32 = rel_err(s.particle_stress[el], s64.particle_stress[el])
+        print(f"elastic stress vs FP64: GPU auto {e64:.2e}, FP32 SVD oracle {e32:.2e}")
+        assert e64 <= TOL
 
 
 def test_stress_fp32_vs_fp64_reported():
@@ -173,29 +195,38 @@ def test_g2p_matches_oracle():
                            s.particle_F, s.particle_F_trial, s.particle_cov, s.invdx, s.grid_v_out, True, s.minBounds)
     assert st == 0
     g = gpu_fields(sim, mpm, xpbd)
+    # the GPU gather is a tensor-product FMA reduction; the oracle sums the 27
+    # nodes in the reference's order: agreement to FP32 rounding
     for k in ("particle_x", "particle_v", "particle_C", "particle_F_trial", "particle_cov"):
-        assert np.array_equal(g[k], getattr(s, k)), (k, rel_err(g[k], getattr(s, k)))
+        assert rel_err(g[k], getattr(s, k)) <= 1e-6, (k, rel_err(g[k], getattr(s, k)))
 
 
-def _run_oracle_steps(s, nsteps, prec="f32"):
+def _run_oracle_steps(s, nsteps, prec="f32"):  # noqa: D103
     o = oracle(prec)
     for _ in range(nsteps):
         orc.mpm_step(o, s)
     return s
 
 
-@pytest.mark.parametrize("vlc", [0, 1])
-def test_one_substep_matches_oracle(vlc):
+@pytest.mark.parametrize("vlc,mode", [(0, 1), (1, 1), (0, 0), (1, 0)])
+def test_one_substep_matches_oracle(vlc, mode):
     torch = _torch()
     from mpmwarpydw_b200.utils import simulationRoutines as S
     sim, mpm, xpbd = small_scene(seed=7, volumetric_locking_correction=vlc, grid_v_damping_scale=0.99)
+    mpm.stress_mode = mode
     s = to_oracle(sim, mpm, xpbd)
+    s64 = to_oracle(sim, mpm, xpbd, np.float64)
     S.mpmSimulationStep(sim, mpm, xpbd, "cuda:0")
     torch.cuda.synchronize()
     _run_oracle_steps(s, 1)
+    _run_oracle_steps(s64, 1, "f64")
     g = gpu_fields(sim, mpm, xpbd)
     assert np.array_equal(g["materialLabel"], s.materialLabel)
-    for k in ("particle_stress", "particle_F", "particle_accumulated_strain", "particle_damage"):
+    if mode == 1:
+        assert rel_err(g["particle_stress"], s.particle_stress) <= TOL
+    else:
+        assert stress_either_err(g["particle_stress"], s.particle_stress, s64.particle_stress) <= TOL
+    for k in ("particle_F", "particle_accumulated_strain", "particle_damage"):
         assert rel_err(g[k], getattr(s, k)) <= TOL, k
     for k in ("grid_m", "grid_v_in", "grid_v_out", "particle_x", "particle_v", "particle_C", "particle_F_trial"):
         e = rel_err(g[k], getattr(s, k))
@@ -223,22 +254,28 @@ def test_fused_multistep_matches_unfused():
 
 
 def test_multistep_conservation_vs_oracle():
-    """20 steps of a gravity-driven block: mass, momentum and damaged fraction
-    agree with the oracle within 1e-3."""
+    """100 fused steps of a 4,096-particle Drucker-Prager block collapse (the
+    64k block-collapse scene at reduced size, cohesion lowered so it yields):
+    total mass, momentum and damaged fraction agree with the oracle's 100
+    reference-order steps within 1e-3."""
     torch = _torch()
+    from mpmwarpydw_b200 import domains
     from mpmwarpydw_b200.utils import simulationRoutines as S
-    sim, mpm, xpbd = small_scene(seed=9, plastic=False, labels=False)
+    d = domains.block_collapse(n_side=16, spacing=0.25, jitter=0.025, seed=0, box=4.0, dx=0.5, cohesion=2e4)
+    sim, mpm, xpbd = domains.build(d, device="cuda:0")
     s = to_oracle(sim, mpm, xpbd)
-    S.run_mpm_substeps(sim, mpm, xpbd, 20)
+    S.run_mpm_substeps(sim, mpm, xpbd, 100)
     torch.cuda.synchronize()
-    _run_oracle_steps(s, 20)
+    _run_oracle_steps(s, 100)
     g = gpu_fields(sim, mpm, xpbd)
     m = s.particle_mass.astype(np.float64)
     mom_g = (m[:, None] * g["particle_v"]).sum(0)
     mom_o = (m[:, None] * s.particle_v).sum(0)
-    assert np.max(np.abs(mom_g - mom_o)) <= 1e-3 * max(np.max(np.abs(mom_o)), 1e-12)
+    print("momentum gpu", mom_g, "oracle", mom_o)
+    assert np.max(np.abs(mom_g - mom_o)) <= 1e-3 * np.max(np.abs(mom_o))
     assert abs(g["grid_m"].sum() - s.grid_m.sum()) <= 1e-3 * s.grid_m.sum()
     dmg_g = float((g["particle_damage"] >= 1).mean()); dmg_o = float((s.particle_damage >= 1).mean())
+    print("damaged fraction gpu", dmg_g, "oracle", dmg_o, "plastic particles", int((s.particle_accumulated_strain > 0).sum()))
     assert abs(dmg_g - dmg_o) <= 1e-3
     assert rel_err(g["particle_x"], s.particle_x) <= 1e-5
 
@@ -247,7 +284,8 @@ def test_status_word_flags_out_of_grid():
     torch = _torch()
     from mpmwarpydw_b200.bind import read_status
     from mpmwarpydw_b200.utils import simulationRoutines as S
-    sim, mpm, xpbd = small_scene(seed=10, labels=False)
+    sim, mpm, xpbd = small_scene(seed=10, labels=False, plastic=False)
+    mpm.ys = torch.full_like(mpm.ys, 1e20)   # keep every particle elastic MPM
     read_status(sim.device)
     x = sim.particle_x.clone()
     x[0] = torch.tensor([1e4, 0.0, 0.0], device="cuda")  # far outside the grid
@@ -256,3 +294,4 @@ def test_status_word_flags_out_of_grid():
     torch.cuda.synchronize()
     st = read_status(sim.device)
     assert st & 1, st
+    assert read_status(sim.device) == 0
