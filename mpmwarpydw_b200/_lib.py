@@ -57,6 +57,27 @@ class Params(ctypes.Structure):
 STRESS_AUTO, STRESS_SVD = 0, 1
 
 
+class XPBD(ctypes.Structure):
+    _fields_ = [("x_int", _P), ("v_int", _P), ("x_dI", _P), ("v_dI", _P), ("delta", _P), ("v_before", _P),
+                ("cum_dist", _P), ("base_radius", _P), ("max_radius", _P), ("counts", _P)]
+
+
+class Hash(ctypes.Structure):
+    _fields_ = [("dims", _I32 * 3), ("cell_width", _F), ("point_ids", _P), ("cell_starts", _P),
+                ("cell_ends", _P), ("point_cells", _P)]
+
+
+class XPBDParams(ctypes.Structure):
+    _fields_ = [("gravity", _F * 3), ("dt", _F), ("v_max", _F), ("iterations", _I32), ("relaxation", _F),
+                ("coupling", _F), ("lock", _I32), ("dyn_friction", _F), ("static_friction", _F),
+                ("static_thr", _F), ("cohesion", _F), ("max_radius", _F), ("sleep_thr", _F),
+                ("bmin", _F * 3), ("bmax", _F * 3), ("swelling_ratio", _F), ("swell_act", _F),
+                ("swell_max", _F), ("xpbd_only", _I32)]
+
+
+XK = dict(INTEGRATE=0, RESET_LABELS=1, BOUND=2, PARTICLE=3, APPLY=4, SLEEP=5, IMPULSES=6, SWELL=7)
+
+
 _SIGS = {
     "mpmw_last_error": (ctypes.c_char_p, []),
     "mpmw_version": (_I, []),
@@ -76,6 +97,12 @@ _SIGS = {
     "mpmw_teleport": (_I, [ctypes.POINTER(Particles), _F, _F, _P]),
     "mpmw_creep": (_I, [ctypes.POINTER(Particles), _P, _F, _F, _F, _F, _P]),
     "mpmw_stats": (_I, [ctypes.POINTER(Particles), _P, _P]),
+    "mpmw_hash_workspace_bytes": (ctypes.c_size_t, [_I64]),
+    "mpmw_hash_build": (_I, [_P, _I64, ctypes.POINTER(Hash), _P, ctypes.c_size_t, _P]),
+    "mpmw_xpbd_kernel": (_I, [_I, ctypes.POINTER(Particles), ctypes.POINTER(XPBD), ctypes.POINTER(Hash),
+                              ctypes.POINTER(XPBDParams), _I, _P]),
+    "mpmw_xpbd_step": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(XPBD), ctypes.POINTER(Hash),
+                            ctypes.POINTER(XPBDParams), _P, ctypes.c_size_t, _P]),
 }
 
 _LIB = None

@@ -351,18 +351,22 @@ __global__ void k_particle_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash
     store3(X.delta, n, i, cur);
 }
 
-// xpbdRoutines.py:221-257 my_apply_particle_deltas, with the surrounding copies
-// (simulationRoutines.py:398-421) folded in: x_int/v_int are updated in place;
-// with write_tmp the deltaInt buffers receive the same values.
-__global__ void k_apply_deltas(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int write_tmp)
+// xpbdRoutines.py:221-257 my_apply_particle_deltas.  x_orig = particle x,
+// x_pred = x_int.  flag 0/1 (substep): the surrounding copies
+// (simulationRoutines.py:398-421) are folded in -- x_int/v_int are updated in
+// place, and with flag 1 the deltaInt buffers receive the same values for every
+// particle.  flag 2 (the kernel alone): results go to x_dI/v_dI for active
+// particles only, x_int/v_int are left untouched.
+__global__ void k_apply_deltas(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int flag)
 {
     const int64_t n = P.n;
     int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     float xn[3], vn[3];
     load3(X.x_int, n, p, xn);
-    load3(X.v_int, n, p, vn);
-    if (P.active[p] == 1) {
+    if (flag != 2) load3(X.v_int, n, p, vn);
+    const bool act = P.active[p] == 1;
+    if (act) {
         float d[3];
         load3(X.delta, n, p, d);
         if (isnan(d[0]) || isnan(d[1]) || isnan(d[2])) d[0] = d[1] = d[2] = 0.f;
@@ -372,10 +376,12 @@ __global__ void k_apply_deltas(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_para
         for (int a = 0; a < 3; ++a) { xn[a] = xn[a] + d[a]; vn[a] = (xn[a] - x0[a]) / q.dt; }
         float m = len3(vn);
         if (m > q.v_max) { float s = q.v_max / m; vn[0] = vn[0] * s; vn[1] = vn[1] * s; vn[2] = vn[2] * s; }
-        store3(X.x_int, n, p, xn);
-        store3(X.v_int, n, p, vn);
+        if (flag != 2) {
+            store3(X.x_int, n, p, xn);
+            store3(X.v_int, n, p, vn);
+        }
     }
-    if (write_tmp) {
+    if (flag == 1 || (flag == 2 && act)) {
         store3(X.x_dI, n, p, xn);
         store3(X.v_dI, n, p, vn);
     }
@@ -408,9 +414,11 @@ __global__ void k_sleep(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q)
     }
 }
 
-// simulationRoutines.py:444-470: v_before_contact <- v, apply_mpm_contact_impulses
-// (xpbdRoutines.py:259-310), then commit x <- x_int, v <- v_int
-__global__ void k_impulses_commit(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q)
+// apply_mpm_contact_impulses (xpbdRoutines.py:259-310): x_orig/v_orig = particle
+// x/v, x_final = x_int, v_out = v_int.  With commit (the substep,
+// simulationRoutines.py:444-470) v_before_contact <- v first and x <- x_int,
+// v <- v_int after.
+__global__ void k_impulses_commit(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int commit)
 {
     const int64_t n = P.n;
     int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -420,7 +428,8 @@ __global__ void k_impulses_commit(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_p
     load3(P.v, n, p, v0);
     load3(X.x_int, n, p, xf);
     load3(X.v_int, n, p, vf);
-    if (X.v_before) store3(X.v_before, n, p, v0);
+    if (commit && X.v_before) store3(X.v_before, n, p, v0);
+    if (!commit && !(P.active[p] == 1 && P.material[p] <= 1)) return;
     if (P.active[p] == 1 && P.material[p] <= 1) {
         xf[0] = x0[0]; xf[1] = x0[1]; xf[2] = x0[2];
         if (q.xpbd_only == 0) {
@@ -432,10 +441,12 @@ __global__ void k_impulses_commit(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_p
             vf[0] = vc[0]; vf[1] = vc[1]; vf[2] = vc[2];
         }
         store3(X.x_int, n, p, xf);
-        store3(X.v_int, n, p, vf);
+        if (q.xpbd_only == 0) store3(X.v_int, n, p, vf);
     }
-    store3(P.x, n, p, xf);
-    store3(P.v, n, p, vf);
+    if (commit) {
+        store3(P.x, n, p, xf);
+        store3(P.v, n, p, vf);
+    }
 }
 
 // xpbdRoutines.py:354-375 swellParticlesType2
@@ -529,7 +540,7 @@ int mpmw_xpbd_kernel(int which, const mpmw_particles_t *p, const mpmw_xpbd_t *x,
         if (!x->cum_dist) { set_error("sleep: cum_dist is required"); return MPMW_E_ARG; }
         k_sleep<<<g, kBlock, 0, s>>>(*p, *x, *q);
         break;
-    case MPMW_XK_IMPULSES: k_impulses_commit<<<g, kBlock, 0, s>>>(*p, *x, *q); break;
+    case MPMW_XK_IMPULSES: k_impulses_commit<<<g, kBlock, 0, s>>>(*p, *x, *q, flag); break;
     case MPMW_XK_SWELL:
         if (!x->base_radius || !x->max_radius || !p->x_pc) { set_error("swell: radii and x_pc are required"); return MPMW_E_ARG; }
         k_swell<<<g, kBlock, 0, s>>>(*p, *x, *q);
@@ -557,7 +568,7 @@ int mpmw_xpbd_step(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_h
         TRY(mpmw_xpbd_kernel(MPMW_XK_APPLY, p, x, h, &qi, it == q->iterations - 1, stream));
     }
     TRY(mpmw_xpbd_kernel(MPMW_XK_SLEEP, p, x, h, q, 1, stream));
-    TRY(mpmw_xpbd_kernel(MPMW_XK_IMPULSES, p, x, h, q, 0, stream));
+    TRY(mpmw_xpbd_kernel(MPMW_XK_IMPULSES, p, x, h, q, 1, stream));
     if (q->swelling_ratio > 0.f) TRY(mpmw_xpbd_kernel(MPMW_XK_SWELL, p, x, h, q, 0, stream));
     (void)s;
     return MPMW_OK;

@@ -1,18 +1,27 @@
-"""GPU parity of the MPM substep kernels against the CPU oracle (FP32 build,
-same operation order) on identical seeded inputs, through the C ABI.
+"""GPU parity of the MPM substep kernels against the CPU oracle on identical
+seeded inputs, through the C ABI.
 
-Tolerances (max-abs error relative to the array's max-abs value):
-  * kernels with no floating-point atomics (stress, grid update, G2P):
-    1e-5 -- they agree to the last bit except where logf/expf differ by an ulp;
-  * P2G and anything downstream of it in the same step: 1e-5 (atomic reordering);
-  * FP64 oracle distance is reported, not asserted, for the FP32 stress (it is
-    the FP32 storage floor of F near identity, common to any FP32 implementation).
+Rules (max-abs error; "array-relative" = relative to the array's max-abs):
+  * grid update: bit-identical to the FP32 oracle (same operations);
+  * G2P: array-relative 1e-6 (tensor-product FMA gather vs the reference's
+    27-term sums);
+  * P2G and everything downstream of it in a step: array-relative 1e-5
+    (floating-point atomics reorder the sums);
+  * stress, per particle (tests.harness.stress_parity_violation): either within
+    1e-5 |tau| + 1 Pa of the FP64 oracle (the default tensor-form return map
+    for |F F^T - I| <= 0.02) or within 1e-5 |tau| + 16 * 2mu * 2^-23 of the FP32
+    oracle (the SVD path, same operations as the oracle; the second term is the
+    stress worth of a few ulps of F near identity, where logf/expf ulp
+    differences land);
+  * accumulated strain, damage, F, labels: per particle equal to the FP32 or the
+    FP64 oracle within 1e-4 relative.
 """
 import numpy as np
 import pytest
 
 from oracle import oracle as orc
-from tests.harness import gpu_fields, oracle, rel_err, small_scene, stress_either_err, to_oracle
+from tests.harness import (close_to_either, gpu_fields, oracle, rel_err, small_scene, stress_parity_violation,
+                           to_oracle)
 
 pytestmark = pytest.mark.gpu
 
@@ -24,17 +33,42 @@ def _torch():
     return torch
 
 
+def _oracle_stress(o, s):
+    o.compute_stress_from_F_trial(
+        s.activeLabel, s.materialLabel, s.particle_x, s.particle_v, s.particle_x_initial_xpbd,
+        s.particle_v_initial_xpbd, s.particle_F, s.particle_F_trial, s.mu, s.lam, s.ys, s.hardening, s.softening,
+        s.particle_density, s.strainCriteria, s.eff, s.eta_shear, s.eta_bulk, s.particle_C, s.particle_stress,
+        s.particle_accumulated_strain, s.particle_damage, s.constitutive_model, s.alpha)
+
+
+def _check_stress_outputs(g, s32, s64, mode, mu0):
+    """Per-particle checks of the stress phase's outputs (see module docstring)."""
+    twomu = 2.0 * mu0.astype(np.float64)
+    if mode == 1:
+        assert np.array_equal(g["materialLabel"], s32.materialLabel)
+        assert stress_parity_violation(g["particle_stress"], s32.particle_stress, s32.particle_stress, twomu) <= 1.0
+    else:
+        lab_ok = (g["materialLabel"] == s32.materialLabel) | (g["materialLabel"] == s64.materialLabel)
+        assert lab_ok.all()
+        v = stress_parity_violation(g["particle_stress"], s32.particle_stress, s64.particle_stress, twomu)
+        assert v <= 1.0, v
+    for k in ("particle_accumulated_strain", "particle_damage", "ys"):
+        ok, bad = close_to_either(g[k], getattr(s32, k), getattr(s64, k), rtol=1e-4, atol=1e-7 if k != "ys" else 1.0)
+        assert ok, (k, bad)
+    ok, bad = close_to_either(g["particle_F"], s32.particle_F, s64.particle_F, rtol=0, atol=2e-6)
+    assert ok, ("F", bad)
+
+
 @pytest.mark.parametrize("mode", [1, 0])
 def test_stress_kernel_matches_oracle(mode):
-    """mode 1 (SVD for every particle) agrees with the FP32 oracle operation by
-    operation; mode 0 (default) sends clearly elastic particles through the
-    SVD-free log strain, whose stress matches the FP64 oracle instead."""
+    """mode 1: SVD return map for every particle (FP32-oracle operations);
+    mode 0 (default): tensor-form return map for small strains, SVD beyond."""
     torch = _torch()
     from mpmwarpydw_b200.utils import mpmRoutines as M
     sim, mpm, xpbd = small_scene(seed=1)
-    o = oracle("f32")
-    s = to_oracle(sim, mpm, xpbd)
+    s32 = to_oracle(sim, mpm, xpbd)
     s64 = to_oracle(sim, mpm, xpbd, np.float64)
+    mu0 = s32.mu.copy()
     M.launch(M.compute_stress_from_F_trial, sim.nPoints, inputs=[
         sim.activeLabel, sim.materialLabel, sim.particle_x, sim.particle_v, xpbd.particle_x_initial_xpbd,
         xpbd.particle_v_initial_xpbd, mpm.particle_F, mpm.particle_F_trial, mpm.mu, mpm.lam, mpm.ys, mpm.hardening,
@@ -42,58 +76,23 @@ def test_stress_kernel_matches_oracle(mode):
         mpm.particle_stress, mpm.particle_accumulated_strain, mpm.particle_damage, mpm.constitutive_model, mpm.alpha,
         mode])
     torch.cuda.synchronize()
-    oracle("f64").compute_stress_from_F_trial(
-        s64.activeLabel, s64.materialLabel, s64.particle_x, s64.particle_v, s64.particle_x_initial_xpbd,
-        s64.particle_v_initial_xpbd, s64.particle_F, s64.particle_F_trial, s64.mu, s64.lam, s64.ys, s64.hardening,
-        s64.softening, s64.particle_density, s64.strainCriteria, s64.eff, s64.eta_shear, s64.eta_bulk, s64.particle_C,
-        s64.particle_stress, s64.particle_accumulated_strain, s64.particle_damage, s64.constitutive_model, s64.alpha)
-    o.compute_stress_from_F_trial(
-        s.activeLabel, s.materialLabel, s.particle_x, s.particle_v, s.particle_x_initial_xpbd,
-        s.particle_v_initial_xpbd, s.particle_F, s.particle_F_trial, s.mu, s.lam, s.ys, s.hardening, s.softening,
-        s.particle_density, s.strainCriteria, s.eff, s.eta_shear, s.eta_bulk, s.particle_C, s.particle_stress,
-        s.particle_accumulated_strain, s.particle_damage, s.constitutive_model, s.alpha)
+    _oracle_stress(oracle("f32"), s32)
+    _oracle_stress(oracle("f64"), s64)
     g = gpu_fields(sim, mpm, xpbd)
-    assert np.array_equal(g["materialLabel"], s.materialLabel)
-    assert (s.materialLabel == 2).sum() > 0, "scene should contain phase transitions"
-    for k in ("particle_F", "particle_accumulated_strain", "particle_damage", "ys", "mu", "lam",
-              "alpha", "particle_v", "particle_x_initial_xpbd", "particle_v_initial_xpbd"):
-        e = rel_err(g[k], getattr(s, k))
-        assert e <= TOL, (k, e)
-    if mode == 1:
-        assert rel_err(g["particle_stress"], s.particle_stress) <= TOL
-    else:
-        e = stress_either_err(g["particle_stress"], s.particle_stress, s64.particle_stress)
-        assert e <= TOL, e
-        # the elastic particles' stress is within 1e-5 of FP64 (the FP32 SVD path is not)
-        el = (s.particle_accumulated_strain == 0) & (s.materialLabel <= 1)
-        e64 = rel_err(g["particle_stress"][el], s64.particle_stress[el])
-        e32 = rel_err(s.particle_stress[el], s64.particle_stress[el])
-        print(f"elastic stress vs FP64: GPU auto {e64:.2e}, FP32 SVD oracle {e32:.2e}")
-        assert e64 <= TOL
-
-
-def test_stress_fp32_vs_fp64_reported():
-    torch = _torch()
-    from mpmwarpydw_b200.utils import mpmRoutines as M
-    sim, mpm, xpbd = small_scene(seed=2, labels=False)
-    s64 = to_oracle(sim, mpm, xpbd, np.float64)
-    M.compute_stress_from_F_trial(
-        sim.activeLabel, sim.materialLabel, sim.particle_x, sim.particle_v, xpbd.particle_x_initial_xpbd,
-        xpbd.particle_v_initial_xpbd, mpm.particle_F, mpm.particle_F_trial, mpm.mu, mpm.lam, mpm.ys, mpm.hardening,
-        mpm.softening, sim.particle_density, mpm.strainCriteria, mpm.eff, mpm.eta_shear, mpm.eta_bulk, mpm.particle_C,
-        mpm.particle_stress, mpm.particle_accumulated_strain, mpm.particle_damage, mpm.constitutive_model, mpm.alpha)
-    torch.cuda.synchronize()
-    oracle("f64").compute_stress_from_F_trial(
-        s64.activeLabel, s64.materialLabel, s64.particle_x, s64.particle_v, s64.particle_x_initial_xpbd,
-        s64.particle_v_initial_xpbd, s64.particle_F, s64.particle_F_trial, s64.mu, s64.lam, s64.ys, s64.hardening,
-        s64.softening, s64.particle_density, s64.strainCriteria, s64.eff, s64.eta_shear, s64.eta_bulk, s64.particle_C,
-        s64.particle_stress, s64.particle_accumulated_strain, s64.particle_damage, s64.constitutive_model, s64.alpha)
-    g = gpu_fields(sim, mpm, xpbd)
-    # elastic particles only: the branch decision itself is precision-sensitive near the yield surface
-    same = (g["materialLabel"] == s64.materialLabel)
-    e = rel_err(g["particle_stress"][same], s64.particle_stress[same])
-    print(f"FP32 GPU stress vs FP64 oracle (strains ~2e-3): {e:.3e}")
-    assert e < 1e-2
+    assert (s32.materialLabel == 2).sum() > 0, "scene should contain phase transitions"
+    assert (s32.particle_accumulated_strain > 0).sum() > 100, "scene should contain plastic particles"
+    _check_stress_outputs(g, s32, s64, mode, mu0)
+    for k in ("mu", "lam", "alpha", "particle_v", "particle_x_initial_xpbd", "particle_v_initial_xpbd"):
+        assert rel_err(g[k], getattr(s32, k)) <= 1e-5, k
+    if mode == 0:
+        # small-strain particles: the GPU is within 1e-5 of FP64 per particle; report the FP32 oracle's distance
+        G = g["particle_stress"].reshape(-1, 9).astype(np.float64)
+        A = s32.particle_stress.reshape(-1, 9).astype(np.float64)
+        B = s64.particle_stress.reshape(-1, 9)
+        sc = np.abs(B).max(1) + 1.0
+        sel = s32.materialLabel <= 1
+        print(f"per-particle stress error vs FP64: GPU auto {np.max(np.abs(G - B).max(1)[sel] / sc[sel]):.2e}, "
+              f"FP32 SVD oracle {np.max(np.abs(A - B).max(1)[sel] / sc[sel]):.2e}")
 
 
 def test_p2g_matches_oracle():
@@ -216,21 +215,22 @@ def test_one_substep_matches_oracle(vlc, mode):
     mpm.stress_mode = mode
     s = to_oracle(sim, mpm, xpbd)
     s64 = to_oracle(sim, mpm, xpbd, np.float64)
+    mu0 = s.mu.copy()
     S.mpmSimulationStep(sim, mpm, xpbd, "cuda:0")
     torch.cuda.synchronize()
     _run_oracle_steps(s, 1)
     _run_oracle_steps(s64, 1, "f64")
     g = gpu_fields(sim, mpm, xpbd)
-    assert np.array_equal(g["materialLabel"], s.materialLabel)
+    _check_stress_outputs(g, s, s64, mode, mu0)
     if mode == 1:
-        assert rel_err(g["particle_stress"], s.particle_stress) <= TOL
+        for k in ("grid_m", "grid_v_in", "grid_v_out", "particle_x", "particle_v", "particle_C", "particle_F_trial"):
+            e = rel_err(g[k], getattr(s, k))
+            assert e <= TOL, (k, e)
     else:
-        assert stress_either_err(g["particle_stress"], s.particle_stress, s64.particle_stress) <= TOL
-    for k in ("particle_F", "particle_accumulated_strain", "particle_damage"):
-        assert rel_err(g[k], getattr(s, k)) <= TOL, k
-    for k in ("grid_m", "grid_v_in", "grid_v_out", "particle_x", "particle_v", "particle_C", "particle_F_trial"):
-        e = rel_err(g[k], getattr(s, k))
-        assert e <= TOL, (k, e)
+        # the grid and the G2P outputs depend on the stress: compare with the FP64 step
+        for k in ("grid_m", "grid_v_in", "grid_v_out", "particle_x", "particle_v", "particle_C", "particle_F_trial"):
+            e = min(rel_err(g[k], getattr(s, k)), rel_err(g[k], getattr(s64, k)))
+            assert e <= TOL, (k, e)
 
 
 def test_fused_multistep_matches_unfused():
@@ -255,29 +255,33 @@ def test_fused_multistep_matches_unfused():
 
 def test_multistep_conservation_vs_oracle():
     """100 fused steps of a 4,096-particle Drucker-Prager block collapse (the
-    64k block-collapse scene at reduced size, cohesion lowered so it yields):
-    total mass, momentum and damaged fraction agree with the oracle's 100
-    reference-order steps within 1e-3."""
+    64k block-collapse scene at reduced size; cohesion 0.1 MPa so that it
+    yields): total mass, momentum and damaged fraction agree with the FP64
+    oracle's 100 reference-order steps within 1e-3.  The FP32 oracle's own
+    distance from FP64 is printed for comparison."""
     torch = _torch()
     from mpmwarpydw_b200 import domains
     from mpmwarpydw_b200.utils import simulationRoutines as S
-    d = domains.block_collapse(n_side=16, spacing=0.25, jitter=0.025, seed=0, box=4.0, dx=0.5, cohesion=2e4)
+    d = domains.block_collapse(n_side=16, spacing=0.25, jitter=0.025, seed=0, box=4.0, dx=0.5, cohesion=1e5)
     sim, mpm, xpbd = domains.build(d, device="cuda:0")
-    s = to_oracle(sim, mpm, xpbd)
+    s32 = to_oracle(sim, mpm, xpbd)
+    s64 = to_oracle(sim, mpm, xpbd, np.float64)
     S.run_mpm_substeps(sim, mpm, xpbd, 100)
     torch.cuda.synchronize()
-    _run_oracle_steps(s, 100)
+    _run_oracle_steps(s32, 100)
+    _run_oracle_steps(s64, 100, "f64")
     g = gpu_fields(sim, mpm, xpbd)
-    m = s.particle_mass.astype(np.float64)
-    mom_g = (m[:, None] * g["particle_v"]).sum(0)
-    mom_o = (m[:, None] * s.particle_v).sum(0)
-    print("momentum gpu", mom_g, "oracle", mom_o)
-    assert np.max(np.abs(mom_g - mom_o)) <= 1e-3 * np.max(np.abs(mom_o))
-    assert abs(g["grid_m"].sum() - s.grid_m.sum()) <= 1e-3 * s.grid_m.sum()
-    dmg_g = float((g["particle_damage"] >= 1).mean()); dmg_o = float((s.particle_damage >= 1).mean())
-    print("damaged fraction gpu", dmg_g, "oracle", dmg_o, "plastic particles", int((s.particle_accumulated_strain > 0).sum()))
-    assert abs(dmg_g - dmg_o) <= 1e-3
-    assert rel_err(g["particle_x"], s.particle_x) <= 1e-5
+    m = s64.particle_mass
+    mom = lambda v: (m[:, None] * np.asarray(v, np.float64)).sum(0)  # noqa: E731
+    mg, m32, m64 = mom(g["particle_v"]), mom(s32.particle_v), mom(s64.particle_v)
+    scale = np.max(np.abs(m64))
+    print(f"momentum rel. to FP64: GPU {np.max(np.abs(mg - m64)) / scale:.2e}, FP32 oracle {np.max(np.abs(m32 - m64)) / scale:.2e}")
+    assert np.max(np.abs(mg - m64)) <= 1e-3 * scale
+    assert abs(g["grid_m"].sum() - s64.grid_m.sum()) <= 1e-3 * s64.grid_m.sum()
+    dg = float((g["particle_damage"] >= 1).mean()); d64 = float((s64.particle_damage >= 1).mean())
+    print("damaged fraction gpu", dg, "fp64", d64, "plastic", int((s64.particle_accumulated_strain > 0).sum()))
+    assert abs(dg - d64) <= 1e-3
+    assert rel_err(g["particle_x"], s64.particle_x) <= 1e-5
 
 
 def test_status_word_flags_out_of_grid():
