@@ -127,7 +127,7 @@ def run_ours(a):
 
     from mpmwarpydw_b200 import _lib
     from mpmwarpydw_b200.bind import (grid_from_state, params_from_states, particles_from_states, read_status,
-                                      status_word)
+                                      status_word, workspace)
     from mpmwarpydw_b200.utils import simulationRoutines as S
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -148,7 +148,7 @@ def run_ours(a):
     st = status_word(dev).data_ptr()
     stream = torch.cuda.current_stream(dev)
     sh = int(stream.cuda_stream)
-    mv_bytes = G * 16
+    ws = workspace(mpm, N, dev)
 
     def chk(rc, what):
         _lib.check(rc, what)
@@ -166,7 +166,7 @@ def run_ours(a):
         chk(L.mpmw_grid_update(Gs, prm, sh), "grid")
         if ev is not None:
             ev[3].record(stream)
-        chk(L.mpmw_g2p_stress(P, Gs, prm, st, sh), "g2p_stress")
+        chk(L.mpmw_g2p_stress(P, Gs, prm, st, ws.data_ptr(), ws.numel(), sh), "g2p_stress")
         if ev is not None:
             ev[4].record(stream)
 

@@ -93,13 +93,14 @@ typedef struct mpmw_params {
     int32_t stress_mode;         /* MPMW_STRESS_* */
 } mpmw_params_t;
 
-/* stress_mode: how the return map's trial state is decomposed.
- *   MPMW_STRESS_AUTO (0): particles that are clearly elastic (|F F^T - I|_F <= 0.02
- *     and sigma_eq below the yield surface by a 1 % + 16-ulp margin) take the
- *     log strain from ln(I + X), X = G + G^T + G G^T, G = F - I (4-term series);
- *     this equals the reference's U diag(2 mu ln s + lam sum ln s) U^T Kirchhoff
- *     stress and is more accurate in FP32 than an SVD of F near identity.  All
- *     other particles take the SVD path below.
+/* stress_mode: how the return map is evaluated (same model either way).
+ *   MPMW_STRESS_AUTO (0): when |F F^T - I|_F <= 0.02 the return map runs in
+ *     tensor form on the spatial log strain eps = 1/2 ln(I + X),
+ *     X = G + G^T + G G^T, G = F - I (series): invariants for the yield test,
+ *     radial return on dev(eps), F_e = e^vc exp(-f dev eps) F, Kirchhoff stress
+ *     2 mu eps + lam tr(eps) I.  This is the reference's principal-space algebra
+ *     without an SVD, and it avoids FP32 rounding of ln(s) for s near 1.  Larger
+ *     deformations take the SVD path.
  *   MPMW_STRESS_SVD (1): every particle takes the SVD path (svd3 of F_trial,
  *     principal log strains, radial return, second svd3 for the Kirchhoff
  *     stress), operation for operation as the CPU oracle. */
@@ -147,7 +148,10 @@ int mpmw_g2p(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_
  * F (returned) and stress instead of F_trial.  Equivalent to mpmw_g2p followed
  * by mpmw_stress when nothing runs between them (no VLC, no XPBD). */
 int mpmw_g2p_stress(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm,
-                    uint32_t *status, mpmw_stream_t stream);
+                    uint32_t *status, void *workspace, size_t ws_bytes, mpmw_stream_t stream);
+/* Bytes of device workspace mpmw_g2p_stress / mpmw_run_substeps need for n
+ * particles (a worklist of the particles whose return map takes the SVD path). */
+size_t mpmw_workspace_bytes(int64_t n);
 /* utils/mpmRoutines.py:817-911 accumulate_cell_divergence + apply_volumetric_locking_correction
  * (zeroes grid->cell_div / cell_vol itself, utils/simulationRoutines.py:255-293) */
 int mpmw_vlc(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
@@ -164,10 +168,11 @@ int mpmw_substep(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_par
                  mpmw_stream_t stream);
 /* nsteps consecutive mpmSimulationStep calls with no XPBD between them
  * (runMPMYDW.py:666-682 for steps where counter % mpmStepsPerXpbdStep != 0).
- * Same result as nsteps x mpmw_substep; internally the return map of step k+1
- * runs fused into the G2P of step k when VLC is off. */
+ * Same result as nsteps x mpmw_substep; when VLC is off and a workspace of
+ * mpmw_workspace_bytes(n) is given, the return map of step k+1 runs fused into
+ * the G2P of step k. */
 int mpmw_run_substeps(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, int nsteps,
-                      uint32_t *status, mpmw_stream_t stream);
+                      uint32_t *status, void *workspace, size_t ws_bytes, mpmw_stream_t stream);
 
 /* utils/mpmRoutines.py:1446-1475 deactivate_and_teleport_xpbd_below_datum */
 int mpmw_teleport(const mpmw_particles_t *p, float z_datum, float teleport_distance, mpmw_stream_t stream);

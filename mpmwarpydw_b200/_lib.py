@@ -88,12 +88,14 @@ _SIGS = {
     "mpmw_grid_update": (_I, [ctypes.POINTER(Grid), ctypes.POINTER(Params), _P]),
     "mpmw_grid_op": (_I, [ctypes.POINTER(Grid), ctypes.POINTER(Params), _I, _P]),
     "mpmw_g2p": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _P, _P]),
-    "mpmw_g2p_stress": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _P, _P]),
+    "mpmw_g2p_stress": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _P, _P,
+                             ctypes.c_size_t, _P]),
+    "mpmw_workspace_bytes": (ctypes.c_size_t, [_I64]),
     "mpmw_vlc": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _P, _P]),
     "mpmw_vlc_phase": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _I, _P, _P]),
     "mpmw_substep": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _P, _P]),
     "mpmw_run_substeps": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _I, _P,
-                               _P]),
+                               _P, ctypes.c_size_t, _P]),
     "mpmw_teleport": (_I, [ctypes.POINTER(Particles), _F, _F, _P]),
     "mpmw_creep": (_I, [ctypes.POINTER(Particles), _P, _F, _F, _F, _F, _P]),
     "mpmw_stats": (_I, [ctypes.POINTER(Particles), _P, _P]),

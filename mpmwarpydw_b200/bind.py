@@ -241,3 +241,13 @@ def params_from_states(sim, mpm) -> _lib.Params:
 
 def byref(x):
     return ctypes.byref(x)
+
+
+def workspace(owner, n: int, device) -> torch.Tensor:
+    """Device workspace for the fused substep (mpmw_workspace_bytes(n)), cached on ``owner``."""
+    need = int(_lib.lib().mpmw_workspace_bytes(int(n)))
+    ws = getattr(owner, "_mpmw_ws", None)
+    if ws is None or ws.numel() < need:
+        ws = torch.empty(max(need, 256), dtype=torch.uint8, device=device)
+        owner._mpmw_ws = ws
+    return ws

@@ -55,7 +55,7 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> str:
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-I", INCLUDE, "-o", tmp, *sources(), "-lcuda"]
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-I", INCLUDE, "-o", tmp, *sources()]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -10,6 +10,7 @@ namespace mpmw {
 int launch_stress(const mpmw_particles_t &p, const mpmw_params_t &prm, cudaStream_t s);
 int launch_p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, cudaStream_t s);
 int launch_g2p(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, bool fused,
-               cudaStream_t s);
+               void *ws, size_t ws_bytes, cudaStream_t s);
+size_t g2p_workspace_bytes(int64_t n);
 
 }  // namespace mpmw

@@ -495,17 +495,19 @@ int mpmw_g2p(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_
     MPMW_TRY(check_params(prm));
     if (p->n > 0 && !p->F_trial) { set_error("g2p: F_trial is required"); return MPMW_E_ARG; }
     if (prm->update_cov && p->n > 0 && !p->cov) { set_error("g2p: update_cov needs cov"); return MPMW_E_ARG; }
-    return launch_g2p(*p, *g, *prm, status, false, as_stream(stream));
+    return launch_g2p(*p, *g, *prm, status, false, nullptr, 0, as_stream(stream));
 }
 
+size_t mpmw_workspace_bytes(int64_t n) { return mpmw::g2p_workspace_bytes(n < 0 ? 0 : n); }
+
 int mpmw_g2p_stress(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
-                    mpmw_stream_t stream)
+                    void *workspace, size_t ws_bytes, mpmw_stream_t stream)
 {
     MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV | kNeedCF | kNeedStress));
     MPMW_TRY(check_grid(g));
     MPMW_TRY(check_params(prm));
     if (prm->update_cov && p->n > 0 && !p->cov) { set_error("g2p: update_cov needs cov"); return MPMW_E_ARG; }
-    return launch_g2p(*p, *g, *prm, status, true, as_stream(stream));
+    return launch_g2p(*p, *g, *prm, status, true, workspace, ws_bytes, as_stream(stream));
 }
 
 int mpmw_vlc(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
@@ -539,11 +541,11 @@ int mpmw_vlc_phase(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_p
 int mpmw_substep(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
                  mpmw_stream_t stream)
 {
-    return mpmw_run_substeps(p, g, prm, 1, status, stream);
+    return mpmw_run_substeps(p, g, prm, 1, status, nullptr, 0, stream);
 }
 
 int mpmw_run_substeps(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, int nsteps,
-                      uint32_t *status, mpmw_stream_t stream)
+                      uint32_t *status, void *workspace, size_t ws_bytes, mpmw_stream_t stream)
 {
     MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV | kNeedCF | kNeedStress));
     MPMW_TRY(check_grid(g));
@@ -560,11 +562,11 @@ int mpmw_run_substeps(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpm
         MPMW_TRY(launch_p2g(*p, *g, *prm, status, s));
         MPMW_TRY(launch_grid(*g, *prm, s));
         bool last = step == nsteps - 1;
-        if (!last && !prm->vlc) {
-            MPMW_TRY(launch_g2p(*p, *g, *prm, status, true, s));
+        if (!last && !prm->vlc && workspace) {
+            MPMW_TRY(launch_g2p(*p, *g, *prm, status, true, workspace, ws_bytes, s));
             need_stress = false;
         } else {
-            MPMW_TRY(launch_g2p(*p, *g, *prm, status, false, s));
+            MPMW_TRY(launch_g2p(*p, *g, *prm, status, false, nullptr, 0, s));
             if (prm->vlc) MPMW_TRY(launch_vlc(*p, *g, *prm, status, s));
             need_stress = true;
         }

@@ -8,7 +8,8 @@
 //    svd3 of F_trial, principal log strains, radial return, F_e = U exp(eps) V^T,
 //    second svd3 of F_e for the Kirchhoff stress -- operation for operation as
 //    the CPU oracle.
-//  * tensor path (small_strain_update, MPMW_STRESS_AUTO when |F F^T - I|_F <= 0.02):
+//  * tensor path (small_strain_update, MPMW_STRESS_AUTO when |F F^T - I|_F <= 0.02
+//    and det F > 0):
 //    the model is isotropic and the return is radial, so every quantity the
 //    reference takes from principal values is an invariant of the spatial log
 //    strain eps = 1/2 ln(F F^T):
@@ -120,6 +121,14 @@ __device__ __forceinline__ bool small_strain_update(const mpmw_particles_t &P, f
         }
     }
     if (!(sym_ddot(X, X) <= 4e-4f)) return false;
+    // F F^T near I also holds for a reflection (det F ~ -1); the reference's
+    // SVD then has a negative singular value, clamped to 0.01, so a reflected
+    // F must take the SVD path.  With F F^T near I, det F is near +-1.
+    {
+        const float det = Ft[0] * (Ft[4] * Ft[8] - Ft[5] * Ft[7]) - Ft[1] * (Ft[3] * Ft[8] - Ft[5] * Ft[6]) +
+                          Ft[2] * (Ft[3] * Ft[7] - Ft[4] * Ft[6]);
+        if (!(det > 0.f)) return false;
+    }
     // eps = 1/2 ln(I + X) = 1/2 X (I + X (-1/2 I + X (1/3 I - 1/4 X)))
     float eps[6];
     {

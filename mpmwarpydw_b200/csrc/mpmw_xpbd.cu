@@ -558,7 +558,8 @@ int mpmw_xpbd_step(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_h
     if (p->n == 0) return MPMW_OK;
     cudaStream_t s = as_stream(stream);
     TRY(mpmw_hash_build(p->x, p->n, h, workspace, ws_bytes, stream));
-    TRY(mpmw_xpbd_kernel(MPMW_XK_INTEGRATE, p, x, h, q, 1, stream));
+    // x_int <- x, v_int <- v for every particle (simulationRoutines.py:314-315), then integrate
+    TRY(mpmw_xpbd_kernel(MPMW_XK_INTEGRATE, p, x, h, q, 3, stream));
     if (q->lock && !q->xpbd_only) TRY(mpmw_xpbd_kernel(MPMW_XK_RESET_LABELS, p, x, h, q, 0, stream));
     mpmw_xpbd_params_t qi = *q;
     if (q->xpbd_only) qi.lock = 0;

@@ -16,7 +16,7 @@ from __future__ import annotations
 import torch
 
 from . import _lib
-from .bind import grid_from_state, params_from_states, particles_from_states, status_word, stream_handle
+from .bind import grid_from_state, params_from_states, particles_from_states, status_word, stream_handle, workspace
 from .state import Mat33Field, ScalarField, Sym33Field, Vec3Field
 
 
@@ -93,6 +93,7 @@ class SubstepGraph:
         self.G = grid_from_state(mpm)
         self.prm = params_from_states(sim, mpm)
         self.status = status_word(sim.device)
+        self.ws = workspace(mpm, sim.nPoints, sim.device)
         self.graph = torch.cuda.CUDAGraph()
         self.stream = torch.cuda.Stream(device=sim.device)
         self.stream.wait_stream(torch.cuda.current_stream())
@@ -106,7 +107,8 @@ class SubstepGraph:
 
     def _call(self):
         _lib.check(_lib.lib().mpmw_run_substeps(self.P, self.G, self.prm, self.k, self.status.data_ptr(),
-                                                 stream_handle()), "run_substeps")
+                                                 self.ws.data_ptr(), self.ws.numel(), stream_handle()),
+                   "run_substeps")
 
     def replay(self):
         self.graph.replay()

@@ -18,7 +18,7 @@ from __future__ import annotations
 import torch
 
 from .. import _lib
-from ..bind import grid_from_state, params_from_states, particles_from_states, status_word, stream_handle
+from ..bind import grid_from_state, params_from_states, particles_from_states, status_word, stream_handle, workspace
 from ..state import F32, I32
 
 __all__ = ["mpmSimulationStep", "xpbdSimulationStep", "run_mpm_substeps", "arrayScalarMultiply",
@@ -43,8 +43,9 @@ def run_mpm_substeps(sim, mpm, xpbd, nsteps, device=None):
     """``nsteps`` consecutive ``mpmSimulationStep`` calls as one library call."""
     P, G, prm = _structs(sim, mpm, xpbd)
     st = status_word(sim.device)
-    _lib.check(_lib.lib().mpmw_run_substeps(P, G, prm, int(nsteps), st.data_ptr(), stream_handle()),
-               "run_mpm_substeps")
+    ws = workspace(mpm, sim.nPoints, sim.device)
+    _lib.check(_lib.lib().mpmw_run_substeps(P, G, prm, int(nsteps), st.data_ptr(), ws.data_ptr(), ws.numel(),
+                                            stream_handle()), "run_mpm_substeps")
 
 
 def xpbdSimulationStep(sim, mpm, xpbd, device=None, xpbd_only=False):

@@ -253,35 +253,56 @@ def test_fused_multistep_matches_unfused():
         assert rel_err(ga[k], gb[k]) <= tol, (k, rel_err(ga[k], gb[k]))
 
 
-def test_multistep_conservation_vs_oracle():
-    """100 fused steps of a 4,096-particle Drucker-Prager block collapse (the
-    64k block-collapse scene at reduced size; cohesion 0.1 MPa so that it
-    yields): total mass, momentum and damaged fraction agree with the FP64
-    oracle's 100 reference-order steps within 1e-3.  The FP32 oracle's own
-    distance from FP64 is printed for comparison."""
+def _block_run(cohesion, nsteps):
+    """``nsteps`` fused GPU steps of a 4,096-particle Drucker-Prager block collapse
+    (the 64k block-collapse scene at reduced size) beside the FP32 and FP64
+    oracles' reference-order steps."""
     torch = _torch()
     from mpmwarpydw_b200 import domains
     from mpmwarpydw_b200.utils import simulationRoutines as S
-    d = domains.block_collapse(n_side=16, spacing=0.25, jitter=0.025, seed=0, box=4.0, dx=0.5, cohesion=1e5)
+    d = domains.block_collapse(n_side=16, spacing=0.25, jitter=0.025, seed=0, box=4.0, dx=0.5, cohesion=cohesion)
     sim, mpm, xpbd = domains.build(d, device="cuda:0")
     s32 = to_oracle(sim, mpm, xpbd)
     s64 = to_oracle(sim, mpm, xpbd, np.float64)
-    S.run_mpm_substeps(sim, mpm, xpbd, 100)
+    S.run_mpm_substeps(sim, mpm, xpbd, nsteps)
     torch.cuda.synchronize()
-    _run_oracle_steps(s32, 100)
-    _run_oracle_steps(s64, 100, "f64")
+    _run_oracle_steps(s32, nsteps)
+    _run_oracle_steps(s64, nsteps, "f64")
     g = gpu_fields(sim, mpm, xpbd)
     m = s64.particle_mass
     mom = lambda v: (m[:, None] * np.asarray(v, np.float64)).sum(0)  # noqa: E731
     mg, m32, m64 = mom(g["particle_v"]), mom(s32.particle_v), mom(s64.particle_v)
     scale = np.max(np.abs(m64))
-    print(f"momentum rel. to FP64: GPU {np.max(np.abs(mg - m64)) / scale:.2e}, FP32 oracle {np.max(np.abs(m32 - m64)) / scale:.2e}")
-    assert np.max(np.abs(mg - m64)) <= 1e-3 * scale
-    assert abs(g["grid_m"].sum() - s64.grid_m.sum()) <= 1e-3 * s64.grid_m.sum()
-    dg = float((g["particle_damage"] >= 1).mean()); d64 = float((s64.particle_damage >= 1).mean())
-    print("damaged fraction gpu", dg, "fp64", d64, "plastic", int((s64.particle_accumulated_strain > 0).sum()))
-    assert abs(dg - d64) <= 1e-3
+    e_gpu, e_32 = np.max(np.abs(mg - m64)) / scale, np.max(np.abs(m32 - m64)) / scale
+    print(f"cohesion {cohesion:g}, {nsteps} steps: momentum rel. to FP64: GPU {e_gpu:.2e}, FP32 oracle {e_32:.2e}")
+    assert abs(g["grid_m"].sum() - s64.grid_m.sum()) <= 1e-5 * s64.grid_m.sum()
+    return g, s32, s64, e_gpu, e_32
+
+
+def test_multistep_elastic_vs_oracle():
+    """100 fused steps of the block with cohesion 1 GPa (no particle yields):
+    momentum within 1e-3 and positions within 1e-5 of the FP64 oracle."""
+    g, s32, s64, e_gpu, e_32 = _block_run(1e9, 100)
+    assert (s64.particle_accumulated_strain > 0).sum() == 0
+    assert e_gpu <= 1e-3
     assert rel_err(g["particle_x"], s64.particle_x) <= 1e-5
+
+
+def test_multistep_plastic_within_fp32_floor():
+    """100 fused steps of the block with cohesion 0.1 MPa (it yields and
+    collapses).  Plastic flow amplifies rounding: the FP32 oracle's own momentum
+    drifts from FP64 by tens of percent, so the GPU is held to the FP32 floor --
+    at most twice the FP32 oracle's distance from FP64 (or 1e-3), for momentum,
+    positions and the damaged fraction."""
+    g, s32, s64, e_gpu, e_32 = _block_run(1e5, 100)
+    assert (s64.particle_accumulated_strain > 0).sum() > 100
+    assert e_gpu <= max(1e-3, 2.0 * e_32)
+    ex_gpu, ex_32 = rel_err(g["particle_x"], s64.particle_x), rel_err(s32.particle_x, s64.particle_x)
+    assert ex_gpu <= max(1e-5, 2.0 * ex_32), (ex_gpu, ex_32)
+    n = len(s64.particle_damage)
+    dg, d32, d64 = ((a >= 1).mean() for a in (g["particle_damage"], s32.particle_damage, s64.particle_damage))
+    print("damaged fraction gpu", dg, "fp32", d32, "fp64", d64)
+    assert abs(dg - d64) <= max(1e-3, 2.0 * abs(d32 - d64)) + 1.0 / n
 
 
 def test_status_word_flags_out_of_grid():
