@@ -96,7 +96,9 @@ __global__ void __launch_bounds__(kBlock) k_g2p(mpmw_particles_t P, mpmw_grid_t 
     __syncthreads();
     if (s_lo[0] == INT32_MAX) return;  // no active MPM particle (uniform)
     const int ox = s_lo[0], oy = s_lo[1], oz = s_lo[2];
-    bool tile = use_tma && (int64_t)s_hi[0] - ox + 3 <= kTileEdge && (int64_t)s_hi[1] - oy + 3 <= kTileEdge &&
+    // once any CTA has reported a TMA timeout the rest of the launch gathers from global memory
+    const bool tma_ok = use_tma && !(status && (*reinterpret_cast<volatile uint32_t *>(status) & MPMW_ST_TIMEOUT));
+    bool tile = tma_ok && (int64_t)s_hi[0] - ox + 3 <= kTileEdge && (int64_t)s_hi[1] - oy + 3 <= kTileEdge &&
                 (int64_t)s_hi[2] - oz + 3 <= kTileEdge;
     uint32_t bad = 0;
     if (tile) {
@@ -107,9 +109,9 @@ __global__ void __launch_bounds__(kBlock) k_g2p(mpmw_particles_t P, mpmw_grid_t 
             tma_load_4d(s_tile, &tmap, 0, oz, oy, ox, &s_bar);
         }
         if (!mbar_wait_bounded(&s_bar, 0)) {
-            // the copy did not complete: report, give it one more bounded wait,
-            // and gather from global memory instead
-            bad |= MPMW_ST_TIMEOUT;
+            // the copy did not complete: report at once (so later CTAs skip TMA),
+            // give it one more bounded wait, and gather from global memory instead
+            raise_status(status, MPMW_ST_TIMEOUT);
             mbar_wait_bounded(&s_bar, 0);
             tile = false;
         }

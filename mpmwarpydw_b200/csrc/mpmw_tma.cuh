@@ -2,7 +2,7 @@
 //
 // Device side: an mbarrier in shared memory, one elected thread issues
 // cp.async.bulk.tensor.4d (no multicast) with complete_tx accounting, every
-// thread waits on the barrier's phase with a bounded number of polls.
+// thread waits on the barrier's phase for a bounded time.
 // Host side: CUtensorMap descriptors of grid velocity arrays, cached per
 // (pointer, dims).
 #pragma once
@@ -15,7 +15,7 @@ namespace mpmw {
 constexpr int kTileEdge = 8;                                       // nodes per tile edge
 constexpr int kTileNodes = kTileEdge * kTileEdge * kTileEdge;      // 512
 constexpr unsigned kTileBytes = kTileNodes * 16u;                  // float4 per node
-constexpr int kMbarMaxPolls = 1 << 20;
+constexpr int kMbarMaxPolls = 1 << 24;  // also bounded by kMbarWaitNs
 
 __device__ __forceinline__ unsigned smem_addr(const void *p)
 {
@@ -34,12 +34,12 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned by
                  : "memory");
 }
 
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned phase)
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, unsigned phase)
 {
     unsigned ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
         : "r"(smem_addr(bar)), "r"(phase)
@@ -47,11 +47,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned phase)
     return ok != 0;
 }
 
-// bounded wait on phase `phase`; returns false if the barrier never completed
+__device__ __forceinline__ uint64_t globaltimer_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for phase `phase` of the barrier for at most kMbarWaitNs of wall time
+// (non-blocking polls with a short back-off); false if it never completed.
+constexpr uint64_t kMbarWaitNs = 200ull * 1000ull * 1000ull;  // 200 ms
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned phase)
 {
-    for (int i = 0; i < kMbarMaxPolls; ++i)
-        if (mbar_try_wait(bar, phase)) return true;
+    if (mbar_test_wait(bar, phase)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    for (int i = 0; i < kMbarMaxPolls; ++i) {
+        if (mbar_test_wait(bar, phase)) return true;
+        if (globaltimer_ns() - t0 > kMbarWaitNs) return false;
+        __nanosleep(32);
+    }
     return false;
 }
 
