@@ -152,6 +152,16 @@ int mpmw_g2p_stress(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_
 /* Bytes of device workspace mpmw_g2p_stress / mpmw_run_substeps need for n
  * particles (a worklist of the particles whose return map takes the SVD path). */
 size_t mpmw_workspace_bytes(int64_t n);
+/* The middle of a fused run (utils/simulationRoutines.py:6-293 applied twice):
+ * substep k's g2p (mpmRoutines.py:715-802), then substep k+1's
+ * compute_stress_from_F_trial (:229-312) and p2g_apic_with_stress (:485-569),
+ * per particle in registers.  grid->v holds substep k's grid velocity and
+ * grid->mv must be zero on entry (it receives substep k+1's P2G).  Writes x and
+ * F; the stress only when store_stress != 0; v, C and F_trial only for
+ * particles that leave the MPM path or need the SVD return map.  A run of such
+ * calls ends with mpmw_g2p, which writes x, v, C and F_trial. */
+int mpmw_g2p2g(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, int store_stress,
+               uint32_t *status, void *workspace, size_t ws_bytes, mpmw_stream_t stream);
 /* utils/mpmRoutines.py:817-911 accumulate_cell_divergence + apply_volumetric_locking_correction
  * (zeroes grid->cell_div / cell_vol itself, utils/simulationRoutines.py:255-293) */
 int mpmw_vlc(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/mpmw.h"
+#include "../../include/mpmw_xpbd.h"
 
 namespace mpmw {
 
@@ -11,6 +12,9 @@ int launch_stress(const mpmw_particles_t &p, const mpmw_params_t &prm, cudaStrea
 int launch_p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, cudaStream_t s);
 int launch_g2p(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, bool fused,
                void *ws, size_t ws_bytes, cudaStream_t s);
+int launch_g2p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st,
+                 bool store_stress, void *ws, size_t ws_bytes, cudaStream_t s);
 size_t g2p_workspace_bytes(int64_t n);
+size_t hash_workspace_bytes(int64_t n);
 
 }  // namespace mpmw

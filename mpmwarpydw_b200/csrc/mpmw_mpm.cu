@@ -112,13 +112,16 @@ __device__ __forceinline__ void apply_bc(int bc, const int *idx, const int *dim,
     }
 }
 
-__global__ void __launch_bounds__(kBlock) k_grid_update(mpmw_grid_t G, mpmw_params_t prm)
+// zero_mv: also clear the accumulators after reading them (for the fused
+// G2P->P2G kernel, which scatters the next substep into them)
+__global__ void __launch_bounds__(kBlock) k_grid_update(mpmw_grid_t G, mpmw_params_t prm, int zero_mv)
 {
     const int nx = G.dims[0], ny = G.dims[1], nz = G.dims[2];
     const int64_t total = (int64_t)nx * ny * nz;
     int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= total) return;
     const float4 a = reinterpret_cast<const float4 *>(G.mv)[g];
+    if (zero_mv) reinterpret_cast<float4 *>(G.mv)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
     float o[3] = {0.f, 0.f, 0.f};
     if (a.x > 1e-15f) {
         float inv = 1.f / a.x;
@@ -393,10 +396,10 @@ static int check_params(const mpmw_params_t *prm)
     } while (0)
 
 // host-side launchers (also used by the multi-step driver)
-int launch_grid(const mpmw_grid_t &g, const mpmw_params_t &prm, cudaStream_t s)
+int launch_grid(const mpmw_grid_t &g, const mpmw_params_t &prm, cudaStream_t s, bool zero_mv = false)
 {
     int64_t G = (int64_t)g.dims[0] * g.dims[1] * g.dims[2];
-    k_grid_update<<<grid_for(G), kBlock, 0, s>>>(g, prm);
+    k_grid_update<<<grid_for(G), kBlock, 0, s>>>(g, prm, zero_mv ? 1 : 0);
     return check_launch("k_grid_update");
 }
 int launch_vlc(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, cudaStream_t s)
@@ -510,6 +513,17 @@ int mpmw_g2p_stress(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_
     return launch_g2p(*p, *g, *prm, status, true, workspace, ws_bytes, as_stream(stream));
 }
 
+int mpmw_g2p2g(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, int store_stress,
+               uint32_t *status, void *workspace, size_t ws_bytes, mpmw_stream_t stream)
+{
+    MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV | kNeedCF | kNeedStress));
+    MPMW_TRY(check_grid(g));
+    MPMW_TRY(check_params(prm));
+    if (p->n > 0 && (!p->vol || !p->mass)) { set_error("g2p2g: vol and mass are required"); return MPMW_E_ARG; }
+    if (prm->update_cov && p->n > 0 && !p->cov) { set_error("g2p2g: update_cov needs cov"); return MPMW_E_ARG; }
+    return launch_g2p2g(*p, *g, *prm, status, store_stress != 0, workspace, ws_bytes, as_stream(stream));
+}
+
 int mpmw_vlc(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
              mpmw_stream_t stream)
 {
@@ -555,20 +569,30 @@ int mpmw_run_substeps(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpm
     if (prm->update_cov && p->n > 0 && !p->cov) { set_error("substep: update_cov needs cov"); return MPMW_E_ARG; }
     if (prm->vlc && (!g->cell_div || !g->cell_vol)) { set_error("substep: vlc needs cell_div/cell_vol"); return MPMW_E_ARG; }
     cudaStream_t s = as_stream(stream);
-    bool need_stress = true;
+    if (nsteps == 0) return MPMW_OK;
+    // Fused schedule (no VLC, workspace given): after the first substep's
+    // stress + P2G, each grid update also clears the accumulators and one
+    // G2P->P2G kernel carries substep k's G2P, substep k+1's return map and
+    // substep k+1's P2G; the last substep ends with the plain G2P.  Otherwise
+    // every substep is stress, P2G, grid update, G2P (+ VLC).
+    const bool fuse = !prm->vlc && workspace != nullptr;
+    MPMW_TRY(launch_stress(*p, *prm, s));
+    MPMW_TRY(zero_grid(*g, s));
+    MPMW_TRY(launch_p2g(*p, *g, *prm, status, s));
     for (int step = 0; step < nsteps; ++step) {
-        if (need_stress) MPMW_TRY(launch_stress(*p, *prm, s));
-        MPMW_TRY(zero_grid(*g, s));
-        MPMW_TRY(launch_p2g(*p, *g, *prm, status, s));
-        MPMW_TRY(launch_grid(*g, *prm, s));
-        bool last = step == nsteps - 1;
-        if (!last && !prm->vlc && workspace) {
-            MPMW_TRY(launch_g2p(*p, *g, *prm, status, true, workspace, ws_bytes, s));
-            need_stress = false;
+        const bool last = step == nsteps - 1;
+        if (!last && fuse) {
+            MPMW_TRY(launch_grid(*g, *prm, s, true));
+            MPMW_TRY(launch_g2p2g(*p, *g, *prm, status, step + 1 == nsteps - 1, workspace, ws_bytes, s));
         } else {
+            MPMW_TRY(launch_grid(*g, *prm, s));
             MPMW_TRY(launch_g2p(*p, *g, *prm, status, false, nullptr, 0, s));
             if (prm->vlc) MPMW_TRY(launch_vlc(*p, *g, *prm, status, s));
-            need_stress = true;
+            if (!last) {
+                MPMW_TRY(launch_stress(*p, *prm, s));
+                MPMW_TRY(zero_grid(*g, s));
+                MPMW_TRY(launch_p2g(*p, *g, *prm, status, s));
+            }
         }
     }
     return MPMW_OK;

@@ -1,201 +1,36 @@
 // mpmw_p2g.cu -- APIC particle-to-grid transfer with stress (reference:
-// utils/mpmRoutines.py:485-569 p2g_apic_with_stress).
-//
-// One CTA per chunk of kP2GChunk consecutive particles:
-//   1. active MPM particles are compacted; each gets its B-spline weights and
-//      per-particle constants in shared memory;
-//   2. consecutive particles with the same stencil base cell (the reference's
-//      truncated base index, bit-exact) form a segment -- they scatter to the
-//      same 27 nodes;
-//   3. one thread per (segment, i, j) stencil column sums its particles'
-//      contributions to the column's 3 nodes in registers (no atomics);
-//   4. columns are added into a shared-memory tile covering the chunk's
-//      stencil bounding box, which is flushed with one float4 atomic per
-//      touched node.  A chunk whose box exceeds the tile adds its columns
-//      straight into global memory, so any particle order is correct; particles
-//      sorted by base cell make segments long and tiles small.
-//
-// Contribution of particle p to node (i,j,k) (quadratic B-spline, fx = grid
-// position - base):
-//   m:   w_ijk m
-//   m v: w_ijk (a + i Bx + j By + k Bz) + S (dwx_i wy_j wz_k, wx_i dwy_j wz_k, wx_i wy_j dwz_k)
-// with B = m C' dx (columns Bx, By, Bz), a = m v - B fx, S = -dt vol inv_dx stress,
-// C' = (1 - r) C + (r/2)(C - C^T) (C' = 0 when r < -0.001).
+// utils/mpmRoutines.py:485-569 p2g_apic_with_stress): one CTA per chunk of
+// kScatterChunk consecutive particles, scattered by p2g_scatter
+// (mpmw_scatter.cuh).
 #include "mpmw_common.cuh"
 #include "mpmw_internal.cuh"
 #include "mpmw_math.cuh"
-#include "mpmw_scan.cuh"
+#include "mpmw_scatter.cuh"
 
 namespace mpmw {
 
-constexpr int kP2GChunk = 256;    // particles (and threads) per CTA
-constexpr int kP2GTile = 1024;    // nodes in the shared tile
-
-struct P2GShared {
-    float4 rec[10][kP2GChunk];    // per compacted particle: see pack order below
-    int base[3][kP2GChunk];
-    int seg_start[kP2GChunk + 1];
-    float4 tile[kP2GTile];
-    int lo[3], hi[3];
-    int nact, nseg;
-};
-
-__device__ __forceinline__ float sel3(const float4 &r, int i) { return i == 0 ? r.x : (i == 1 ? r.y : r.z); }
-
-__global__ void __launch_bounds__(kP2GChunk) k_p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
-                                                   uint32_t *status)
+__global__ void __launch_bounds__(kScatterChunk) k_p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
+                                                       uint32_t *status)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    P2GShared &S = *reinterpret_cast<P2GShared *>(smem_raw);
-    const int t = threadIdx.x;
+    ScatterShared &S = *reinterpret_cast<ScatterShared *>(smem_raw);
     const int64_t n = P.n;
-    const int64_t p = (int64_t)blockIdx.x * kP2GChunk + t;
-    const int nx = G.dims[0], ny = G.dims[1], nz = G.dims[2];
-    float4 *__restrict__ gmv = reinterpret_cast<float4 *>(G.mv);
-
-    if (t < 3) { S.lo[t] = INT32_MAX; S.hi[t] = INT32_MIN; }
-    bool act = p < n && P.active[p] == 1 && P.material[p] <= 1;
-    int total;
-    const int k = block_excl_scan(act ? 1 : 0, &total);  // compacted slot (syncs)
-    if (t == 0) S.nact = total;
-    int b0 = 0, b1 = 0, b2 = 0;
+    const int64_t p = (int64_t)blockIdx.x * kScatterChunk + threadIdx.x;
+    const bool act = p < n && P.active[p] == 1 && P.material[p] <= 1;
+    float xp[3] = {0.f, 0.f, 0.f}, v[3] = {0.f, 0.f, 0.f}, C0[9], st6[6];
+    float m = 0.f, vol = 0.f;
     if (act) {
-        float xp[3];
         load3(P.x, n, p, xp);
-        Weights W;
-        weights(xp, prm.min_bounds, prm.inv_dx, W);
-        b0 = W.base[0]; b1 = W.base[1]; b2 = W.base[2];
-        float C0[9], st[9], v[3];
-        load9(P.C, n, p, C0);
-        load_sym6(P.stress, n, p, st);
         load3(P.v, n, p, v);
-        const float m = P.mass[p];
-        const float r = prm.rpic_damping;
-        float Cp[9];
+        load9(P.C, n, p, C0);
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b)
-                Cp[3 * a + b] = (1.f - r) * C0[3 * a + b] + (r / 2.f) * (C0[3 * a + b] - C0[3 * b + a]);
-        if (r < -0.001f) {
-#pragma unroll
-            for (int q = 0; q < 9; ++q) Cp[q] = 0.f;
-        }
-        const float mdx = m * prm.dx;
-        float B[9];  // B[3*row + col] = m C'[row][col] dx
-#pragma unroll
-        for (int q = 0; q < 9; ++q) B[q] = Cp[q] * mdx;
-        float a[3];
-#pragma unroll
-        for (int row = 0; row < 3; ++row)
-            a[row] = fma_(-B[3 * row + 0], W.fx[0], fma_(-B[3 * row + 1], W.fx[1], fma_(-B[3 * row + 2], W.fx[2], m * v[row])));
-        const float sc = -(prm.dt * P.vol[p]) * prm.inv_dx;
-        S.rec[0][k] = make_float4(W.w[0][0], W.w[0][1], W.w[0][2], m);
-        S.rec[1][k] = make_float4(W.dw[0][0], W.dw[0][1], W.dw[0][2], sc * st[0]);
-        S.rec[2][k] = make_float4(W.w[1][0], W.w[1][1], W.w[1][2], sc * st[4]);
-        S.rec[3][k] = make_float4(W.dw[1][0], W.dw[1][1], W.dw[1][2], sc * st[8]);
-        S.rec[4][k] = make_float4(W.w[2][0], W.w[2][1], W.w[2][2], sc * st[1]);
-        S.rec[5][k] = make_float4(W.dw[2][0], W.dw[2][1], W.dw[2][2], sc * st[2]);
-        S.rec[6][k] = make_float4(a[0], a[1], a[2], sc * st[5]);
-        S.rec[7][k] = make_float4(B[0], B[3], B[6], 0.f);   // Bx = column 0
-        S.rec[8][k] = make_float4(B[1], B[4], B[7], 0.f);   // By
-        S.rec[9][k] = make_float4(B[2], B[5], B[8], 0.f);   // Bz
-        S.base[0][k] = b0; S.base[1][k] = b1; S.base[2][k] = b2;
+        for (int e = 0; e < 6; ++e) st6[e] = P.stress[(int64_t)e * n + p];
+        m = P.mass[p];
+        vol = P.vol[p];
     }
-    // chunk bounding box of stencil bases
-    {
-        int lo0 = act ? b0 : INT32_MAX, lo1 = act ? b1 : INT32_MAX, lo2 = act ? b2 : INT32_MAX;
-        int hi0 = act ? b0 : INT32_MIN, hi1 = act ? b1 : INT32_MIN, hi2 = act ? b2 : INT32_MIN;
-        lo0 = __reduce_min_sync(0xffffffffu, lo0); lo1 = __reduce_min_sync(0xffffffffu, lo1); lo2 = __reduce_min_sync(0xffffffffu, lo2);
-        hi0 = __reduce_max_sync(0xffffffffu, hi0); hi1 = __reduce_max_sync(0xffffffffu, hi1); hi2 = __reduce_max_sync(0xffffffffu, hi2);
-        if ((t & 31) == 0) {
-            atomicMin(&S.lo[0], lo0); atomicMin(&S.lo[1], lo1); atomicMin(&S.lo[2], lo2);
-            atomicMax(&S.hi[0], hi0); atomicMax(&S.hi[1], hi1); atomicMax(&S.hi[2], hi2);
-        }
-    }
-    __syncthreads();
-    const int nact = S.nact;
-    if (nact == 0) return;  // uniform
-    // segments: runs of equal base in compacted order
-    bool head = t < nact &&
-                (t == 0 || S.base[0][t] != S.base[0][t - 1] || S.base[1][t] != S.base[1][t - 1] ||
-                 S.base[2][t] != S.base[2][t - 1]);
-    int nseg;
-    const int sidx = block_excl_scan(head ? 1 : 0, &nseg);
-    if (head) S.seg_start[sidx] = t;
-    if (t == 0) S.seg_start[nseg] = nact;
-    const int ox = S.lo[0], oy = S.lo[1], oz = S.lo[2];
-    const int64_t ex = (int64_t)S.hi[0] - ox + 3, ey = (int64_t)S.hi[1] - oy + 3, ez = (int64_t)S.hi[2] - oz + 3;
-    const bool use_tile = ex * ey * ez <= kP2GTile;
-    const int tv = use_tile ? (int)(ex * ey * ez) : 0, eyi = (int)ey, ezi = (int)ez;
-    for (int q = t; q < tv; q += kP2GChunk) S.tile[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-    __syncthreads();
-
     uint32_t bad = 0;
-    for (int item = t; item < nseg * 9; item += kP2GChunk) {
-        const int s = item / 9, ij = item - 9 * s, i = ij / 3, j = ij - 3 * i;
-        const float fi = (float)i, fj = (float)j;
-        const int k0 = S.seg_start[s], k1 = S.seg_start[s + 1];
-        float am0 = 0.f, am1 = 0.f, am2 = 0.f;
-        float ax0 = 0.f, ay0 = 0.f, az0 = 0.f, ax1 = 0.f, ay1 = 0.f, az1 = 0.f, ax2 = 0.f, ay2 = 0.f, az2 = 0.f;
-        for (int q = k0; q < k1; ++q) {
-            const float4 r0 = S.rec[0][q], r1 = S.rec[1][q], r2 = S.rec[2][q], r3 = S.rec[3][q], r4 = S.rec[4][q],
-                         r5 = S.rec[5][q], r6 = S.rec[6][q], r7 = S.rec[7][q], r8 = S.rec[8][q], r9 = S.rec[9][q];
-            const float wxi = sel3(r0, i), dwxi = sel3(r1, i), wyj = sel3(r2, j), dwyj = sel3(r3, j);
-            const float m = r0.w;
-            const float s00 = r1.w, s11 = r2.w, s22 = r3.w, s01 = r4.w, s02 = r5.w, s12 = r6.w;
-            const float wxy = wxi * wyj, g0 = dwxi * wyj, g1 = wxi * dwyj, wm = wxy * m;
-            // A = a + i Bx + j By
-            const float A0 = fma_(fj, r8.x, fma_(fi, r7.x, r6.x));
-            const float A1 = fma_(fj, r8.y, fma_(fi, r7.y, r6.y));
-            const float A2 = fma_(fj, r8.z, fma_(fi, r7.z, r6.z));
-            // Q = S (g0, g1, 0), R = wxy S[:,2]
-            const float Q0 = fma_(s00, g0, s01 * g1), Q1 = fma_(s01, g0, s11 * g1), Q2 = fma_(s02, g0, s12 * g1);
-            const float R0 = wxy * s02, R1 = wxy * s12, R2 = wxy * s22;
-            // P_k = wxy (A + k Bz) + Q
-            const float P00 = fma_(wxy, A0, Q0), P01 = fma_(wxy, A1, Q1), P02 = fma_(wxy, A2, Q2);
-            const float dz0 = wxy * r9.x, dz1 = wxy * r9.y, dz2 = wxy * r9.z;
-            const float P10 = P00 + dz0, P11 = P01 + dz1, P12 = P02 + dz2;
-            const float P20 = P10 + dz0, P21 = P11 + dz1, P22 = P12 + dz2;
-            am0 = fma_(r4.x, wm, am0); am1 = fma_(r4.y, wm, am1); am2 = fma_(r4.z, wm, am2);
-            ax0 = fma_(r4.x, P00, fma_(r5.x, R0, ax0)); ay0 = fma_(r4.x, P01, fma_(r5.x, R1, ay0)); az0 = fma_(r4.x, P02, fma_(r5.x, R2, az0));
-            ax1 = fma_(r4.y, P10, fma_(r5.y, R0, ax1)); ay1 = fma_(r4.y, P11, fma_(r5.y, R1, ay1)); az1 = fma_(r4.y, P12, fma_(r5.y, R2, az1));
-            ax2 = fma_(r4.z, P20, fma_(r5.z, R0, ax2)); ay2 = fma_(r4.z, P21, fma_(r5.z, R1, ay2)); az2 = fma_(r4.z, P22, fma_(r5.z, R2, az2));
-        }
-        const int gx = S.base[0][k0] + i, gy = S.base[1][k0] + j, gz0 = S.base[2][k0];
-        const float4 c[3] = {make_float4(am0, ax0, ay0, az0), make_float4(am1, ax1, ay1, az1),
-                             make_float4(am2, ax2, ay2, az2)};
-        if (use_tile) {
-            const int tb = ((gx - ox) * eyi + (gy - oy)) * ezi + (gz0 - oz);
-#pragma unroll
-            for (int kk = 0; kk < 3; ++kk) {
-                float *d = reinterpret_cast<float *>(&S.tile[tb + kk]);
-                atomicAdd(d + 0, c[kk].x);
-                atomicAdd(d + 1, c[kk].y);
-                atomicAdd(d + 2, c[kk].z);
-                atomicAdd(d + 3, c[kk].w);
-            }
-        } else {
-#pragma unroll
-            for (int kk = 0; kk < 3; ++kk) {
-                const int gz = gz0 + kk;
-                if (gx < 0 || gy < 0 || gz < 0 || gx >= nx || gy >= ny || gz >= nz) { bad = MPMW_ST_OOB; continue; }
-                atomicAdd(&gmv[((int64_t)gx * ny + gy) * nz + gz], c[kk]);
-            }
-        }
-    }
-    if (use_tile) {
-        __syncthreads();
-        for (int q = t; q < tv; q += kP2GChunk) {
-            float4 a = S.tile[q];
-            if (a.x == 0.f && a.y == 0.f && a.z == 0.f && a.w == 0.f) continue;
-            int lz = q % ezi, rest = q / ezi;
-            int ly = rest % eyi, lx = rest / eyi;
-            int ix = ox + lx, iy = oy + ly, iz = oz + lz;
-            if (ix < 0 || iy < 0 || iz < 0 || ix >= nx || iy >= ny || iz >= nz) { bad = MPMW_ST_OOB; continue; }
-            atomicAdd(&gmv[((int64_t)ix * ny + iy) * nz + iz], a);
-        }
-    }
+    p2g_scatter(S, act, xp, v, C0, st6, m, vol, prm, reinterpret_cast<float4 *>(G.mv), G.dims[0], G.dims[1],
+                G.dims[2], bad);
     if (bad) raise_status(status, bad);
 }
 
@@ -205,8 +40,8 @@ int launch_p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_param
 {
     if (p.n == 0) return MPMW_OK;
     int dev = 0;
-    cudaGetDevice(&dev);
-    const size_t smem = sizeof(P2GShared);
+    if (cudaGetDevice(&dev) != cudaSuccess) { set_error("p2g: no current device"); return MPMW_E_DEVICE; }
+    const size_t smem = sizeof(ScatterShared);
     if (dev >= 0 && dev < 64 && !g_p2g_attr[dev]) {
         if (cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
             set_error("p2g: cannot reserve %zu bytes of shared memory", smem);
@@ -214,7 +49,7 @@ int launch_p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_param
         }
         g_p2g_attr[dev] = true;
     }
-    k_p2g<<<grid_for(p.n, kP2GChunk), kP2GChunk, smem, s>>>(p, g, prm, st);
+    k_p2g<<<grid_for(p.n, kScatterChunk), kScatterChunk, smem, s>>>(p, g, prm, st);
     return check_launch("k_p2g");
 }
 

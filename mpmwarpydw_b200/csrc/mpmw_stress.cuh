@@ -98,12 +98,13 @@ __device__ __forceinline__ void sym_exp_small(const float *A, float *E)
     for (int e = 0; e < 6; ++e) E[e] = P[e] + (e < 3 ? 1.f : 0.f);
 }
 
-// Tensor-form return map for |F F^T - I|_F <= 0.02 (see file header).
-// Returns false, touching nothing, when the deformation is larger.
+// Tensor-form return map for |F F^T - I|_F <= 0.02 and det F > 0 (see file
+// header).  Returns 0, touching nothing, when it does not apply; 1 when done;
+// 2 when done and the particle became an XPBD particle (T = 0).
 // On success writes Fout, the symmetric Kirchhoff stress T (before the viscous
 // term) and the same per-particle side effects as the SVD path.
 template <bool HaveXV>
-__device__ __forceinline__ bool small_strain_update(const mpmw_particles_t &P, float eff, int64_t p, const float *Ft,
+__device__ __forceinline__ int small_strain_update(const mpmw_particles_t &P, float eff, int64_t p, const float *Ft,
                                                     const float *xr, float *vr, float *Fout, float *T)
 {
     const int64_t n = P.n;
@@ -120,14 +121,14 @@ __device__ __forceinline__ bool small_strain_update(const mpmw_particles_t &P, f
                         fma_(G[3 * r + 2], G[3 * c + 2], G[3 * r + c] + G[3 * c + r])));
         }
     }
-    if (!(sym_ddot(X, X) <= 4e-4f)) return false;
+    if (!(sym_ddot(X, X) <= 4e-4f)) return 0;
     // F F^T near I also holds for a reflection (det F ~ -1); the reference's
     // SVD then has a negative singular value, clamped to 0.01, so a reflected
     // F must take the SVD path.  With F F^T near I, det F is near +-1.
     {
         const float det = Ft[0] * (Ft[4] * Ft[8] - Ft[5] * Ft[7]) - Ft[1] * (Ft[3] * Ft[8] - Ft[5] * Ft[6]) +
                           Ft[2] * (Ft[3] * Ft[7] - Ft[4] * Ft[6]);
-        if (!(det > 0.f)) return false;
+        if (!(det > 0.f)) return 0;
     }
     // eps = 1/2 ln(I + X) = 1/2 X (I + X (-1/2 I + X (1/3 I - 1/4 X)))
     float eps[6];
@@ -192,7 +193,7 @@ __device__ __forceinline__ bool small_strain_update(const mpmw_particles_t &P, f
             P.ys[p] = 0.f; P.mu[p] = 0.f; P.lam[p] = 0.f; P.alpha[p] = 0.f;
 #pragma unroll
             for (int k = 0; k < 9; ++k) T[k] = 0.f;
-            return true;
+            return 2;
         }
         const float f = dgamma / edn;
         const float vc = (0.3f * alpha) * dgamma;
@@ -218,7 +219,7 @@ __device__ __forceinline__ bool small_strain_update(const mpmw_particles_t &P, f
 #pragma unroll
     for (int e = 0; e < 6; ++e) t6[e] = fma_(twomu, enew[e], e < 3 ? ltr : 0.f);
     sym_to_full(t6, T);
-    return true;
+    return 1;
 }
 
 // Return map + Kirchhoff + Kelvin-Voigt for one particle.

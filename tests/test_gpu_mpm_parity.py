@@ -233,12 +233,17 @@ def test_one_substep_matches_oracle(vlc, mode):
             assert e <= TOL, (k, e)
 
 
-def test_fused_multistep_matches_unfused():
-    """run_mpm_substeps(k) (return map fused into G2P) == k x mpmSimulationStep."""
+@pytest.mark.parametrize("mode", [0, 1])
+def test_fused_multistep_matches_unfused(mode):
+    """run_mpm_substeps(k) (G2P, next return map and next P2G fused in one
+    kernel; SVD-path particles through the list kernel -- all of them in mode 1)
+    == k x mpmSimulationStep."""
     torch = _torch()
     from mpmwarpydw_b200.utils import simulationRoutines as S
     a = small_scene(seed=8)
     b = small_scene(seed=8)
+    a[1].stress_mode = mode
+    b[1].stress_mode = mode
     for _ in range(5):
         S.mpmSimulationStep(*a, "cuda:0")
     S.run_mpm_substeps(*b, 5)
@@ -280,12 +285,16 @@ def _block_run(cohesion, nsteps):
 
 
 def test_multistep_elastic_vs_oracle():
-    """100 fused steps of the block with cohesion 1 GPa (no particle yields):
-    momentum within 1e-3 and positions within 1e-5 of the FP64 oracle."""
+    """100 fused steps of the block with cohesion 1 GPa (no particle yields).
+    Positions stay within 1e-5 of the FP64 oracle.  The block settles onto the
+    frictional floor and rings, so the velocity is phase-sensitive: the FP32
+    oracle's total momentum is about 1.5 % from FP64 while its positions agree
+    to 2e-6.  Momentum is therefore held to the FP32 floor: at most twice the
+    FP32 oracle's distance from FP64 (or 1e-3)."""
     g, s32, s64, e_gpu, e_32 = _block_run(1e9, 100)
     assert (s64.particle_accumulated_strain > 0).sum() == 0
-    assert e_gpu <= 1e-3
     assert rel_err(g["particle_x"], s64.particle_x) <= 1e-5
+    assert e_gpu <= max(1e-3, 2.0 * e_32)
 
 
 def test_multistep_plastic_within_fp32_floor():
