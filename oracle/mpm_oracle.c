@@ -11,9 +11,12 @@
  * CUDA kernels (left-to-right sums, no contraction: built with
  * -ffp-contract=off), so it agrees with them to the last bit except where the
  * GPU reorders floating-point atomics (P2G, cell sums, reductions) or where
- * logf/expf differ by an ulp.  The FP64 build is the precision reference, and
- * is pinned against the reference's own kernel source executed in double
- * precision (tests/golden/gen_golden.py).
+ * logf/expf differ by an ulp.  The FP64 build is the precision reference.
+ * Pinned: tests/test_oracle_golden.py checks it against golden vectors made by
+ * executing the reference's own mpmSimulationStep / xpbdSimulationStep source
+ * in float64 under a stand-in for the Warp API (tests/golden/gen_golden.py,
+ * tests/golden/fakewarp.py) -- agreement to ~1e-13 with identical labels --
+ * and against analytic known answers (tests/test_oracle_known_answers.py).
  *
  * Every function cites the reference kernel it restates (paths are relative to
  * the MPMWarpYDW project root).  Arrays use the reference layout: vec3 = 3
