@@ -74,6 +74,17 @@ size_t mpmw_hash_workspace_bytes(int64_t n);
 /* wp.HashGrid.build (simulationRoutines.py:311): x is [3][n] SoA. */
 int mpmw_hash_build(const float *x, int64_t n, const mpmw_hash_t *h, void *workspace, size_t ws_bytes,
                     mpmw_stream_t stream);
+/* No counterpart in the reference.  mpmw_hash_build without a caller workspace:
+ * for callers that cannot allocate device memory when they build the hash (a
+ * host embedding the solver under a fixed device-memory budget, or a loop that
+ * must not call cudaMalloc once stepping has started).  Its scratch is a
+ * 13 MiB static device array inside the library, so n is limited to
+ * MPMW_HASH_NOALLOC_MAX_POINTS; larger n returns MPMW_E_ARG.  The first call on
+ * a device (that device current) resolves the array's address; make it before
+ * any stream capture.  All calls on a device share the array: calls whose GPU
+ * work overlaps race on it, so order them on one stream. */
+#define MPMW_HASH_NOALLOC_MAX_POINTS 1048576
+int mpmw_hash_build_noalloc(const float *x, int64_t n, const mpmw_hash_t *h, mpmw_stream_t stream);
 /* One XPBD kernel (MPMW_XK_*). */
 int mpmw_xpbd_kernel(int which, const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_hash_t *h,
                      const mpmw_xpbd_params_t *q, int flag, mpmw_stream_t stream);

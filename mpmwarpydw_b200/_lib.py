@@ -103,6 +103,7 @@ _SIGS = {
     "mpmw_stats": (_I, [ctypes.POINTER(Particles), _P, _P]),
     "mpmw_hash_workspace_bytes": (ctypes.c_size_t, [_I64]),
     "mpmw_hash_build": (_I, [_P, _I64, ctypes.POINTER(Hash), _P, ctypes.c_size_t, _P]),
+    "mpmw_hash_build_noalloc": (_I, [_P, _I64, ctypes.POINTER(Hash), _P]),
     "mpmw_xpbd_kernel": (_I, [_I, ctypes.POINTER(Particles), ctypes.POINTER(XPBD), ctypes.POINTER(Hash),
                               ctypes.POINTER(XPBDParams), _I, _P]),
     "mpmw_xpbd_step": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(XPBD), ctypes.POINTER(Hash),
