@@ -142,7 +142,7 @@ struct G2P2GShared {
 // which the caller has zeroed).  StoreStress: also write the stress (the last
 // fused substep of a run).
 template <bool StoreStress>
-__global__ void __launch_bounds__(kScatterChunk) k_g2p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
+__global__ void __launch_bounds__(kScatterChunk, 3) k_g2p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
                                                         uint32_t *status, int *svd_list, int *svd_count,
                                                         const __grid_constant__ CUtensorMap tmap, int use_tma)
 {

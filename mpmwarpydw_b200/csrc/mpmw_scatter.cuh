@@ -12,7 +12,9 @@
 //      truncated base index, bit-exact) form a segment -- they scatter to the
 //      same 27 nodes;
 //   3. one thread per (segment, i, j) stencil column sums its particles'
-//      contributions to the column's 3 nodes in registers (no atomics);
+//      contributions to the column's 3 nodes in registers, for as many complete
+//      passes over the threads as there are; the (column, particle) pairs of
+//      the columns left over are split evenly over all threads;
 //   4. columns are added (shared-memory atomics) into a structure-of-arrays
 //      tile covering the CTA's stencil bounding box -- one float array per
 //      component, so the four adds of a node hit four arrays and lanes of a
@@ -41,6 +43,7 @@ struct ScatterShared {
     float4 rec[10][kScatterChunk];   // per compacted particle (swizzled slot)
     int base[3][kScatterChunk];
     int seg_start[kScatterChunk + 1];
+    int seg_of[kScatterChunk];      // segment of each compacted particle
     float tile[4][kScatterTile];     // m, m vx, m vy, m vz
     int lo[3], hi[3];
 };
@@ -48,6 +51,76 @@ struct ScatterShared {
 __device__ __forceinline__ int scatter_slot(int k) { return k ^ ((k >> 3) & 7); }
 
 __device__ __forceinline__ float sel3(const float4 &r, int i) { return i == 0 ? r.x : (i == 1 ? r.y : r.z); }
+
+// Register sums of one stencil column (i, j) of one segment: the 3 nodes
+// k = 0..2 of (m, m vx, m vy, m vz).
+struct ColumnSums {
+    float am0, am1, am2, ax0, ay0, az0, ax1, ay1, az1, ax2, ay2, az2;
+
+    __device__ __forceinline__ void zero()
+    {
+        am0 = am1 = am2 = 0.f;
+        ax0 = ay0 = az0 = ax1 = ay1 = az1 = ax2 = ay2 = az2 = 0.f;
+    }
+
+    // add the contribution of the particle in record slot q to column ij
+    template <class Shared>
+    __device__ __forceinline__ void add(const Shared &S, int q, int ij)
+    {
+        const int i = ij / 3, j = ij - 3 * (ij / 3);
+        const float fi = (float)i, fj = (float)j;
+        const float4 r0 = S.rec[0][q], r1 = S.rec[1][q], r2 = S.rec[2][q], r3 = S.rec[3][q], r4 = S.rec[4][q],
+                     r5 = S.rec[5][q], r6 = S.rec[6][q], r7 = S.rec[7][q], r8 = S.rec[8][q], r9 = S.rec[9][q];
+        const float wxi = sel3(r0, i), dwxi = sel3(r1, i), wyj = sel3(r2, j), dwyj = sel3(r3, j);
+        const float mm = r0.w;
+        const float s00 = r1.w, s11 = r2.w, s22 = r3.w, s01 = r4.w, s02 = r5.w, s12 = r6.w;
+        const float wxy = wxi * wyj, g0 = dwxi * wyj, g1 = wxi * dwyj, wm = wxy * mm;
+        // A = a + i Bx + j By
+        const float A0 = fma_(fj, r8.x, fma_(fi, r7.x, r6.x));
+        const float A1 = fma_(fj, r8.y, fma_(fi, r7.y, r6.y));
+        const float A2 = fma_(fj, r8.z, fma_(fi, r7.z, r6.z));
+        // Q = S (g0, g1, 0), R = wxy S[:,2]
+        const float Q0 = fma_(s00, g0, s01 * g1), Q1 = fma_(s01, g0, s11 * g1), Q2 = fma_(s02, g0, s12 * g1);
+        const float R0 = wxy * s02, R1 = wxy * s12, R2 = wxy * s22;
+        // P_k = wxy (A + k Bz) + Q
+        const float P00 = fma_(wxy, A0, Q0), P01 = fma_(wxy, A1, Q1), P02 = fma_(wxy, A2, Q2);
+        const float dz0 = wxy * r9.x, dz1 = wxy * r9.y, dz2 = wxy * r9.z;
+        const float P10 = P00 + dz0, P11 = P01 + dz1, P12 = P02 + dz2;
+        const float P20 = P10 + dz0, P21 = P11 + dz1, P22 = P12 + dz2;
+        am0 = fma_(r4.x, wm, am0); am1 = fma_(r4.y, wm, am1); am2 = fma_(r4.z, wm, am2);
+        ax0 = fma_(r4.x, P00, fma_(r5.x, R0, ax0)); ay0 = fma_(r4.x, P01, fma_(r5.x, R1, ay0)); az0 = fma_(r4.x, P02, fma_(r5.x, R2, az0));
+        ax1 = fma_(r4.y, P10, fma_(r5.y, R0, ax1)); ay1 = fma_(r4.y, P11, fma_(r5.y, R1, ay1)); az1 = fma_(r4.y, P12, fma_(r5.y, R2, az1));
+        ax2 = fma_(r4.z, P20, fma_(r5.z, R0, ax2)); ay2 = fma_(r4.z, P21, fma_(r5.z, R1, ay2)); az2 = fma_(r4.z, P22, fma_(r5.z, R2, az2));
+    }
+
+    // add the column's 3 nodes into the shared tile (or global memory)
+    template <class Shared>
+    __device__ __forceinline__ void emit(Shared &S, int k0, int ij, bool use_tile, int ox, int oy, int oz, int eyi,
+                                         int ezi, float4 *__restrict__ gmv, int nx, int ny, int nz, uint32_t &bad) const
+    {
+        const int i = ij / 3, j = ij - 3 * (ij / 3);
+        const int gx = S.base[0][k0] + i, gy = S.base[1][k0] + j, gz0 = S.base[2][k0];
+        const float4 c[3] = {make_float4(am0, ax0, ay0, az0), make_float4(am1, ax1, ay1, az1),
+                             make_float4(am2, ax2, ay2, az2)};
+        if (use_tile) {
+            const int tb = ((gx - ox) * eyi + (gy - oy)) * ezi + (gz0 - oz);
+#pragma unroll
+            for (int kk = 0; kk < 3; ++kk) {
+                atomicAdd(&S.tile[0][tb + kk], c[kk].x);
+                atomicAdd(&S.tile[1][tb + kk], c[kk].y);
+                atomicAdd(&S.tile[2][tb + kk], c[kk].z);
+                atomicAdd(&S.tile[3][tb + kk], c[kk].w);
+            }
+        } else {
+#pragma unroll
+            for (int kk = 0; kk < 3; ++kk) {
+                const int gz = gz0 + kk;
+                if (gx < 0 || gy < 0 || gz < 0 || gx >= nx || gy >= ny || gz >= nz) { bad |= MPMW_ST_OOB; continue; }
+                atomicAdd(&gmv[((int64_t)gx * ny + gy) * nz + gz], c[kk]);
+            }
+        }
+    }
+};
 
 // Every thread of the CTA must call this (it synchronizes the block).
 // xp: position; v: velocity; C: velocity gradient (row-major); st6: symmetric
@@ -119,6 +192,7 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
     int nseg;
     const int sidx = block_excl_scan(head ? 1 : 0, &nseg);
     if (head) S.seg_start[sidx] = t;
+    if (t < nact) S.seg_of[t] = head ? sidx : sidx - 1;
     if (t == 0) S.seg_start[nseg] = nact;
     const int ox = S.lo[0], oy = S.lo[1], oz = S.lo[2];
     const int64_t ex = (int64_t)S.hi[0] - ox + 3, ey = (int64_t)S.hi[1] - oy + 3, ez = (int64_t)S.hi[2] - oz + 3;
@@ -129,55 +203,51 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
     }
     __syncthreads();
 
-    for (int item = t; item < nseg * 9; item += kScatterChunk) {
-        const int s = item / 9, ij = item - 9 * s, i = ij / 3, j = ij - 3 * i;
-        const float fi = (float)i, fj = (float)j;
+    // Work: the pairs (stencil column ij = 3i + j of segment s, particle of s).
+    // Segment s (particles k0..k1-1, L = k1 - k0) owns pairs [9 k0, 9 k1), ordered
+    // by column, then particle; item q = 9 s + ij is one column of one segment.
+    // Complete passes over the threads take whole items (a thread sums its
+    // column's particles in registers and adds the 3 nodes once); the pairs of
+    // the items left over are then split evenly over all threads, each summing a
+    // contiguous run and adding a column whenever its run leaves one.
+    ColumnSums acc;
+    const int items = 9 * nseg;
+    const int full_items = (items / kScatterChunk) * kScatterChunk;
+    for (int q = t; q < full_items; q += kScatterChunk) {
+        const int s = q / 9, ij = q - 9 * s;
         const int k0 = S.seg_start[s], k1 = S.seg_start[s + 1];
-        float am0 = 0.f, am1 = 0.f, am2 = 0.f;
-        float ax0 = 0.f, ay0 = 0.f, az0 = 0.f, ax1 = 0.f, ay1 = 0.f, az1 = 0.f, ax2 = 0.f, ay2 = 0.f, az2 = 0.f;
-        for (int kq = k0; kq < k1; ++kq) {
-            const int q = scatter_slot(kq);
-            const float4 r0 = S.rec[0][q], r1 = S.rec[1][q], r2 = S.rec[2][q], r3 = S.rec[3][q], r4 = S.rec[4][q],
-                         r5 = S.rec[5][q], r6 = S.rec[6][q], r7 = S.rec[7][q], r8 = S.rec[8][q], r9 = S.rec[9][q];
-            const float wxi = sel3(r0, i), dwxi = sel3(r1, i), wyj = sel3(r2, j), dwyj = sel3(r3, j);
-            const float mm = r0.w;
-            const float s00 = r1.w, s11 = r2.w, s22 = r3.w, s01 = r4.w, s02 = r5.w, s12 = r6.w;
-            const float wxy = wxi * wyj, g0 = dwxi * wyj, g1 = wxi * dwyj, wm = wxy * mm;
-            // A = a + i Bx + j By
-            const float A0 = fma_(fj, r8.x, fma_(fi, r7.x, r6.x));
-            const float A1 = fma_(fj, r8.y, fma_(fi, r7.y, r6.y));
-            const float A2 = fma_(fj, r8.z, fma_(fi, r7.z, r6.z));
-            // Q = S (g0, g1, 0), R = wxy S[:,2]
-            const float Q0 = fma_(s00, g0, s01 * g1), Q1 = fma_(s01, g0, s11 * g1), Q2 = fma_(s02, g0, s12 * g1);
-            const float R0 = wxy * s02, R1 = wxy * s12, R2 = wxy * s22;
-            // P_k = wxy (A + k Bz) + Q
-            const float P00 = fma_(wxy, A0, Q0), P01 = fma_(wxy, A1, Q1), P02 = fma_(wxy, A2, Q2);
-            const float dz0 = wxy * r9.x, dz1 = wxy * r9.y, dz2 = wxy * r9.z;
-            const float P10 = P00 + dz0, P11 = P01 + dz1, P12 = P02 + dz2;
-            const float P20 = P10 + dz0, P21 = P11 + dz1, P22 = P12 + dz2;
-            am0 = fma_(r4.x, wm, am0); am1 = fma_(r4.y, wm, am1); am2 = fma_(r4.z, wm, am2);
-            ax0 = fma_(r4.x, P00, fma_(r5.x, R0, ax0)); ay0 = fma_(r4.x, P01, fma_(r5.x, R1, ay0)); az0 = fma_(r4.x, P02, fma_(r5.x, R2, az0));
-            ax1 = fma_(r4.y, P10, fma_(r5.y, R0, ax1)); ay1 = fma_(r4.y, P11, fma_(r5.y, R1, ay1)); az1 = fma_(r4.y, P12, fma_(r5.y, R2, az1));
-            ax2 = fma_(r4.z, P20, fma_(r5.z, R0, ax2)); ay2 = fma_(r4.z, P21, fma_(r5.z, R1, ay2)); az2 = fma_(r4.z, P22, fma_(r5.z, R2, az2));
-        }
-        const int gx = S.base[0][k0] + i, gy = S.base[1][k0] + j, gz0 = S.base[2][k0];
-        const float4 c[3] = {make_float4(am0, ax0, ay0, az0), make_float4(am1, ax1, ay1, az1),
-                             make_float4(am2, ax2, ay2, az2)};
-        if (use_tile) {
-            const int tb = ((gx - ox) * eyi + (gy - oy)) * ezi + (gz0 - oz);
-#pragma unroll
-            for (int kk = 0; kk < 3; ++kk) {
-                atomicAdd(&S.tile[0][tb + kk], c[kk].x);
-                atomicAdd(&S.tile[1][tb + kk], c[kk].y);
-                atomicAdd(&S.tile[2][tb + kk], c[kk].z);
-                atomicAdd(&S.tile[3][tb + kk], c[kk].w);
-            }
-        } else {
-#pragma unroll
-            for (int kk = 0; kk < 3; ++kk) {
-                const int gz = gz0 + kk;
-                if (gx < 0 || gy < 0 || gz < 0 || gx >= nx || gy >= ny || gz >= nz) { bad |= MPMW_ST_OOB; continue; }
-                atomicAdd(&gmv[((int64_t)gx * ny + gy) * nz + gz], c[kk]);
+        acc.zero();
+        for (int kq = k0; kq < k1; ++kq) acc.add(S, scatter_slot(kq), ij);
+        acc.emit(S, k0, ij, use_tile, ox, oy, oz, eyi, ezi, gmv, nx, ny, nz, bad);
+    }
+    if (full_items < items) {
+        const int s0 = full_items / 9, ij0 = full_items - 9 * s0;
+        const int pstart = 9 * S.seg_start[s0] + ij0 * (S.seg_start[s0 + 1] - S.seg_start[s0]);
+        const int total = 9 * nact;
+        const int per = (total - pstart + kScatterChunk - 1) / kScatterChunk;
+        int g = pstart + t * per;
+        const int gend = min(total, g + per);
+        if (g < gend) {
+            int s = S.seg_of[g / 9];
+            int k0 = S.seg_start[s], L = S.seg_start[s + 1] - k0;
+            int off = g - 9 * k0;
+            int ij = off / L, r = off - ij * L;
+            acc.zero();
+            for (; g < gend; ++g) {
+                acc.add(S, scatter_slot(k0 + r), ij);
+                ++r;
+                if (r == L || g + 1 == gend) {
+                    acc.emit(S, k0, ij, use_tile, ox, oy, oz, eyi, ezi, gmv, nx, ny, nz, bad);
+                    acc.zero();
+                }
+                if (r == L) {
+                    r = 0;
+                    if (++ij == 9) {
+                        ij = 0;
+                        ++s;
+                        if (s < nseg) { k0 = S.seg_start[s]; L = S.seg_start[s + 1] - k0; }
+                    }
+                }
             }
         }
     }
