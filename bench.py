@@ -377,8 +377,34 @@ def run_reference(a):
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+def run_profile_small(k):
+    """K substeps of a 788,160-particle tunnel (120x60x120 lattice cells, same
+    per-particle work as the bench workload) through mpmw_run_substeps, for
+    ncu captures that must stay small; prints one status line."""
+    import torch
+
+    from mpmwarpydw_b200 import _lib, domains
+    from mpmwarpydw_b200.bind import grid_from_state, params_from_states, particles_from_states, status_word, workspace
+    from mpmwarpydw_b200.engine import sort_particles
+    dev = torch.device("cuda", 0)
+    d = domains.tunnel(nx=120, ny=60, nz=120)
+    sim, mpm, xpbd = domains.build(d, device=dev)
+    sort_particles(sim, mpm, xpbd)
+    L = _lib.lib()
+    P, G, prm = particles_from_states(sim, mpm, xpbd), grid_from_state(mpm), params_from_states(sim, mpm)
+    ws = workspace(mpm, sim.nPoints, dev)
+    st = status_word(dev)
+    _lib.check(L.mpmw_run_substeps(P, G, prm, int(k), st.data_ptr(), ws.data_ptr(), ws.numel(),
+                                   torch.cuda.current_stream(dev).cuda_stream), "run_substeps")
+    torch.cuda.synchronize(dev)
+    print(json.dumps({"profile_small": {"particles": sim.nPoints, "grid": list(mpm.gridDims), "substeps": int(k),
+                                        "status_word": int(st.item())}}))
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--profile-small", type=int, default=0, metavar="K",
+                    help="run K substeps of the 788,160-particle tunnel and exit (small case for ncu)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=10)
@@ -389,7 +415,9 @@ def main():
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3
-    if a.impl == "reference":
+    if a.profile_small:
+        run_profile_small(a.profile_small)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)
