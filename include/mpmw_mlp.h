@@ -1,0 +1,70 @@
+/*
+ * mpmw_mlp.h -- C ABI of the learned return-map surrogate in libmpmw.so.
+ *
+ * No counterpart in the reference.  MPMWarpYDW's Drucker-Prager return map
+ * (utils/mpmRoutines.py:314-453) is closed form; this is an optional surrogate
+ * for the return of plastic trial states, with the plain map as the fallback.
+ *
+ * Network: 8 -> 64 -> 64 -> 64 -> 4, SiLU after each hidden layer.  Parameters
+ * are one FP32 array of MPMW_MLP_NPARAM floats in this order (row-major,
+ * W[out][in]): W1[64][8] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[4][64] b4[4].
+ *
+ * Features of a plastic trial state with principal log strains e (sorted
+ * descending), in units of the yield strain y = ys / (2 mu):
+ *   x = ( e/|e| (3), log10(|e| / y), alpha, beta, D, nu )
+ * Targets: ( (e_ret - e)/|e| (3), d_acc/|e| ), where e_ret are the returned
+ * principal log strains and d_acc the accumulated-plastic-strain increment.
+ *
+ * Conventions as in mpmw.h: device pointers, int status, stream-ordered, no
+ * allocation (callers pass scratch).
+ */
+#ifndef MPMW_MLP_H
+#define MPMW_MLP_H
+
+#include "mpmw.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPMW_MLP_IN 8
+#define MPMW_MLP_HID 64
+#define MPMW_MLP_OUT 4
+#define MPMW_MLP_NPARAM 9156
+/* bytes of the packed BF16 weights for the tensor-core inference kernel */
+#define MPMW_MLP_PACKED_BYTES 20480
+
+/* Training set: n labelled plastic trial states drawn as
+ *   |e| log-uniform in [1e-6, 1e-1], direction uniform on the sphere,
+ *   friction angle U(20, 45) deg -> alpha, dilation U(0, 10) deg -> beta,
+ *   cohesion log-uniform in [0.1, 5] MPa, E log-uniform in [1, 50] GPa,
+ *   nu U(0.15, 0.35), D U(0, 1),
+ * keeping only states whose trial is plastic; labels from the plain
+ * principal-space return map in double precision.  x: [n][8], y: [n][4]. */
+int mpmw_dp_samples(int64_t n, uint64_t seed, float *x, float *y, mpmw_stream_t stream);
+
+/* FP32 forward pass with the weights rounded to BF16 (biases FP32): y = f(x). */
+int mpmw_mlp_forward(const float *params, const float *x, int64_t n, float *y, mpmw_stream_t stream);
+
+/* Mean-squared-error loss over n samples and its gradient with respect to the
+ * FP32 parameters (straight-through through the BF16 rounding of the
+ * weights).  grad[MPMW_MLP_NPARAM] and loss[1] are overwritten. */
+int mpmw_mlp_grad(const float *params, const float *x, const float *y, int64_t n, float *grad, float *loss,
+                  mpmw_stream_t stream);
+
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8), step counts from 1. */
+int mpmw_mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr, mpmw_stream_t stream);
+
+/* Pack the FP32 weights as BF16 operand tiles for mpmw_mlp_infer_tc. */
+int mpmw_mlp_pack(const float *params, void *packed, mpmw_stream_t stream);
+
+/* Tensor-core inference (tcgen05.mma, BF16 operands, FP32 accumulators in
+ * tensor memory): y[n][4] = f(x[n][8]) with the packed weights and the FP32
+ * biases of `params`.  Bounded waits report MPMW_ST_TIMEOUT in *status. */
+int mpmw_mlp_infer_tc(const void *packed, const float *params, const float *x, int64_t n, float *y,
+                      uint32_t *status, mpmw_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPMW_MLP_H */

@@ -56,6 +56,8 @@ class Params(ctypes.Structure):
 
 STRESS_AUTO, STRESS_SVD = 0, 1
 
+MLP_IN, MLP_HID, MLP_OUT, MLP_NPARAM, MLP_PACKED_BYTES = 8, 64, 4, 9156, 20480
+
 
 class XPBD(ctypes.Structure):
     _fields_ = [("x_int", _P), ("v_int", _P), ("x_dI", _P), ("v_dI", _P), ("delta", _P), ("v_before", _P),
@@ -101,6 +103,12 @@ _SIGS = {
     "mpmw_teleport": (_I, [ctypes.POINTER(Particles), _F, _F, _P]),
     "mpmw_creep": (_I, [ctypes.POINTER(Particles), _P, _F, _F, _F, _F, _P]),
     "mpmw_stats": (_I, [ctypes.POINTER(Particles), _P, _P]),
+    "mpmw_dp_samples": (_I, [_I64, ctypes.c_uint64, _P, _P, _P]),
+    "mpmw_mlp_forward": (_I, [_P, _P, _I64, _P, _P]),
+    "mpmw_mlp_grad": (_I, [_P, _P, _P, _I64, _P, _P, _P]),
+    "mpmw_mlp_adam": (_I, [_P, _P, _P, _P, _I, _F, _P]),
+    "mpmw_mlp_pack": (_I, [_P, _P, _P]),
+    "mpmw_mlp_infer_tc": (_I, [_P, _P, _P, _I64, _P, _P, _P]),
     "mpmw_hash_workspace_bytes": (ctypes.c_size_t, [_I64]),
     "mpmw_hash_build": (_I, [_P, _I64, ctypes.POINTER(Hash), _P, ctypes.c_size_t, _P]),
     "mpmw_hash_build_noalloc": (_I, [_P, _I64, ctypes.POINTER(Hash), _P]),

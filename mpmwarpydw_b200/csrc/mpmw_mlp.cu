@@ -1,0 +1,624 @@
+// mpmw_mlp.cu -- learned surrogate of the Drucker-Prager return map: training
+// samples, FP32 training kernels (forward, backward, Adam) and tensor-core
+// inference (tcgen05.mma, BF16 operands, FP32 accumulators in tensor memory).
+//
+// The return map it learns is the reference's closed-form radial return in
+// principal log-strain space (utils/mpmRoutines.py:339-453):
+//   tau = 2 mu e + lam tr(e), p = tr(tau)/3, sigma_eq = |dev tau|,
+//   yield = (1 - D)(ys - alpha p); plastic if sigma_eq > yield,
+//   edn = |dev e| + 1e-6, dgamma = edn - yield / (2 mu), d_acc = sqrt(2/3) dgamma,
+//   e_ret = e - (dgamma / edn) dev e + beta dgamma.
+// Features and targets are defined in include/mpmw_mlp.h.
+#include <cuda_bf16.h>
+
+#include "mpmw_common.cuh"
+#include "mpmw_tma.cuh"
+#include "../../include/mpmw_mlp.h"
+
+namespace mpmw {
+namespace mlp {
+
+constexpr int IN = MPMW_MLP_IN, H = MPMW_MLP_HID, OUT = MPMW_MLP_OUT, NP = MPMW_MLP_NPARAM;
+constexpr int oW1 = 0, oB1 = oW1 + H * IN, oW2 = oB1 + H, oB2 = oW2 + H * H, oW3 = oB2 + H, oB3 = oW3 + H * H,
+              oW4 = oB3 + H, oB4 = oW4 + OUT * H;
+static_assert(oB4 + OUT == NP, "parameter packing");
+
+// ---------------------------------------------------------------------------
+// samples
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t splitmix(uint64_t &s)
+{
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ double u01(uint64_t &s) { return (double)(splitmix(s) >> 11) * (1.0 / 9007199254740992.0); }
+
+__device__ __forceinline__ double dp_alpha(double deg)
+{
+    const double sn = sin(deg * (3.14159265358979323846 / 180.0));
+    return 2.0 * sn / (sqrt(3.0) * (3.0 - sn));
+}
+
+// Plain principal-space return (double).  Returns 0 for an elastic trial, 1 for
+// a plastic return (e_ret, d_acc written), 2 when the reference would set D = 1
+// instead (ys < 0 or yield < 0).
+__device__ int dp_return(const double *e, double mu, double lam, double ys, double alpha, double beta, double D,
+                         double *er, double &dacc)
+{
+    const double tr = e[0] + e[1] + e[2];
+    const double mean = tr / 3.0;
+    const double ed[3] = {e[0] - mean, e[1] - mean, e[2] - mean};
+    double tau[3], p = 0.0;
+    for (int k = 0; k < 3; ++k) { tau[k] = 2.0 * mu * e[k] + lam * tr; p += tau[k]; }
+    p /= 3.0;
+    double seq = 0.0;
+    for (int k = 0; k < 3; ++k) seq += (tau[k] - p) * (tau[k] - p);
+    seq = sqrt(seq);
+    const double yield_eff = (1.0 - D) * (ys - alpha * p);
+    if (ys < 0.0 || yield_eff < 0.0) return 2;
+    if (!(seq > yield_eff)) return 0;
+    const double edn = sqrt(ed[0] * ed[0] + ed[1] * ed[1] + ed[2] * ed[2]) + 1e-6;
+    const double dg = edn - yield_eff / (2.0 * mu);
+    dacc = sqrt(2.0 / 3.0) * dg;
+    const double f = dg / edn, vc = beta * dg;
+    for (int k = 0; k < 3; ++k) er[k] = (e[k] - f * ed[k]) + vc;
+    return 1;
+}
+
+__global__ void k_dp_samples(int64_t n, uint64_t seed, float *__restrict__ x, float *__restrict__ y)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double e[3] = {0, 0, 0}, er[3] = {0, 0, 0}, dacc = 0.0, mag = 1e-6, yv = 1.0, alpha = 0, beta = 0, D = 0, nu = 0.25;
+    for (int attempt = 0; attempt < 64; ++attempt) {
+        uint64_t s = seed ^ (0xD1B54A32D192ED03ull * (uint64_t)(i + 1)) ^ ((uint64_t)attempt << 56);
+        mag = pow(10.0, -6.0 + 5.0 * u01(s));
+        // direction: normalized Gaussian (Box-Muller)
+        double g[3];
+        for (int k = 0; k < 3; k += 2) {
+            const double u1 = fmax(u01(s), 1e-300), u2 = u01(s);
+            const double r = sqrt(-2.0 * log(u1)), th = 6.283185307179586 * u2;
+            g[k] = r * cos(th);
+            if (k + 1 < 3) g[k + 1] = r * sin(th);
+        }
+        const double gn = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]) + 1e-300;
+        for (int k = 0; k < 3; ++k) e[k] = mag * g[k] / gn;
+        // sort descending
+        if (e[0] < e[1]) { double t = e[0]; e[0] = e[1]; e[1] = t; }
+        if (e[1] < e[2]) { double t = e[1]; e[1] = e[2]; e[2] = t; }
+        if (e[0] < e[1]) { double t = e[0]; e[0] = e[1]; e[1] = t; }
+        alpha = dp_alpha(20.0 + 25.0 * u01(s));
+        beta = dp_alpha(10.0 * u01(s));
+        const double ys = 1e5 * pow(50.0, u01(s));
+        const double E = 1e9 * pow(50.0, u01(s));
+        nu = 0.15 + 0.2 * u01(s);
+        D = u01(s);
+        const double mu = E / (2.0 * (1.0 + nu)), lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+        yv = ys / (2.0 * mu);
+        if (dp_return(e, mu, lam, ys, alpha, beta, D, er, dacc) == 1) break;
+        er[0] = e[0]; er[1] = e[1]; er[2] = e[2]; dacc = 0.0;  // elastic fallback after 64 attempts
+    }
+    float *xo = x + 8 * i, *yo = y + 4 * i;
+    xo[0] = (float)(e[0] / mag); xo[1] = (float)(e[1] / mag); xo[2] = (float)(e[2] / mag);
+    xo[3] = (float)log10(mag / yv);
+    xo[4] = (float)alpha; xo[5] = (float)beta; xo[6] = (float)D; xo[7] = (float)nu;
+    for (int k = 0; k < 3; ++k) yo[k] = (float)((er[k] - e[k]) / mag);
+    yo[3] = (float)(dacc / mag);
+}
+
+// ---------------------------------------------------------------------------
+// FP32 training kernels: a CTA holds a tile of kTile samples and all weights
+// (rounded to BF16) in shared memory.
+// ---------------------------------------------------------------------------
+constexpr int kTile = 64;
+constexpr int kThreads = 256;
+constexpr int kLd = H + 1;  // padded row stride of transposed weights (conflict-free both ways)
+
+struct TrainShared {
+    float w1t[IN][kLd], w2t[H][kLd], w3t[H][kLd], w4t[H][OUT + 1];
+    float b1[H], b2[H], b3[H], b4[OUT];
+    float x[kTile][IN];
+    float a1[kTile][H], a2[kTile][H], a3[kTile][H];     // activations
+    float d1[kTile][H], d2[kTile][H], d3[kTile][H];     // SiLU'(z)
+    float out[kTile][OUT];
+    float gz[kTile][H], ga[kTile][H];                   // backward scratch
+    float loss;
+};
+
+__device__ __forceinline__ float bf16r(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
+
+__device__ __forceinline__ void silu_pair(float z, float &a, float &d)
+{
+    const float s = 1.f / (1.f + expf(-z));
+    a = z * s;
+    d = s * (1.f + z * (1.f - s));
+}
+
+__device__ void load_weights(TrainShared &S, const float *__restrict__ P)
+{
+    for (int q = threadIdx.x; q < H * IN; q += blockDim.x) { int j = q / IN, k = q % IN; S.w1t[k][j] = bf16r(P[oW1 + q]); }
+    for (int q = threadIdx.x; q < H * H; q += blockDim.x) {
+        int j = q / H, k = q % H;
+        S.w2t[k][j] = bf16r(P[oW2 + q]);
+        S.w3t[k][j] = bf16r(P[oW3 + q]);
+    }
+    for (int q = threadIdx.x; q < OUT * H; q += blockDim.x) { int o = q / H, k = q % H; S.w4t[k][o] = bf16r(P[oW4 + q]); }
+    for (int q = threadIdx.x; q < H; q += blockDim.x) { S.b1[q] = P[oB1 + q]; S.b2[q] = P[oB2 + q]; S.b3[q] = P[oB3 + q]; }
+    if (threadIdx.x < OUT) S.b4[threadIdx.x] = P[oB4 + threadIdx.x];
+}
+
+// forward over the tile (rows >= rows_valid are zero inputs)
+__device__ void tile_forward(TrainShared &S)
+{
+    for (int q = threadIdx.x; q < kTile * H; q += blockDim.x) {
+        const int s = q / H, j = q % H;
+        float z = S.b1[j];
+#pragma unroll
+        for (int k = 0; k < IN; ++k) z = fmaf(S.x[s][k], S.w1t[k][j], z);
+        silu_pair(z, S.a1[s][j], S.d1[s][j]);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < kTile * H; q += blockDim.x) {
+        const int s = q / H, j = q % H;
+        float z = S.b2[j];
+        for (int k = 0; k < H; ++k) z = fmaf(S.a1[s][k], S.w2t[k][j], z);
+        silu_pair(z, S.a2[s][j], S.d2[s][j]);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < kTile * H; q += blockDim.x) {
+        const int s = q / H, j = q % H;
+        float z = S.b3[j];
+        for (int k = 0; k < H; ++k) z = fmaf(S.a2[s][k], S.w3t[k][j], z);
+        silu_pair(z, S.a3[s][j], S.d3[s][j]);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < kTile * OUT; q += blockDim.x) {
+        const int s = q / OUT, o = q % OUT;
+        float z = S.b4[o];
+        for (int k = 0; k < H; ++k) z = fmaf(S.a3[s][k], S.w4t[k][o], z);
+        S.out[s][o] = z;
+    }
+    __syncthreads();
+}
+
+__device__ void load_x(TrainShared &S, const float *__restrict__ X, int64_t row0, int64_t n)
+{
+    for (int q = threadIdx.x; q < kTile * IN; q += blockDim.x) {
+        const int s = q / IN, k = q % IN;
+        const int64_t r = row0 + s;
+        S.x[s][k] = r < n ? X[r * IN + k] : 0.f;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_mlp_forward(const float *__restrict__ P, const float *__restrict__ X,
+                                                          int64_t n, float *__restrict__ Y)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TrainShared &S = *reinterpret_cast<TrainShared *>(smem_raw);
+    const int64_t row0 = (int64_t)blockIdx.x * kTile;
+    load_weights(S, P);
+    load_x(S, X, row0, n);
+    __syncthreads();
+    tile_forward(S);
+    for (int q = threadIdx.x; q < kTile * OUT; q += blockDim.x) {
+        const int s = q / OUT, o = q % OUT;
+        if (row0 + s < n) Y[(row0 + s) * OUT + o] = S.out[s][o];
+    }
+}
+
+// gradient of mean((out - y)^2) over all n*OUT entries
+__global__ void __launch_bounds__(kThreads) k_mlp_grad(const float *__restrict__ P, const float *__restrict__ X,
+                                                       const float *__restrict__ Yt, int64_t n, float *__restrict__ G,
+                                                       float *__restrict__ loss)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TrainShared &S = *reinterpret_cast<TrainShared *>(smem_raw);
+    const int64_t row0 = (int64_t)blockIdx.x * kTile;
+    const int rows = n - row0 < (int64_t)kTile ? (int)(n - row0) : kTile;
+    load_weights(S, P);
+    load_x(S, X, row0, n);
+    if (threadIdx.x == 0) S.loss = 0.f;
+    __syncthreads();
+    tile_forward(S);
+    const float inv = 2.f / (float)((double)n * OUT);
+    // d out (stored in gz[:, 0..3])
+    float lsum = 0.f;
+    for (int q = threadIdx.x; q < kTile * OUT; q += blockDim.x) {
+        const int s = q / OUT, o = q % OUT;
+        float d = 0.f;
+        if (s < rows) {
+            const float r = S.out[s][o] - Yt[(row0 + s) * OUT + o];
+            lsum += r * r;
+            d = inv * r;
+        }
+        S.gz[s][o] = d;
+    }
+    atomicAdd(&S.loss, lsum);
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(loss, S.loss / (float)((double)n * OUT));
+    // layer 4: weights and bias, and d a3
+    for (int q = threadIdx.x; q < OUT * H; q += blockDim.x) {
+        const int o = q / H, k = q % H;
+        float gw = 0.f;
+        for (int s = 0; s < kTile; ++s) gw = fmaf(S.gz[s][o], S.a3[s][k], gw);
+        atomicAdd(&G[oW4 + q], gw);
+    }
+    if (threadIdx.x < OUT) {
+        float gb = 0.f;
+        for (int s = 0; s < kTile; ++s) gb += S.gz[s][threadIdx.x];
+        atomicAdd(&G[oB4 + threadIdx.x], gb);
+    }
+    for (int q = threadIdx.x; q < kTile * H; q += blockDim.x) {
+        const int s = q / H, k = q % H;
+        float da = 0.f;
+#pragma unroll
+        for (int o = 0; o < OUT; ++o) da = fmaf(S.gz[s][o], S.w4t[k][o], da);
+        S.ga[s][k] = da * S.d3[s][k];  // d z3
+    }
+    __syncthreads();
+    // layer 3
+    for (int q = threadIdx.x; q < H * H; q += blockDim.x) {
+        const int j = q / H, k = q % H;
+        float gw = 0.f;
+        for (int s = 0; s < kTile; ++s) gw = fmaf(S.ga[s][j], S.a2[s][k], gw);
+        atomicAdd(&G[oW3 + q], gw);
+    }
+    if (threadIdx.x < H) {
+        float gb = 0.f;
+        for (int s = 0; s < kTile; ++s) gb += S.ga[s][threadIdx.x];
+        atomicAdd(&G[oB3 + threadIdx.x], gb);
+    }
+    for (int q = threadIdx.x; q < kTile * H; q += blockDim.x) {
+        const int s = q / H, k = q % H;
+        float da = 0.f;
+        for (int j = 0; j < H; ++j) da = fmaf(S.ga[s][j], S.w3t[k][j], da);
+        S.gz[s][k] = da * S.d2[s][k];  // d z2
+    }
+    __syncthreads();
+    // layer 2
+    for (int q = threadIdx.x; q < H * H; q += blockDim.x) {
+        const int j = q / H, k = q % H;
+        float gw = 0.f;
+        for (int s = 0; s < kTile; ++s) gw = fmaf(S.gz[s][j], S.a1[s][k], gw);
+        atomicAdd(&G[oW2 + q], gw);
+    }
+    if (threadIdx.x < H) {
+        float gb = 0.f;
+        for (int s = 0; s < kTile; ++s) gb += S.gz[s][threadIdx.x];
+        atomicAdd(&G[oB2 + threadIdx.x], gb);
+    }
+    for (int q = threadIdx.x; q < kTile * H; q += blockDim.x) {
+        const int s = q / H, k = q % H;
+        float da = 0.f;
+        for (int j = 0; j < H; ++j) da = fmaf(S.gz[s][j], S.w2t[k][j], da);
+        S.ga[s][k] = da * S.d1[s][k];  // d z1
+    }
+    __syncthreads();
+    // layer 1
+    for (int q = threadIdx.x; q < H * IN; q += blockDim.x) {
+        const int j = q / IN, k = q % IN;
+        float gw = 0.f;
+        for (int s = 0; s < kTile; ++s) gw = fmaf(S.ga[s][j], S.x[s][k], gw);
+        atomicAdd(&G[oW1 + q], gw);
+    }
+    if (threadIdx.x < H) {
+        float gb = 0.f;
+        for (int s = 0; s < kTile; ++s) gb += S.ga[s][threadIdx.x];
+        atomicAdd(&G[oB1 + threadIdx.x], gb);
+    }
+}
+
+__global__ void k_mlp_adam(float *__restrict__ P, const float *__restrict__ G, float *__restrict__ M,
+                           float *__restrict__ V, float lr, float c1, float c2)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= NP) return;
+    const float g = G[q];
+    const float m = 0.9f * M[q] + 0.1f * g;
+    const float v = 0.999f * V[q] + 0.001f * g * g;
+    M[q] = m;
+    V[q] = v;
+    P[q] -= lr * (m / c1) / (sqrtf(v / c2) + 1e-8f);
+}
+
+// ---------------------------------------------------------------------------
+// tensor-core inference
+// ---------------------------------------------------------------------------
+// Operand tiles in shared memory use the canonical K-major layout without
+// swizzle: 8x8 BF16 core matrices of 128 contiguous bytes (8 rows of 16 bytes);
+// the core matrix (row block rb, k block kb) of an R x K tile sits at
+// (rb * K/8 + kb) * 128 bytes.  Descriptor: leading (K-direction) byte offset
+// 128, stride (row-direction) byte offset K/8 * 128.
+constexpr int kTcRows = 128;                 // M of every MMA (one row per thread)
+constexpr int kPackW1 = 0, kPackW2 = 2048, kPackW3 = 2048 + 8192, kPackW4 = 2048 + 2 * 8192;
+static_assert(kPackW4 + 2048 == MPMW_MLP_PACKED_BYTES, "packed size");
+
+__host__ __device__ __forceinline__ int core_offset(int r, int k, int K)
+{
+    return ((r >> 3) * (K >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2;
+}
+
+__global__ void k_mlp_pack(const float *__restrict__ P, __nv_bfloat16 *__restrict__ W)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned char *base = reinterpret_cast<unsigned char *>(W);
+    auto put = [&](int off, int r, int k, int K, float v) {
+        *reinterpret_cast<__nv_bfloat16 *>(base + off + core_offset(r, k, K)) = __float2bfloat16_rn(v);
+    };
+    if (q < H * 16) {  // W1: 64 x 16 (inputs 8..15 zero)
+        const int r = q / 16, k = q % 16;
+        put(kPackW1, r, k, 16, k < IN ? P[oW1 + r * IN + k] : 0.f);
+    }
+    if (q < H * H) {
+        const int r = q / H, k = q % H;
+        put(kPackW2, r, k, H, P[oW2 + q]);
+        put(kPackW3, r, k, H, P[oW3 + q]);
+    }
+    if (q < 16 * H) {  // W4: 16 x 64 (outputs 4..15 zero)
+        const int r = q / H, k = q % H;
+        put(kPackW4, r, k, H, r < OUT ? P[oW4 + r * H + k] : 0.f);
+    }
+}
+
+struct TcShared {
+    unsigned char w[MPMW_MLP_PACKED_BYTES];   // B operands
+    unsigned char a[kTcRows * H * 2];         // A operand (activations)
+    float bias[3 * H + OUT];
+    uint64_t bar;
+    uint32_t tmem;
+    int timeout;
+};
+
+__device__ __forceinline__ uint64_t smem_desc(const void *p, uint32_t lbo, uint32_t sbo)
+{
+    const uint64_t a = smem_addr(p);
+    return ((a & 0x3FFFFull) >> 4) | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ uint32_t idesc_bf16(int N)
+{
+    // F32 accumulate, BF16 A and B, both K-major, N/8, M/16 (M = 128)
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kTcRows >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t id, int acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+        "l"(ad), "l"(bd), "r"(id), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 16 consecutive FP32 accumulator columns of this thread's row
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float *v)
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// write this thread's row of 64 BF16 activations into the K = 64 A tile
+__device__ __forceinline__ void put_row64(unsigned char *a, int r, const float *h)
+{
+#pragma unroll
+    for (int kb = 0; kb < 8; ++kb) {
+        __nv_bfloat162 v[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) v[c] = __floats2bfloat162_rn(h[8 * kb + 2 * c], h[8 * kb + 2 * c + 1]);
+        *reinterpret_cast<uint4 *>(a + core_offset(r, 8 * kb, H)) = *reinterpret_cast<uint4 *>(v);
+    }
+}
+
+__global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const unsigned char *__restrict__ packed,
+                                                          const float *__restrict__ P, const float *__restrict__ X,
+                                                          int64_t n, float *__restrict__ Y, uint32_t *status)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    TcShared &S = *reinterpret_cast<TcShared *>(smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u));
+    const int t = threadIdx.x, warp = t >> 5;
+    const int64_t row = (int64_t)blockIdx.x * kTcRows + t;
+    // weights and biases
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(packed);
+        uint4 *dst = reinterpret_cast<uint4 *>(S.w);
+        for (int q = t; q < MPMW_MLP_PACKED_BYTES / 16; q += kTcRows) dst[q] = src[q];
+        for (int q = t; q < H; q += kTcRows) {
+            S.bias[q] = P[oB1 + q];
+            S.bias[H + q] = P[oB2 + q];
+            S.bias[2 * H + q] = P[oB3 + q];
+        }
+        if (t < OUT) S.bias[3 * H + t] = P[oB4 + t];
+    }
+    // layer-1 operand: this row's 8 features, K padded to 16
+    {
+        float f[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) f[k] = 0.f;
+        if (row < n) {
+#pragma unroll
+            for (int k = 0; k < IN; ++k) f[k] = X[row * IN + k];
+        }
+#pragma unroll
+        for (int kb = 0; kb < 2; ++kb) {
+            __nv_bfloat162 v[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) v[c] = __floats2bfloat162_rn(f[8 * kb + 2 * c], f[8 * kb + 2 * c + 1]);
+            *reinterpret_cast<uint4 *>(S.a + core_offset(t, 8 * kb, 16)) = *reinterpret_cast<uint4 *>(v);
+        }
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&S.tmem)),
+                     "r"(64)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (t == 0) { mbar_init(&S.bar, 1); S.timeout = 0; }
+    proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = S.tmem;
+    const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
+    unsigned phase = 0;
+    float h[H];
+    for (int layer = 0; layer < 4; ++layer) {
+        const int K = layer == 0 ? 16 : H;
+        const int N = layer == 3 ? 16 : H;
+        if (t == 0 && !S.timeout) {
+            tc_fence_after();
+            const unsigned char *w = S.w + (layer == 0 ? kPackW1 : layer == 1 ? kPackW2 : layer == 2 ? kPackW3 : kPackW4);
+            const uint32_t id = idesc_bf16(N);
+            for (int kk = 0; kk < K / 16; ++kk) {
+                const uint64_t ad = smem_desc(S.a + kk * 256, 128, (K / 8) * 128);
+                const uint64_t bd = smem_desc(w + kk * 256, 128, (K / 8) * 128);
+                tc_mma(tmem, ad, bd, id, kk > 0);
+            }
+            tc_commit(&S.bar);
+        }
+        if (!mbar_wait_bounded(&S.bar, phase)) {
+            S.timeout = 1;
+            raise_status(status, MPMW_ST_TIMEOUT);
+        }
+        phase ^= 1u;
+        tc_fence_after();
+        // accumulators of this thread's row
+        for (int c = 0; c < N; c += 16) tc_ld16(lane_addr + (uint32_t)c, h + c);
+        tc_wait_ld();
+        if (layer < 3) {
+            const float *b = S.bias + layer * H;
+#pragma unroll
+            for (int j = 0; j < H; ++j) {
+                const float z = h[j] + b[j];
+                h[j] = z / (1.f + expf(-z));
+            }
+            put_row64(S.a, t, h);
+            proxy_fence();
+            tc_fence_before();
+            __syncthreads();
+        } else if (row < n) {
+#pragma unroll
+            for (int o = 0; o < OUT; ++o) Y[row * OUT + o] = h[o] + S.bias[3 * H + o];
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64) : "memory");
+    }
+}
+
+}  // namespace mlp
+}  // namespace mpmw
+
+using namespace mpmw;
+using namespace mpmw::mlp;
+
+static bool g_mlp_attr[64];
+
+static int set_smem_attrs()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { set_error("mlp: no current device"); return MPMW_E_DEVICE; }
+    if (dev >= 0 && dev < 64 && !g_mlp_attr[dev]) {
+        const int ts = (int)sizeof(TrainShared), tc = (int)sizeof(TcShared) + 1024;
+        if (cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, ts) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, ts) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc) != cudaSuccess) {
+            set_error("mlp: cannot reserve shared memory");
+            return MPMW_E_DEVICE;
+        }
+        g_mlp_attr[dev] = true;
+    }
+    return MPMW_OK;
+}
+
+extern "C" {
+
+int mpmw_dp_samples(int64_t n, uint64_t seed, float *x, float *y, mpmw_stream_t stream)
+{
+    if (n < 0 || (n > 0 && (!x || !y))) { set_error("dp_samples: bad arguments"); return MPMW_E_ARG; }
+    if (n == 0) return MPMW_OK;
+    k_dp_samples<<<grid_for(n), kBlock, 0, as_stream(stream)>>>(n, seed, x, y);
+    return check_launch("k_dp_samples");
+}
+
+int mpmw_mlp_forward(const float *params, const float *x, int64_t n, float *y, mpmw_stream_t stream)
+{
+    if (!params || n < 0 || (n > 0 && (!x || !y))) { set_error("mlp_forward: bad arguments"); return MPMW_E_ARG; }
+    if (n == 0) return MPMW_OK;
+    { int rc_ = set_smem_attrs(); if (rc_ != MPMW_OK) return rc_; }
+    const unsigned g = (unsigned)((n + kTile - 1) / kTile);
+    k_mlp_forward<<<g, kThreads, sizeof(TrainShared), as_stream(stream)>>>(params, x, n, y);
+    return check_launch("k_mlp_forward");
+}
+
+int mpmw_mlp_grad(const float *params, const float *x, const float *y, int64_t n, float *grad, float *loss,
+                  mpmw_stream_t stream)
+{
+    if (!params || !grad || !loss || n <= 0 || !x || !y) { set_error("mlp_grad: bad arguments"); return MPMW_E_ARG; }
+    { int rc_ = set_smem_attrs(); if (rc_ != MPMW_OK) return rc_; }
+    cudaStream_t s = as_stream(stream);
+    if (cudaMemsetAsync(grad, 0, NP * sizeof(float), s) != cudaSuccess ||
+        cudaMemsetAsync(loss, 0, sizeof(float), s) != cudaSuccess) {
+        set_error("mlp_grad: memset failed");
+        return MPMW_E_DEVICE;
+    }
+    const unsigned g = (unsigned)((n + kTile - 1) / kTile);
+    k_mlp_grad<<<g, kThreads, sizeof(TrainShared), s>>>(params, x, y, n, grad, loss);
+    return check_launch("k_mlp_grad");
+}
+
+int mpmw_mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr, mpmw_stream_t stream)
+{
+    if (!params || !grad || !m || !v || step < 1) { set_error("mlp_adam: bad arguments"); return MPMW_E_ARG; }
+    const float c1 = 1.f - powf(0.9f, (float)step), c2 = 1.f - powf(0.999f, (float)step);
+    k_mlp_adam<<<(NP + 255) / 256, 256, 0, as_stream(stream)>>>(params, grad, m, v, lr, c1, c2);
+    return check_launch("k_mlp_adam");
+}
+
+int mpmw_mlp_pack(const float *params, void *packed, mpmw_stream_t stream)
+{
+    if (!params || !packed) { set_error("mlp_pack: bad arguments"); return MPMW_E_ARG; }
+    if ((reinterpret_cast<uintptr_t>(packed) & 15u) != 0) { set_error("mlp_pack: packed must be 16-byte aligned"); return MPMW_E_ARG; }
+    cudaStream_t s = as_stream(stream);
+    if (cudaMemsetAsync(packed, 0, MPMW_MLP_PACKED_BYTES, s) != cudaSuccess) { set_error("mlp_pack: memset failed"); return MPMW_E_DEVICE; }
+    k_mlp_pack<<<(H * H + 255) / 256, 256, 0, s>>>(params, reinterpret_cast<__nv_bfloat16 *>(packed));
+    return check_launch("k_mlp_pack");
+}
+
+int mpmw_mlp_infer_tc(const void *packed, const float *params, const float *x, int64_t n, float *y,
+                      uint32_t *status, mpmw_stream_t stream)
+{
+    if (!packed || !params || n < 0 || (n > 0 && (!x || !y))) { set_error("mlp_infer_tc: bad arguments"); return MPMW_E_ARG; }
+    if ((reinterpret_cast<uintptr_t>(packed) & 15u) != 0) { set_error("mlp_infer_tc: packed must be 16-byte aligned"); return MPMW_E_ARG; }
+    if (n == 0) return MPMW_OK;
+    { int rc_ = set_smem_attrs(); if (rc_ != MPMW_OK) return rc_; }
+    const unsigned g = (unsigned)((n + kTcRows - 1) / kTcRows);
+    k_mlp_infer_tc<<<g, kTcRows, sizeof(TcShared) + 1024, as_stream(stream)>>>(
+        static_cast<const unsigned char *>(packed), params, x, n, y, status);
+    return check_launch("k_mlp_infer_tc");
+}
+
+}  // extern "C"
