@@ -250,6 +250,8 @@ def run_ours(a):
         "status_word": status,
         "clocks": clocks.summary(),
     }
+    if world == 1 and not a.no_surrogate:
+        out["surrogate"] = surrogate_comparison(sim, mpm, xpbd, dev)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(a)
     if rank == 0:
@@ -257,6 +259,74 @@ def run_ours(a):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def surrogate_comparison(sim, mpm, xpbd, dev, reps=10):
+    """Plain vs learned return map in the stress phase on the bench state (after
+    the timed substeps): the surrogate network is trained on the GPU first
+    (seeded, timed separately), then each stress phase runs `reps` times from
+    the same restored state, timed with CUDA events."""
+    import torch
+
+    from mpmwarpydw_b200 import _lib
+    from mpmwarpydw_b200.bind import params_from_states, particles_from_states, status_word
+    from mpmwarpydw_b200.surrogate import ReturnMapSurrogate, compute_stress, stats_summary
+    stream = torch.cuda.current_stream(dev)
+    t0 = time.perf_counter()
+    net = ReturnMapSurrogate(dev, seed=0)
+    x, y = net.samples(4_000_000, 1)
+    losses = net.train(x, y, steps=20000, batch=16384)
+    torch.cuda.synchronize(dev)
+    train_s = time.perf_counter() - t0
+    del x, y
+    tensors = _state_tensors(sim, mpm, xpbd)
+    snap = [t.clone() for t in tensors]
+
+    def restore():
+        for t, s0 in zip(tensors, snap):
+            t.copy_(s0)
+
+    L = _lib.lib()
+    P, prm = particles_from_states(sim, mpm, xpbd), params_from_states(sim, mpm)
+    st = status_word(dev).data_ptr()
+    stress = mpm._s_particle_stress
+    acc = mpm._s_particle_accumulated_strain
+
+    def timed(fn):
+        ts = []
+        for r in range(reps + 2):
+            restore()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            if r >= 2:
+                ts.append(e0.elapsed_time(e1))
+        return sorted(ts)[len(ts) // 2]
+
+    ms_plain = timed(lambda: _lib.check(L.mpmw_stress(P, prm, st, stream.cuda_stream), "stress"))
+    s_plain, acc_plain = stress.clone(), acc.clone()
+    stats = torch.zeros(6, dtype=torch.int32, device=dev)
+
+    def surr():
+        stats.zero_()
+        compute_stress(sim, mpm, xpbd, net, gate_tol=1e-3, audit=1.0, audit_seed=7, stats=stats)
+
+    ms_surr = timed(surr)
+    s_surr = stress.clone()
+    plastic = acc_plain > snap[[i for i, t in enumerate(tensors) if t.data_ptr() == acc.data_ptr()][0]]
+    d = (s_surr - s_plain)[:, plastic]
+    ref = s_plain[:, plastic]
+    err = float(torch.linalg.norm(d.double()) / torch.linalg.norm(ref.double()).clamp_min(1e-30)) if ref.numel() else 0.0
+    restore()
+    n = sim.nPoints
+    summ = stats_summary(stats)
+    return {"stress_phase_plain": n / (ms_plain * 1e-3), "stress_phase_surrogate": n / (ms_surr * 1e-3),
+            "unit": "particle-updates/s", "speedup": ms_plain / ms_surr, "plastic_particles": int(plastic.sum().item()),
+            **summ, "stress_err_vs_plain_over_plastic": err, "gate_tol": 1e-3, "audit_fraction": 1.0,
+            "train_seconds": train_s, "train_loss_first_last": [losses[0], losses[-1]],
+            "network": "8-64-64-64-4 SiLU, BF16 tcgen05 inference, FP32 accumulate"}
 
 
 def load_traffic(kernel):
@@ -412,6 +482,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=250_000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the plain-vs-learned return map comparison")
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3

@@ -36,7 +36,9 @@ extern "C" {
 
 /* Training set: n labelled plastic trial states drawn as
  *   |e| log-uniform in [1e-6, 1e-1], direction uniform on the sphere,
- *   friction angle U(20, 45) deg -> alpha, dilation U(0, 10) deg -> beta,
+ *   friction angle U(20, 45) deg -> alpha; beta = 0.3 alpha (the reference's
+ *   dilation, utils/mpmRoutines.py:424) for half the samples, else a dilation
+ *   angle U(0, 10) deg -> beta;
  *   cohesion log-uniform in [0.1, 5] MPa, E log-uniform in [1, 50] GPa,
  *   nu U(0.15, 0.35), D U(0, 1),
  * keeping only states whose trial is plastic; labels from the plain
@@ -63,6 +65,25 @@ int mpmw_mlp_pack(const float *params, void *packed, mpmw_stream_t stream);
  * biases of `params`.  Bounded waits report MPMW_ST_TIMEOUT in *status. */
 int mpmw_mlp_infer_tc(const void *packed, const float *params, const float *x, int64_t n, float *y,
                       uint32_t *status, mpmw_stream_t stream);
+
+/* Workspace bytes of mpmw_stress_surrogate for n particles. */
+size_t mpmw_surrogate_workspace_bytes(int64_t n);
+
+/* The stress phase (utils/mpmRoutines.py:229-312) with the surrogate for the
+ * return of plastic trial states.  Particles outside the tensor form's range,
+ * elastic trials and trials that set D = 1 are computed exactly as mpmw_stress
+ * (MPMW_STRESS_AUTO).  A surrogate return is accepted only if its yield
+ * residual, flow-rule magnitude and volumetric part each agree with the return
+ * identities within gate_tol (relative); otherwise the exact closed form is
+ * used.  audit_per_mille of the surrogate's returns (chosen by a hash of the
+ * particle index and audit_seed; audited before the gate) are compared with
+ * the exact return.  stats (device, 6 x uint32, accumulated; the caller zeroes
+ * it): surrogate candidates, gate fallbacks, audited, largest audited relative
+ * stress error (float bits), sum of audited relative errors (float bits),
+ * audited within 1e-3. */
+int mpmw_stress_surrogate(const mpmw_particles_t *p, const mpmw_params_t *prm, const void *packed,
+                          const float *mlp_params, float gate_tol, int audit_per_mille, uint64_t audit_seed,
+                          uint32_t *stats, uint32_t *status, void *workspace, size_t ws_bytes, mpmw_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -109,6 +109,9 @@ _SIGS = {
     "mpmw_mlp_adam": (_I, [_P, _P, _P, _P, _I, _F, _P]),
     "mpmw_mlp_pack": (_I, [_P, _P, _P]),
     "mpmw_mlp_infer_tc": (_I, [_P, _P, _P, _I64, _P, _P, _P]),
+    "mpmw_surrogate_workspace_bytes": (ctypes.c_size_t, [_I64]),
+    "mpmw_stress_surrogate": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Params), _P, _P, _F, _I,
+                                   ctypes.c_uint64, _P, _P, _P, ctypes.c_size_t, _P]),
     "mpmw_hash_workspace_bytes": (ctypes.c_size_t, [_I64]),
     "mpmw_hash_build": (_I, [_P, _I64, ctypes.POINTER(Hash), _P, ctypes.c_size_t, _P]),
     "mpmw_hash_build_noalloc": (_I, [_P, _I64, ctypes.POINTER(Hash), _P]),

@@ -100,6 +100,31 @@ __device__ __forceinline__ void sort_cols(float *lam, float *V)
     }
 }
 
+// Eigen-decomposition of a symmetric 3x3 A (row-major, full): A = Q diag(lam) Q^T,
+// lam in decreasing order, Q a rotation (cyclic Jacobi, as in svd3).
+__device__ __forceinline__ void sym_eigen3(const float *A, float *lam, float *Q)
+{
+    float S[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) S[k] = A[k];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Q[k] = 0.f;
+    Q[0] = Q[4] = Q[8] = 1.f;
+#pragma unroll 1
+    for (int sw = 0; sw < kSvdMaxSweeps; ++sw) {
+        bool r0 = jacobi_rot<0, 1>(S, Q);
+        bool r1 = jacobi_rot<0, 2>(S, Q);
+        bool r2 = jacobi_rot<1, 2>(S, Q);
+        if (!(r0 || r1 || r2)) break;
+    }
+    lam[0] = S[0]; lam[1] = S[4]; lam[2] = S[8];
+    sort_cols<0, 1>(lam, Q);
+    sort_cols<0, 2>(lam, Q);
+    sort_cols<1, 2>(lam, Q);
+    float detQ = (Q[0] * (Q[4] * Q[8] - Q[5] * Q[7]) - Q[1] * (Q[3] * Q[8] - Q[5] * Q[6])) + Q[2] * (Q[3] * Q[7] - Q[4] * Q[6]);
+    if (detQ < 0.f) { Q[2] = -Q[2]; Q[5] = -Q[5]; Q[8] = -Q[8]; }
+}
+
 __device__ __forceinline__ void svd3(const float *F, float *U, float *sig, float *V)
 {
     float S[9];

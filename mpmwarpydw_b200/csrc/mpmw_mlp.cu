@@ -91,7 +91,9 @@ __global__ void k_dp_samples(int64_t n, uint64_t seed, float *__restrict__ x, fl
         if (e[1] < e[2]) { double t = e[1]; e[1] = e[2]; e[2] = t; }
         if (e[0] < e[1]) { double t = e[0]; e[0] = e[1]; e[1] = t; }
         alpha = dp_alpha(20.0 + 25.0 * u01(s));
-        beta = dp_alpha(10.0 * u01(s));
+        // half the samples use the reference's fixed dilation beta = 0.3 alpha
+        // (utils/mpmRoutines.py:424), half a dilation angle U(0, 10) deg
+        beta = u01(s) < 0.5 ? 0.3 * alpha : dp_alpha(10.0 * u01(s));
         const double ys = 1e5 * pow(50.0, u01(s));
         const double E = 1e9 * pow(50.0, u01(s));
         nu = 0.15 + 0.2 * u01(s);
@@ -430,10 +432,15 @@ __device__ __forceinline__ void put_row64(unsigned char *a, int r, const float *
     }
 }
 
+// n_dev (optional): a device count that lowers n (a worklist filled by an
+// earlier kernel); CTAs past it exit before touching tensor memory.
 __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const unsigned char *__restrict__ packed,
                                                           const float *__restrict__ P, const float *__restrict__ X,
-                                                          int64_t n, float *__restrict__ Y, uint32_t *status)
+                                                          int64_t n, float *__restrict__ Y, uint32_t *status,
+                                                          const int *__restrict__ n_dev)
 {
+    if (n_dev) n = min(n, (int64_t)*n_dev);
+    if ((int64_t)blockIdx.x * kTcRows >= n) return;  // uniform
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     TcShared &S = *reinterpret_cast<TcShared *>(smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u));
     const int t = threadIdx.x, warp = t >> 5;
@@ -617,8 +624,26 @@ int mpmw_mlp_infer_tc(const void *packed, const float *params, const float *x, i
     { int rc_ = set_smem_attrs(); if (rc_ != MPMW_OK) return rc_; }
     const unsigned g = (unsigned)((n + kTcRows - 1) / kTcRows);
     k_mlp_infer_tc<<<g, kTcRows, sizeof(TcShared) + 1024, as_stream(stream)>>>(
-        static_cast<const unsigned char *>(packed), params, x, n, y, status);
+        static_cast<const unsigned char *>(packed), params, x, n, y, status, nullptr);
     return check_launch("k_mlp_infer_tc");
 }
+
+}  // extern "C"
+
+namespace mpmw {
+// the inference kernel over a worklist whose length is on the device
+int launch_mlp_infer_tc_dev(const void *packed, const float *params, const float *x, int64_t n_max, const int *n_dev,
+                            float *y, uint32_t *status, cudaStream_t s)
+{
+    if (n_max <= 0) return MPMW_OK;
+    { int rc_ = set_smem_attrs(); if (rc_ != MPMW_OK) return rc_; }
+    const unsigned g = (unsigned)((n_max + mlp::kTcRows - 1) / mlp::kTcRows);
+    mlp::k_mlp_infer_tc<<<g, mlp::kTcRows, sizeof(mlp::TcShared) + 1024, s>>>(
+        static_cast<const unsigned char *>(packed), params, x, n_max, y, status, n_dev);
+    return check_launch("k_mlp_infer_tc");
+}
+}  // namespace mpmw
+
+extern "C" {
 
 }  // extern "C"

@@ -16,7 +16,7 @@ import math
 import torch
 
 from . import _lib
-from .bind import status_word, stream_handle
+from .bind import params_from_states, particles_from_states, status_word, stream_handle
 
 OFFSETS = dict(W1=(0, (64, 8)), b1=(512, (64,)), W2=(576, (64, 64)), b2=(4672, (64,)), W3=(4736, (64, 64)),
                b3=(8832, (64,)), W4=(8896, (4, 64)), b4=(9152, (4,)))
@@ -107,3 +107,41 @@ class ReturnMapSurrogate:
         self.params.copy_(d["params"].to(self.device))
         self.step = int(d.get("step", 0))
         self._packed_step = -1
+
+
+def compute_stress(sim, mpm, xpbd, net: ReturnMapSurrogate, gate_tol: float = 1e-3, audit: float = 0.01,
+                   audit_seed: int = 0, stats=None):
+    """The stress phase (compute_stress_from_F_trial) with the surrogate for
+    plastic returns: gate, audit and exact fallback as mpmw_stress_surrogate.
+    Returns the (6,) int32 device stats (see :func:`stats_summary`),
+    accumulated into ``stats``."""
+    dev = sim.device
+    if stats is None:
+        stats = torch.zeros(6, dtype=torch.int32, device=dev)
+    n = sim.nPoints
+    need = int(_lib.lib().mpmw_surrogate_workspace_bytes(n))
+    ws = getattr(mpm, "_mpmw_surr_ws", None)
+    if ws is None or ws.numel() < need:
+        ws = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
+        mpm._mpmw_surr_ws = ws
+    P = particles_from_states(sim, mpm, xpbd)
+    prm = params_from_states(sim, mpm)
+    packed = net.pack()
+    st = status_word(dev)
+    _lib.check(_lib.lib().mpmw_stress_surrogate(P, prm, packed.data_ptr(), net.params.data_ptr(), float(gate_tol),
+                                                int(round(audit * 1000)), int(audit_seed), stats.data_ptr(),
+                                                st.data_ptr(), ws.data_ptr(), ws.numel(), stream_handle()),
+               "stress_surrogate")
+    return stats
+
+
+def stats_summary(stats) -> dict:
+    """[candidates, fallbacks, audited, largest audited relative stress error,
+    sum of audited relative errors, audited within 1e-3] as a dict."""
+    import struct
+    s = [v & 0xFFFFFFFF for v in stats.detach().cpu().to(torch.int64).tolist()]
+    f = lambda u: struct.unpack("<f", struct.pack("<I", u))[0]  # noqa: E731
+    aud = s[2]
+    return {"candidates": s[0], "fallbacks": s[1], "accepted": s[0] - s[1], "audited": aud,
+            "audit_max_rel_err": f(s[3]), "audit_mean_rel_err": f(s[4]) / aud if aud else 0.0,
+            "audit_within_1e-3": s[5]}

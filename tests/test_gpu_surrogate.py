@@ -101,3 +101,42 @@ def test_training_gain():
     l1 = float(((net.infer(xv) - yv) ** 2).mean().item())
     print(f"surrogate validation MSE: untrained {l0:.3e}, trained {l1:.3e} (train loss {losses[0]:.2e} -> {losses[-1]:.2e})")
     assert l1 <= 1e-2 * l0
+
+
+def test_surrogate_stress_phase_vs_fp64_oracle():
+    """The stress phase with the trained surrogate for plastic returns (gate
+    1e-3, every accepted return audited) against the FP64 oracle's plain stress
+    phase on the parity scene: stress error at most 1e-3 norm-wise over the
+    plastic particles, labels equal except at most 1 % of the surrogate
+    candidates (damage thresholds reached with the predicted increment).
+    Elastic and out-of-range particles take the exact path."""
+    import torch
+
+    from mpmwarpydw_b200.surrogate import ReturnMapSurrogate, compute_stress, stats_summary
+    from tests.harness import gpu_fields, oracle, small_scene, to_oracle
+    net = ReturnMapSurrogate("cuda:0", seed=6)
+    x, y = net.samples(2_000_000, 17)
+    net.train(x, y, steps=6000, batch=16384)
+    sim, mpm, xpbd = small_scene(seed=21)
+    s64 = to_oracle(sim, mpm, xpbd, np.float64)
+    stats = compute_stress(sim, mpm, xpbd, net, gate_tol=1e-3, audit=1.0, audit_seed=3)
+    torch.cuda.synchronize()
+    o = oracle("f64")
+    o.compute_stress_from_F_trial(
+        s64.activeLabel, s64.materialLabel, s64.particle_x, s64.particle_v, s64.particle_x_initial_xpbd,
+        s64.particle_v_initial_xpbd, s64.particle_F, s64.particle_F_trial, s64.mu, s64.lam, s64.ys, s64.hardening,
+        s64.softening, s64.particle_density, s64.strainCriteria, s64.eff, s64.eta_shear, s64.eta_bulk, s64.particle_C,
+        s64.particle_stress, s64.particle_accumulated_strain, s64.particle_damage, s64.constitutive_model, s64.alpha)
+    g = gpu_fields(sim, mpm, xpbd)
+    st = stats_summary(stats)
+    plastic = s64.particle_accumulated_strain > to_oracle(*small_scene(seed=21), np.float64).particle_accumulated_strain
+    mpm_now = (s64.materialLabel <= 1) & plastic
+    d = (g["particle_stress"].reshape(-1, 9) - s64.particle_stress.reshape(-1, 9))[mpm_now]
+    ref = s64.particle_stress.reshape(-1, 9)[mpm_now]
+    err = float(np.linalg.norm(d) / np.linalg.norm(ref))
+    mism = int((g["materialLabel"] != s64.materialLabel).sum())
+    print(f"surrogate stress phase: {st}, plastic particles {int(mpm_now.sum())}, "
+          f"norm-wise stress error vs FP64 {err:.2e}, label mismatches {mism}")
+    assert st["candidates"] > 50
+    assert err <= 1e-3
+    assert mism <= max(1, st["candidates"] // 100)
