@@ -136,7 +136,34 @@ __global__ void __launch_bounds__(kBlock) k_g2p(mpmw_particles_t P, mpmw_grid_t 
 struct G2P2GShared {
     GatherShared g;
     ScatterShared s;
+    uint64_t pbar;  // particle-field read-ahead
 };
+
+// Particle fields read ahead by k_g2p2g (bulk copies into the scatter's record
+// area, which is free until the scatter): F (9), mu, lam, ys, alpha, damage,
+// eta_shear, eta_bulk, mass, vol.
+constexpr int kAheadFields = 18;
+struct AheadFields {
+    float f[kAheadFields][kScatterChunk];
+};
+static_assert(sizeof(AheadFields) <= sizeof(ScatterShared::rec), "read-ahead fits the record area");
+
+__device__ __forceinline__ const float *ahead_src(const mpmw_particles_t &P, int field)
+{
+    const int64_t n = P.n;
+    if (field < 9) return P.F + (int64_t)field * n;
+    switch (field) {
+    case 9: return P.mu;
+    case 10: return P.lam;
+    case 11: return P.ys;
+    case 12: return P.alpha;
+    case 13: return P.damage;
+    case 14: return P.eta_shear;
+    case 15: return P.eta_bulk;
+    case 16: return P.mass;
+    default: return P.vol;
+    }
+}
 
 // G2P of substep k, return map of substep k+1, P2G of substep k+1 (into grid.mv,
 // which the caller has zeroed).  StoreStress: also write the stress (the last
@@ -144,14 +171,27 @@ struct G2P2GShared {
 template <bool StoreStress>
 __global__ void __launch_bounds__(kScatterChunk, 3) k_g2p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
                                                         uint32_t *status, int *svd_list, int *svd_count,
-                                                        const __grid_constant__ CUtensorMap tmap, int use_tma)
+                                                        const __grid_constant__ CUtensorMap tmap, int use_tma,
+                                                        int use_ahead)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     // the TMA destination (S.g.tile) must be 128-byte aligned: round the base up
     // (the launch reserves 128 bytes for this)
     G2P2GShared &S = *reinterpret_cast<G2P2GShared *>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
     const int64_t n = P.n;
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = threadIdx.x;
+    const int64_t p0 = (int64_t)blockIdx.x * blockDim.x;
+    const int64_t p = p0 + t;
+    // read-ahead of the particle fields used after the gather (full CTAs only;
+    // the host checks the 16-byte alignment the bulk copies need)
+    const bool ahead = use_ahead && p0 + kScatterChunk <= n;
+    AheadFields &AF = *reinterpret_cast<AheadFields *>(&S.s.rec[0][0]);
+    if (ahead && t == 0) {
+        mbar_init(&S.pbar, 1);
+        mbar_arrive_expect_tx(&S.pbar, kAheadFields * kScatterChunk * 4u);
+#pragma unroll 1
+        for (int f = 0; f < kAheadFields; ++f) bulk_load(&AF.f[f][0], ahead_src(P, f) + p0, kScatterChunk * 4u, &S.pbar);
+    }
     const bool act = p < n && P.active[p] == 1 && P.material[p] <= 1;
     float xp[3] = {0.f, 0.f, 0.f};
     Weights W;
@@ -161,8 +201,19 @@ __global__ void __launch_bounds__(kScatterChunk, 3) k_g2p2g(mpmw_particles_t P, 
     }
     bool tile = false;
     int ox = 0, oy = 0, oz = 0;
-    if (!gather_prepare(S.g, act, W, &tmap, use_tma, status, tile, ox, oy, oz)) return;  // uniform
+    if (!gather_prepare(S.g, act, W, &tmap, use_tma, status, tile, ox, oy, oz)) {
+        // no active particle: the read-ahead must still land before the CTA exits
+        if (ahead && !mbar_wait_bounded(&S.pbar, 0)) raise_status(status, MPMW_ST_TIMEOUT);
+        return;  // uniform
+    }
     uint32_t bad = 0;
+    bool ahead_ok = ahead;
+    if (ahead && !mbar_wait_bounded(&S.pbar, 0)) {
+        // report, wait once more for the copies in flight, and read global memory
+        raise_status(status, MPMW_ST_TIMEOUT);
+        mbar_wait_bounded(&S.pbar, 0);
+        ahead_ok = false;
+    }
     bool scat = false;
     float xn[3] = {0.f, 0.f, 0.f}, nv[3] = {0.f, 0.f, 0.f}, nC[9], st6[6];
     float m = 0.f, vol = 0.f;
@@ -173,14 +224,33 @@ __global__ void __launch_bounds__(kScatterChunk, 3) k_g2p2g(mpmw_particles_t P, 
         for (int a = 0; a < 3; ++a) xn[a] = fma_(prm.dt, nv[a], xp[a]);
         if (!(isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]))) bad |= MPMW_ST_NAN;
         float Ft[9];
-        g2p_deformation(P, prm, p, nF, Ft);
+        {
+            float Fpre[9];
+            if (ahead_ok) {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) Fpre[k] = AF.f[k][t];
+            } else {
+                load9(P.F, n, p, Fpre);
+            }
+            g2p_deformation(P, prm, p, nF, Ft, Fpre);
+        }
         store3(P.x, n, p, xn);
+        MatScalars ms;
+        float eta_s, eta_b;
+        if (ahead_ok) {
+            ms.mu = AF.f[9][t]; ms.lam = AF.f[10][t]; ms.ys = AF.f[11][t]; ms.alpha = AF.f[12][t]; ms.D = AF.f[13][t];
+            eta_s = AF.f[14][t]; eta_b = AF.f[15][t]; m = AF.f[16][t]; vol = AF.f[17][t];
+        } else {
+            ms.mu = P.mu[p]; ms.lam = P.lam[p]; ms.ys = P.ys[p]; ms.alpha = P.alpha[p]; ms.D = P.damage[p];
+            eta_s = P.eta_shear[p]; eta_b = P.eta_bulk[p]; m = P.mass[p]; vol = P.vol[p];
+        }
         float Fo[9], T[9];
-        const int rm = prm.stress_mode == MPMW_STRESS_AUTO ? small_strain_update<true>(P, prm.eff, p, Ft, xn, nv, Fo, T)
-                                                           : 0;
+        const int rm = prm.stress_mode == MPMW_STRESS_AUTO
+                           ? small_strain_update<true>(P, prm.eff, p, Ft, xn, nv, Fo, T, &ms)
+                           : 0;
         if (rm != 0) {
             float out[9];
-            add_viscous(T, nC, P.eta_shear[p], P.eta_bulk[p], out);
+            add_viscous(T, nC, eta_s, eta_b, out);
             store9(P.F, n, p, Fo);
             st6[0] = out[0]; st6[1] = out[4]; st6[2] = out[8]; st6[3] = out[1]; st6[4] = out[2]; st6[5] = out[5];
             if (StoreStress || rm == 2) store_sym6(P.stress, n, p, out);
@@ -190,8 +260,6 @@ __global__ void __launch_bounds__(kScatterChunk, 3) k_g2p2g(mpmw_particles_t P, 
                 store9(P.C, n, p, nC);
             } else {
                 scat = true;
-                m = P.mass[p];
-                vol = P.vol[p];
             }
         } else {
             store9(P.F_trial, n, p, Ft);
@@ -336,9 +404,18 @@ int launch_g2p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_par
     int *count = static_cast<int *>(ws);
     int *list = reinterpret_cast<int *>(static_cast<char *>(ws) + 256);
     if (cudaMemsetAsync(count, 0, sizeof(int), s) != cudaSuccess) { set_error("g2p2g: memset failed"); return MPMW_E_DEVICE; }
+    // the read-ahead bulk copies need every field's chunk start 16-byte aligned
+    int use_ahead = (p.n % 4 == 0) ? 1 : 0;
+    for (int f = 0; f < kAheadFields && use_ahead; ++f) {
+        const float *base = f < 9 ? p.F + (int64_t)f * p.n
+                                  : (f == 9 ? p.mu : f == 10 ? p.lam : f == 11 ? p.ys : f == 12 ? p.alpha
+                                     : f == 13 ? p.damage : f == 14 ? p.eta_shear : f == 15 ? p.eta_bulk
+                                     : f == 16 ? p.mass : p.vol);
+        if (!base || (reinterpret_cast<uintptr_t>(base) & 15u) != 0) use_ahead = 0;
+    }
     const unsigned grid = grid_for(p.n, kScatterChunk);
-    if (store_stress) k_g2p2g<true><<<grid, kScatterChunk, smem, s>>>(p, g, prm, st, list, count, map, use_tma);
-    else k_g2p2g<false><<<grid, kScatterChunk, smem, s>>>(p, g, prm, st, list, count, map, use_tma);
+    if (store_stress) k_g2p2g<true><<<grid, kScatterChunk, smem, s>>>(p, g, prm, st, list, count, map, use_tma, use_ahead);
+    else k_g2p2g<false><<<grid, kScatterChunk, smem, s>>>(p, g, prm, st, list, count, map, use_tma, use_ahead);
     MPMW_TRY_LAUNCH("k_g2p2g");
     k_stress_p2g_list<<<148 * 4, kBlock, 0, s>>>(p, g, prm, st, list, count);
     return check_launch("k_stress_p2g_list");

@@ -144,14 +144,20 @@ __device__ __forceinline__ void gather_particle(const GatherShared &S, bool tile
     }
 }
 
-// F_trial = (I + dt grad v) F = F + dt (grad v F); optional covariance update
+// F_trial = (I + dt grad v) F = F + dt (grad v F); optional covariance update.
+// Fpre: F read ahead (else loaded here).
 __device__ __forceinline__ void g2p_deformation(const mpmw_particles_t &P, const mpmw_params_t &prm, int64_t p,
-                                                const float *nF, float *Ft)
+                                                const float *nF, float *Ft, const float *Fpre = nullptr)
 {
     const int64_t n = P.n;
     const float dt = prm.dt;
     float F[9];
-    load9(P.F, n, p, F);
+    if (Fpre) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) F[k] = Fpre[k];
+    } else {
+        load9(P.F, n, p, F);
+    }
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll

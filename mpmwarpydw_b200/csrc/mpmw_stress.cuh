@@ -103,9 +103,15 @@ __device__ __forceinline__ void sym_exp_small(const float *A, float *E)
 // 2 when done and the particle became an XPBD particle (T = 0).
 // On success writes Fout, the symmetric Kirchhoff stress T (before the viscous
 // term) and the same per-particle side effects as the SVD path.
+// Material scalars of one particle read ahead of the return map (optional).
+struct MatScalars {
+    float mu, lam, ys, alpha, D;
+};
+
 template <bool HaveXV>
 __device__ __forceinline__ int small_strain_update(const mpmw_particles_t &P, float eff, int64_t p, const float *Ft,
-                                                    const float *xr, float *vr, float *Fout, float *T)
+                                                    const float *xr, float *vr, float *Fout, float *T,
+                                                    const MatScalars *pre = nullptr)
 {
     const int64_t n = P.n;
     float G[9];
@@ -144,7 +150,9 @@ __device__ __forceinline__ int small_strain_update(const mpmw_particles_t &P, fl
 #pragma unroll
         for (int e = 0; e < 6; ++e) eps[e] = 0.5f * L[e];
     }
-    float mu = P.mu[p], lam = P.lam[p], ys = P.ys[p], alpha = P.alpha[p], D = P.damage[p];
+    float mu, lam, ys, alpha, D;
+    if (pre) { mu = pre->mu; lam = pre->lam; ys = pre->ys; alpha = pre->alpha; D = pre->D; }
+    else { mu = P.mu[p]; lam = P.lam[p]; ys = P.ys[p]; alpha = P.alpha[p]; D = P.damage[p]; }
     const float tr = (eps[0] + eps[1]) + eps[2];
     const float mean_eps = tr / 3.f;
     float dev[6] = {eps[0] - mean_eps, eps[1] - mean_eps, eps[2] - mean_eps, eps[3], eps[4], eps[5]};

@@ -82,6 +82,16 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
+// 1-D bulk copy global -> shared (no multicast), completion signalled on `bar`.
+// dst and src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
 // Host: tensor map over a (nx, ny, nz, 4) float32 grid array, box
 // (4, kTileEdge, kTileEdge, kTileEdge), zero fill outside the array.
 // Returns false if the driver rejects the descriptor.
