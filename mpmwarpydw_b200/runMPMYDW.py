@@ -1,0 +1,239 @@
+"""Simulation driver with the reference's configuration surface (runMPMYDW.py).
+
+    python -m mpmwarpydw_b200.runMPMYDW --config cfg.json [--flag value ...] [--check_interval K]
+
+Flags, defaults and the JSON merge rule are the reference's (utils/getArgs.py).
+The structure is the reference's big-step loop (runMPMYDW.py:633-903):
+
+  for each big step:
+    phase 1 (MPM + XPBD): gravity pulse for gravity_pulse_duration, MPM
+      substeps with an XPBD step after every substep whose counter is a
+      positive multiple of mpmStepsPerXpbdStep; stop after nSteps substeps, or
+      once at least 1000 substeps ran and the residual (sum |v|/r over active
+      particles / active count) is below residualThreshold, or when the mean
+      damage grew by less than damage_stall_threshold per substep for
+      damage_stall_duration;
+    phase 2 (XPBD only, xpbdOnlyDuration): debris settling, stopping early when
+      the sleeping fraction of XPBD particles reaches
+      xpbd_sleep_termination_ratio;
+    end: XPBD particles below the deactivation datum are deactivated and moved
+      out of the domain.
+
+The reference reads the residual and the mean damage back to the host after
+every substep; ``--check_interval K`` (K = 1 is the reference) reads them every
+K substeps instead, and the MPM substeps in between run as one fused library
+call (their XPBD steps still fall on the same counters).  Termination is then
+decided at those points.
+
+Domain input (``--domainFile``): an HDF5 file in the reference's schema when
+h5py is importable, an .npz with the same keys (``x`` [3, N] or [N, 3],
+``particle_volume`` [N], optional per-particle ``density``, ``E``, ``nu``,
+``ys``, ``alpha``, ``hardening``, ``softening``, ``eta_shear``, ``eta_bulk``,
+``strainCriteria``, ``damage``), or ``synthetic:<name>`` for a seeded generator
+of ``domains`` (``block_collapse``, ``caving_block``, ``tunnel``).
+Output (``saveFlag``): one .npz of particle state per render interval in
+``outputFolder``.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+import time
+
+import numpy as np
+import torch
+
+from . import domains as _domains
+from .engine import original_order, sort_particles
+from .scene import build_states
+from .utils import mpmRoutines
+from .utils import simulationRoutines as S
+from .utils.getArgs import get_args
+from .utils.simStates import vec3
+
+PROPERTY_NAMES = ("density", "E", "nu", "ys", "alpha", "hardening", "softening", "eta_shear", "eta_bulk",
+                  "strainCriteria", "damage")
+MIN_STEPS = 1000  # runMPMYDW.py:654
+
+
+def load_domain(path: str, args):
+    """(x [N,3], particle_volume [N], props, overrides) for --domainFile."""
+    if path.startswith("synthetic:"):
+        name = path.split(":", 1)[1]
+        d = getattr(_domains, name)()
+        return d.x, d.vol, d.props, d.overrides, d
+    if path.endswith(".npz"):
+        z = np.load(path)
+        get = lambda k: np.asarray(z[k])  # noqa: E731
+        keys = set(z.files)
+    else:
+        try:
+            import h5py
+        except ImportError as e:  # pragma: no cover - depends on the install
+            raise RuntimeError(f"{path}: reading HDF5 needs h5py; convert it to .npz or install h5py") from e
+        f = h5py.File(path, "r")
+        get = lambda k: np.asarray(f[k])  # noqa: E731
+        keys = set(f.keys())
+    x = get("x")
+    if x.shape[0] == 3 and x.shape[-1] != 3:
+        x = x.T
+    vol = get("particle_volume").reshape(-1)
+    props = {k: get(k).reshape(-1) for k in PROPERTY_NAMES if k in keys}
+    return x.astype(np.float32), vol.astype(np.float32), props, {}, None
+
+
+def save_state(sim, mpm, xpbd, folder, big_step, counter, checkpoint=False):
+    """Particle state in input order as an .npz (positions, velocities, labels,
+    damage, accumulated strain, stress, F, radius); the end-of-big-step
+    checkpoint gets its own name."""
+    os.makedirs(folder, exist_ok=True)
+    o = lambda t: original_order(sim, t).detach().cpu().numpy()  # noqa: E731
+    tag = "checkpoint" if checkpoint else "sim_step"
+    path = os.path.join(folder, f"{tag}_{big_step:04d}_{counter:08d}.npz")
+    np.savez_compressed(path, x=o(sim.particle_x), v=o(sim.particle_v), materialLabel=o(sim.materialLabel),
+                        activeLabel=o(sim.activeLabel), damage=o(mpm.particle_damage),
+                        accumulated_strain=o(mpm.particle_accumulated_strain), stress=o(mpm.particle_stress),
+                        F=o(mpm.particle_F), radius=o(sim.particle_radius), t=sim.t)
+    return path
+
+
+class PhaseOneMonitor:
+    """Termination of phase 1 (runMPMYDW.py:656-727), host side."""
+
+    def __init__(self, n_steps, residual_threshold, stall_threshold, stall_steps, min_steps=MIN_STEPS):
+        self.n_steps, self.residual_threshold = n_steps, residual_threshold
+        self.stall_threshold, self.stall_steps, self.min_steps = stall_threshold, stall_steps, min_steps
+        self.counter, self.residual, self.stall = 0, 1e10, 0
+        self.prev_damage = None
+        self.stopped_early = False
+
+    def running(self):
+        return self.counter < self.n_steps and (self.counter < self.min_steps or self.residual > self.residual_threshold)
+
+    def update(self, k, residual, mean_damage):
+        """Account k substeps ending with (residual, mean damage); returns False
+        when the damage stall ends the phase."""
+        self.counter += k
+        self.residual = residual
+        if self.prev_damage is None:
+            self.prev_damage = mean_damage
+        change = mean_damage - self.prev_damage
+        if change < self.stall_threshold * k and self.counter > self.min_steps:
+            self.stall += k
+        else:
+            self.stall = 0
+        self.prev_damage = mean_damage
+        if self.stall >= self.stall_steps and self.counter > self.min_steps:
+            self.stopped_early = True
+            return False
+        return True
+
+
+def _stats(sim, mpm):
+    """(residual, mean damage over active, counts) from one device reduction."""
+    s = S.step_stats(sim, mpm).cpu().numpy()
+    active = s[1]
+    residual = s[0] / active if active > 0 else 0.0
+    mean_damage = s[2] / active if active > 0 else 0.0
+    return float(residual), float(mean_damage), s
+
+
+def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=None):
+    dev = torch.device(device)
+    torch.cuda.set_device(dev)
+    x, vol, props, overrides, dom = load_domain(args.domainFile, args)
+    for k, v in overrides.items():
+        setattr(args, k, v)
+    kw = {}
+    if dom is not None:
+        kw = dict(dx=dom.dx, minBounds=dom.minBounds, gridDims=dom.gridDims)
+    sim, mpm, xpbd = build_states(args, x, vol, props, device=dev, adjust_dt=True, **kw)
+    sort_particles(sim, mpm, xpbd)
+    log = print if verbose else (lambda *a, **k: None)
+    log(f"particles {sim.nPoints}, grid {mpm.gridDims}, dx {sim.dx:.4f}, dt {sim.dt:.3e}, "
+        f"XPBD every {sim.mpmStepsPerXpbdStep} substeps")
+    ratio = max(1, int(sim.mpmStepsPerXpbdStep))
+    base_gravity = sim.gravity
+    next_save = sim.t + args.render_interval
+    start = time.time()
+    saved = []
+    big_steps = sim.bigSteps if max_big_steps is None else min(sim.bigSteps, max_big_steps)
+    for big in range(big_steps):
+        pulse_steps = int(args.gravity_pulse_duration / sim.dt) if args.gravity_pulse_duration > 0 else 0
+        pulsing = args.gravity_pulse_factor != 1.0 and pulse_steps > 0
+        if pulsing:
+            sim.gravity = vec3(*[g * args.gravity_pulse_factor for g in base_gravity])
+        _, d0, _ = _stats(sim, mpm)
+        mon = PhaseOneMonitor(sim.nSteps, sim.residualThreshold, sim.damage_stall_threshold,
+                              int(sim.damage_stall_duration / sim.dt))
+        mon.prev_damage = d0
+        while mon.running():
+            c = mon.counter
+            # substeps up to the next check: stop at the pulse end and never skip past nSteps
+            k = min(check_interval, sim.nSteps - c)
+            if pulsing and c < pulse_steps:
+                k = min(k, pulse_steps - c)
+            done = 0
+            while done < k:
+                cc = c + done
+                nxt = ratio if cc == 0 else ((cc + ratio - 1) // ratio) * ratio  # next XPBD counter
+                m = min(k - done, nxt - cc + 1)
+                if m == 1:
+                    S.mpmSimulationStep(sim, mpm, xpbd, dev)
+                else:
+                    S.run_mpm_substeps(sim, mpm, xpbd, m)
+                if cc + m - 1 == nxt:
+                    S.xpbdSimulationStep(sim, mpm, xpbd, dev)
+                done += m
+            sim.t += k * sim.dt
+            residual, mean_damage, counts = _stats(sim, mpm)
+            if pulsing and mon.counter + k == pulse_steps:
+                sim.gravity = base_gravity
+            if not mon.update(k, residual, mean_damage):
+                log(f"    early termination: damage stalled for {sim.damage_stall_duration}s")
+                break
+            if mon.counter % 100 < k:
+                log(f"  big step {big + 1}, substep {mon.counter}, t {sim.t:.4f}s, residual {residual:.4e}, "
+                    f"mean damage {mean_damage:.6f}, MPM {int(counts[3])}+{int(counts[5])}, "
+                    f"XPBD {int(counts[4])}+{int(counts[6])}, wall {time.time() - start:.2f}s")
+            if sim.saveFlag and sim.t >= next_save - 0.5 * sim.dt:
+                saved.append(save_state(sim, mpm, xpbd, sim.outputFolder, big, mon.counter))
+                next_save += args.render_interval
+        if pulsing:
+            sim.gravity = base_gravity
+        log(f"  phase 1 done after {mon.counter} substeps ({mon.counter * sim.dt:.3f}s simulated)")
+        # phase 2: XPBD only
+        for j in range(1, sim.xpbdOnlySteps + 1):
+            S.xpbdSimulationStep(sim, mpm, xpbd, dev, xpbd_only=True)
+            sim.t += sim.dtxpbd
+            if sim.xpbd_sleep_termination_ratio < 1.0:
+                tot, slp = int(sim.numTotalXPBD.item()), int(sim.numSleepingXPBD.item())
+                if tot > 0 and slp / tot >= sim.xpbd_sleep_termination_ratio:
+                    log(f"    phase 2 stopped early: {slp}/{tot} XPBD particles asleep")
+                    break
+        # end of big step: deactivate XPBD particles below the datum
+        minB, maxB = np.asarray(sim.minBounds, np.float64), np.asarray(sim.maxBounds, np.float64)
+        z_datum = args.xpbd_deactivation_z_datum if args.xpbd_deactivation_z_datum is not None else float(minB[2])
+        mpmRoutines.deactivate_and_teleport_xpbd_below_datum(sim.particle_x, sim.particle_v, sim.activeLabel,
+                                                              sim.materialLabel, float(z_datum),
+                                                              2.0 * float(maxB[2] - minB[2]))
+        if sim.saveFlag:
+            saved.append(save_state(sim, mpm, xpbd, sim.outputFolder, big, mon.counter, checkpoint=True))
+    torch.cuda.synchronize(dev)
+    log(f"simulation complete in {time.time() - start:.2f}s")
+    return sim, mpm, xpbd, saved
+
+
+def main(argv=None):
+    argv = sys.argv[1:] if argv is None else list(argv)
+    extra = argparse.ArgumentParser(add_help=False)
+    extra.add_argument("--check_interval", type=int, default=1)
+    extra.add_argument("--device", type=str, default="cuda:0")
+    ex, rest = extra.parse_known_args(argv)
+    args = get_args(rest)
+    run(args, check_interval=max(1, ex.check_interval), device=ex.device)
+
+
+if __name__ == "__main__":
+    main()
