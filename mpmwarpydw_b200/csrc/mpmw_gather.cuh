@@ -76,27 +76,33 @@ __device__ __forceinline__ bool gather_prepare(GatherShared &S, bool act, const 
     return true;
 }
 
-// Phase 2 (per active particle): the tensor-product gather.
+// Phase 2 (per active particle): the tensor-product gather.  The x and y
+// components share every weight, so they are summed as float2 pairs with the
+// packed FP32 FMA (__ffma2_rn: two FMAs, each rounded once, in one
+// instruction); the z component is summed alone.  Same operations and
+// rounding as three scalar FMAs.
+__device__ __forceinline__ float2 ffma2(float w, float2 g, float2 acc) { return __ffma2_rn(make_float2(w, w), g, acc); }
+
 __device__ __forceinline__ void gather_particle(const GatherShared &S, bool tile, int ox, int oy, int oz,
                                                 const Weights &W, const mpmw_grid_t &G, float inv_dx, float *nv,
                                                 float *nF, float *nC, uint32_t &bad)
 {
     const int nx = G.dims[0], ny = G.dims[1], nz = G.dims[2];
     const float4 *__restrict__ gv = reinterpret_cast<const float4 *>(G.v);
-    float gx[3] = {0.f, 0.f, 0.f}, gy[3] = {0.f, 0.f, 0.f}, gz[3] = {0.f, 0.f, 0.f};
-    float Mi[3] = {0.f, 0.f, 0.f}, Mj[3] = {0.f, 0.f, 0.f}, Mk[3] = {0.f, 0.f, 0.f};
-    nv[0] = nv[1] = nv[2] = 0.f;
+    float2 v2 = make_float2(0.f, 0.f), gx2 = v2, gy2 = v2, gz2 = v2, Mi2 = v2, Mj2 = v2, Mk2 = v2;
+    float vz = 0.f, gxz = 0.f, gyz = 0.f, gzz = 0.f, Miz = 0.f, Mjz = 0.f, Mkz = 0.f;
     const bool inside = W.base[0] >= 0 && W.base[1] >= 0 && W.base[2] >= 0 && W.base[0] + 2 < nx &&
                         W.base[1] + 2 < ny && W.base[2] + 2 < nz;
     if (!inside) bad |= MPMW_ST_OOB;
     const int tb = ((W.base[0] - ox) * kTileEdge + (W.base[1] - oy)) * kTileEdge + (W.base[2] - oz);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-        float SS[3] = {0.f, 0.f, 0.f}, SD[3] = {0.f, 0.f, 0.f}, TS[3] = {0.f, 0.f, 0.f}, US[3] = {0.f, 0.f, 0.f},
-              SJ[3] = {0.f, 0.f, 0.f};
+        float2 SS2 = make_float2(0.f, 0.f), SD2 = SS2, TS2 = SS2, US2 = SS2, SJ2 = SS2;
+        float SSz = 0.f, SDz = 0.f, TSz = 0.f, USz = 0.f, SJz = 0.f;
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-            float Sv[3] = {0.f, 0.f, 0.f}, Tv[3] = {0.f, 0.f, 0.f}, Uv[3] = {0.f, 0.f, 0.f};
+            float2 Sv2 = make_float2(0.f, 0.f), Tv2 = Sv2, Uv2 = Sv2;
+            float Svz = 0.f, Tvz = 0.f, Uvz = 0.f;
             const int ix = W.base[0] + i, iy = W.base[1] + j;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
@@ -106,32 +112,30 @@ __device__ __forceinline__ void gather_particle(const GatherShared &S, bool tile
                 else if (inside || (ix >= 0 && iy >= 0 && iz >= 0 && ix < nx && iy < ny && iz < nz))
                     g = __ldg(&gv[((int64_t)ix * ny + iy) * nz + iz]);
                 const float wz = W.w[2][k], dwz = W.dw[2][k], kwz = (float)k * wz;
-                Sv[0] = fma_(wz, g.x, Sv[0]); Sv[1] = fma_(wz, g.y, Sv[1]); Sv[2] = fma_(wz, g.z, Sv[2]);
-                Tv[0] = fma_(dwz, g.x, Tv[0]); Tv[1] = fma_(dwz, g.y, Tv[1]); Tv[2] = fma_(dwz, g.z, Tv[2]);
-                Uv[0] = fma_(kwz, g.x, Uv[0]); Uv[1] = fma_(kwz, g.y, Uv[1]); Uv[2] = fma_(kwz, g.z, Uv[2]);
+                const float2 gxy = make_float2(g.x, g.y);
+                Sv2 = ffma2(wz, gxy, Sv2); Svz = fma_(wz, g.z, Svz);
+                Tv2 = ffma2(dwz, gxy, Tv2); Tvz = fma_(dwz, g.z, Tvz);
+                Uv2 = ffma2(kwz, gxy, Uv2); Uvz = fma_(kwz, g.z, Uvz);
             }
             const float wy = W.w[1][j], dwy = W.dw[1][j], jwy = (float)j * wy;
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                SS[r] = fma_(wy, Sv[r], SS[r]);
-                SD[r] = fma_(dwy, Sv[r], SD[r]);
-                TS[r] = fma_(wy, Tv[r], TS[r]);
-                US[r] = fma_(wy, Uv[r], US[r]);
-                SJ[r] = fma_(jwy, Sv[r], SJ[r]);
-            }
+            SS2 = ffma2(wy, Sv2, SS2); SSz = fma_(wy, Svz, SSz);
+            SD2 = ffma2(dwy, Sv2, SD2); SDz = fma_(dwy, Svz, SDz);
+            TS2 = ffma2(wy, Tv2, TS2); TSz = fma_(wy, Tvz, TSz);
+            US2 = ffma2(wy, Uv2, US2); USz = fma_(wy, Uvz, USz);
+            SJ2 = ffma2(jwy, Sv2, SJ2); SJz = fma_(jwy, Svz, SJz);
         }
         const float wx = W.w[0][i], dwx = W.dw[0][i], iwx = (float)i * wx;
-#pragma unroll
-        for (int r = 0; r < 3; ++r) {
-            nv[r] = fma_(wx, SS[r], nv[r]);
-            gx[r] = fma_(dwx, SS[r], gx[r]);
-            gy[r] = fma_(wx, SD[r], gy[r]);
-            gz[r] = fma_(wx, TS[r], gz[r]);
-            Mi[r] = fma_(iwx, SS[r], Mi[r]);
-            Mj[r] = fma_(wx, SJ[r], Mj[r]);
-            Mk[r] = fma_(wx, US[r], Mk[r]);
-        }
+        v2 = ffma2(wx, SS2, v2); vz = fma_(wx, SSz, vz);
+        gx2 = ffma2(dwx, SS2, gx2); gxz = fma_(dwx, SSz, gxz);
+        gy2 = ffma2(wx, SD2, gy2); gyz = fma_(wx, SDz, gyz);
+        gz2 = ffma2(wx, TS2, gz2); gzz = fma_(wx, TSz, gzz);
+        Mi2 = ffma2(iwx, SS2, Mi2); Miz = fma_(iwx, SSz, Miz);
+        Mj2 = ffma2(wx, SJ2, Mj2); Mjz = fma_(wx, SJz, Mjz);
+        Mk2 = ffma2(wx, US2, Mk2); Mkz = fma_(wx, USz, Mkz);
     }
+    nv[0] = v2.x; nv[1] = v2.y; nv[2] = vz;
+    const float gx[3] = {gx2.x, gx2.y, gxz}, gy[3] = {gy2.x, gy2.y, gyz}, gz[3] = {gz2.x, gz2.y, gzz};
+    const float Mi[3] = {Mi2.x, Mi2.y, Miz}, Mj[3] = {Mj2.x, Mj2.y, Mjz}, Mk[3] = {Mk2.x, Mk2.y, Mkz};
     const float c4 = 4.f * inv_dx;
 #pragma unroll
     for (int r = 0; r < 3; ++r) {

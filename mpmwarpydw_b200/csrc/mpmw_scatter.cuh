@@ -53,14 +53,22 @@ __device__ __forceinline__ int scatter_slot(int k) { return k ^ ((k >> 3) & 7); 
 __device__ __forceinline__ float sel3(const float4 &r, int i) { return i == 0 ? r.x : (i == 1 ? r.y : r.z); }
 
 // Register sums of one stencil column (i, j) of one segment: the 3 nodes
-// k = 0..2 of (m, m vx, m vy, m vz).
+// k = 0..2 of (m, m vx, m vy, m vz).  The x and y momentum components (and
+// the masses of nodes 0 and 1) are summed as float2 pairs with the packed FP32
+// FMA; every component sees the same operations and roundings as the scalar
+// form fma(w_k, P_k, fma(dw_k, R, acc)).
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+
 struct ColumnSums {
-    float am0, am1, am2, ax0, ay0, az0, ax1, ay1, az1, ax2, ay2, az2;
+    float2 m01, axy[3];
+    float m2, az[3];
 
     __device__ __forceinline__ void zero()
     {
-        am0 = am1 = am2 = 0.f;
-        ax0 = ay0 = az0 = ax1 = ay1 = az1 = ax2 = ay2 = az2 = 0.f;
+        m01 = make_float2(0.f, 0.f);
+        m2 = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { axy[k] = make_float2(0.f, 0.f); az[k] = 0.f; }
     }
 
     // add the contribution of the particle in record slot q to column ij
@@ -76,21 +84,28 @@ struct ColumnSums {
         const float s00 = r1.w, s11 = r2.w, s22 = r3.w, s01 = r4.w, s02 = r5.w, s12 = r6.w;
         const float wxy = wxi * wyj, g0 = dwxi * wyj, g1 = wxi * dwyj, wm = wxy * mm;
         // A = a + i Bx + j By
-        const float A0 = fma_(fj, r8.x, fma_(fi, r7.x, r6.x));
-        const float A1 = fma_(fj, r8.y, fma_(fi, r7.y, r6.y));
+        const float2 A01 = __ffma2_rn(dup2(fj), make_float2(r8.x, r8.y),
+                                      __ffma2_rn(dup2(fi), make_float2(r7.x, r7.y), make_float2(r6.x, r6.y)));
         const float A2 = fma_(fj, r8.z, fma_(fi, r7.z, r6.z));
         // Q = S (g0, g1, 0), R = wxy S[:,2]
-        const float Q0 = fma_(s00, g0, s01 * g1), Q1 = fma_(s01, g0, s11 * g1), Q2 = fma_(s02, g0, s12 * g1);
-        const float R0 = wxy * s02, R1 = wxy * s12, R2 = wxy * s22;
+        const float2 Q01 = __ffma2_rn(make_float2(s00, s01), dup2(g0), __fmul2_rn(make_float2(s01, s11), dup2(g1)));
+        const float Q2 = fma_(s02, g0, s12 * g1);
+        const float2 R01 = __fmul2_rn(dup2(wxy), make_float2(s02, s12));
+        const float R2 = wxy * s22;
         // P_k = wxy (A + k Bz) + Q
-        const float P00 = fma_(wxy, A0, Q0), P01 = fma_(wxy, A1, Q1), P02 = fma_(wxy, A2, Q2);
-        const float dz0 = wxy * r9.x, dz1 = wxy * r9.y, dz2 = wxy * r9.z;
-        const float P10 = P00 + dz0, P11 = P01 + dz1, P12 = P02 + dz2;
-        const float P20 = P10 + dz0, P21 = P11 + dz1, P22 = P12 + dz2;
-        am0 = fma_(r4.x, wm, am0); am1 = fma_(r4.y, wm, am1); am2 = fma_(r4.z, wm, am2);
-        ax0 = fma_(r4.x, P00, fma_(r5.x, R0, ax0)); ay0 = fma_(r4.x, P01, fma_(r5.x, R1, ay0)); az0 = fma_(r4.x, P02, fma_(r5.x, R2, az0));
-        ax1 = fma_(r4.y, P10, fma_(r5.y, R0, ax1)); ay1 = fma_(r4.y, P11, fma_(r5.y, R1, ay1)); az1 = fma_(r4.y, P12, fma_(r5.y, R2, az1));
-        ax2 = fma_(r4.z, P20, fma_(r5.z, R0, ax2)); ay2 = fma_(r4.z, P21, fma_(r5.z, R1, ay2)); az2 = fma_(r4.z, P22, fma_(r5.z, R2, az2));
+        float2 P01 = __ffma2_rn(dup2(wxy), A01, Q01);
+        float P2 = fma_(wxy, A2, Q2);
+        const float2 dz01 = __fmul2_rn(dup2(wxy), make_float2(r9.x, r9.y));
+        const float dz2 = wxy * r9.z;
+        m01 = __ffma2_rn(make_float2(r4.x, r4.y), dup2(wm), m01);
+        m2 = fma_(r4.z, wm, m2);
+        const float wz[3] = {r4.x, r4.y, r4.z}, dwz[3] = {r5.x, r5.y, r5.z};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if (k > 0) { P01 = __fadd2_rn(P01, dz01); P2 = P2 + dz2; }
+            axy[k] = __ffma2_rn(dup2(wz[k]), P01, __ffma2_rn(dup2(dwz[k]), R01, axy[k]));
+            az[k] = fma_(wz[k], P2, fma_(dwz[k], R2, az[k]));
+        }
     }
 
     // add the column's 3 nodes into the shared tile (or global memory)
@@ -100,8 +115,9 @@ struct ColumnSums {
     {
         const int i = ij / 3, j = ij - 3 * (ij / 3);
         const int gx = S.base[0][k0] + i, gy = S.base[1][k0] + j, gz0 = S.base[2][k0];
-        const float4 c[3] = {make_float4(am0, ax0, ay0, az0), make_float4(am1, ax1, ay1, az1),
-                             make_float4(am2, ax2, ay2, az2)};
+        const float mk[3] = {m01.x, m01.y, m2};
+        const float4 c[3] = {make_float4(mk[0], axy[0].x, axy[0].y, az[0]), make_float4(mk[1], axy[1].x, axy[1].y, az[1]),
+                             make_float4(mk[2], axy[2].x, axy[2].y, az[2])};
         if (use_tile) {
             const int tb = ((gx - ox) * eyi + (gy - oy)) * ezi + (gz0 - oz);
 #pragma unroll
