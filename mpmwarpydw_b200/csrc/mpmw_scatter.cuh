@@ -4,13 +4,16 @@
 //
 // For the kScatterChunk particles of a CTA (one per thread; `act` marks those
 // that scatter):
-//   1. scattering particles are compacted; each stores its B-spline weights and
-//      per-particle constants (10 float4) in shared memory, in slots swizzled so
-//      that particles about 8 apart (one cell's worth in base-cell order) fall
-//      in different banks;
-//   2. consecutive particles with the same stencil base cell (the reference's
-//      truncated base index, bit-exact) form a segment -- they scatter to the
-//      same 27 nodes;
+//   1. scattering particles are counting-sorted by stencil base cell (the
+//      reference's truncated base index, bit-exact) over the CTA's bounding box
+//      of base cells; all particles of one base cell form one segment -- they
+//      scatter to the same 27 nodes -- whatever their order in memory, so
+//      particles that drift across cell boundaries between global sorts do not
+//      fragment the segments.  A CTA whose box has more than kScatterTile cells
+//      compacts instead, and runs of equal base in memory order form segments;
+//   2. each particle stores its B-spline weights and per-particle constants
+//      (10 float4) in shared memory at its sorted slot, swizzled so that
+//      particles about 8 apart fall in different banks;
 //   3. one thread per (segment, i, j) stencil column sums its particles'
 //      contributions to the column's 3 nodes in registers, for as many complete
 //      passes over the threads as there are; the (column, particle) pairs of
@@ -148,49 +151,18 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
                                             int nz, uint32_t &bad)
 {
     const int t = threadIdx.x;
+    int *bins = reinterpret_cast<int *>(&S.tile[0][0]);  // counting-sort bins (the tile is not in use yet)
     __syncthreads();  // S may still be in use by the caller's previous phase
     if (t < 3) { S.lo[t] = INT32_MAX; S.hi[t] = INT32_MIN; }
-    int nact;
-    const int k = block_excl_scan(act ? 1 : 0, &nact);  // compacted slot (syncs)
-    if (nact == 0) return;                               // uniform
+    for (int q = t; q < kScatterTile; q += kScatterChunk) bins[q] = 0;
+    // stencil base cell, as weights() computes it
     int b0 = 0, b1 = 0, b2 = 0;
     if (act) {
-        Weights W;
-        weights(xp, prm.min_bounds, prm.inv_dx, W);
-        b0 = W.base[0]; b1 = W.base[1]; b2 = W.base[2];
-        const float r = prm.rpic_damping;
-        float Cp[9];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b)
-                Cp[3 * a + b] = (1.f - r) * C0[3 * a + b] + (r / 2.f) * (C0[3 * a + b] - C0[3 * b + a]);
-        if (r < -0.001f) {
-#pragma unroll
-            for (int q = 0; q < 9; ++q) Cp[q] = 0.f;
-        }
-        const float mdx = m * prm.dx;
-        float B[9];  // B[3*row + col] = m C'[row][col] dx
-#pragma unroll
-        for (int q = 0; q < 9; ++q) B[q] = Cp[q] * mdx;
-        float a[3];
-#pragma unroll
-        for (int row = 0; row < 3; ++row)
-            a[row] = fma_(-B[3 * row + 0], W.fx[0], fma_(-B[3 * row + 1], W.fx[1], fma_(-B[3 * row + 2], W.fx[2], m * v[row])));
-        const float sc = -(prm.dt * vol) * prm.inv_dx;
-        const int q = scatter_slot(k);
-        S.rec[0][q] = make_float4(W.w[0][0], W.w[0][1], W.w[0][2], m);
-        S.rec[1][q] = make_float4(W.dw[0][0], W.dw[0][1], W.dw[0][2], sc * st6[0]);
-        S.rec[2][q] = make_float4(W.w[1][0], W.w[1][1], W.w[1][2], sc * st6[1]);
-        S.rec[3][q] = make_float4(W.dw[1][0], W.dw[1][1], W.dw[1][2], sc * st6[2]);
-        S.rec[4][q] = make_float4(W.w[2][0], W.w[2][1], W.w[2][2], sc * st6[3]);
-        S.rec[5][q] = make_float4(W.dw[2][0], W.dw[2][1], W.dw[2][2], sc * st6[4]);
-        S.rec[6][q] = make_float4(a[0], a[1], a[2], sc * st6[5]);
-        S.rec[7][q] = make_float4(B[0], B[3], B[6], 0.f);   // Bx = column 0
-        S.rec[8][q] = make_float4(B[1], B[4], B[7], 0.f);   // By
-        S.rec[9][q] = make_float4(B[2], B[5], B[8], 0.f);   // Bz
-        S.base[0][k] = b0; S.base[1][k] = b1; S.base[2][k] = b2;
+        b0 = (int)((xp[0] - prm.min_bounds[0]) * prm.inv_dx - 0.5f);
+        b1 = (int)((xp[1] - prm.min_bounds[1]) * prm.inv_dx - 0.5f);
+        b2 = (int)((xp[2] - prm.min_bounds[2]) * prm.inv_dx - 0.5f);
     }
+    __syncthreads();  // the box's initial values are in place before any warp adds its bounds
     {
         int lo0 = act ? b0 : INT32_MAX, lo1 = act ? b1 : INT32_MAX, lo2 = act ? b2 : INT32_MAX;
         int hi0 = act ? b0 : INT32_MIN, hi1 = act ? b1 : INT32_MIN, hi2 = act ? b2 : INT32_MIN;
@@ -202,14 +174,106 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
         }
     }
     __syncthreads();
-    // segments: runs of equal base in compacted order
-    const bool head = t < nact && (t == 0 || S.base[0][t] != S.base[0][t - 1] ||
-                                   S.base[1][t] != S.base[1][t - 1] || S.base[2][t] != S.base[2][t - 1]);
-    int nseg;
-    const int sidx = block_excl_scan(head ? 1 : 0, &nseg);
-    if (head) S.seg_start[sidx] = t;
-    if (t < nact) S.seg_of[t] = head ? sidx : sidx - 1;
-    if (t == 0) S.seg_start[nseg] = nact;
+    if (S.lo[0] == INT32_MAX) return;  // nothing scatters (uniform)
+    int nact, nseg;
+    {
+        // record of this particle, written at `slot` of segment `seg`
+        auto put_record = [&](int slot, int seg) {
+            Weights W;
+            weights(xp, prm.min_bounds, prm.inv_dx, W);
+            const float r = prm.rpic_damping;
+            float Cp[9];
+#pragma unroll
+            for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+                for (int bb = 0; bb < 3; ++bb)
+                    Cp[3 * aa + bb] = (1.f - r) * C0[3 * aa + bb] + (r / 2.f) * (C0[3 * aa + bb] - C0[3 * bb + aa]);
+            if (r < -0.001f) {
+#pragma unroll
+                for (int q = 0; q < 9; ++q) Cp[q] = 0.f;
+            }
+            const float mdx = m * prm.dx;
+            float B[9];  // B[3*row + col] = m C'[row][col] dx
+#pragma unroll
+            for (int q = 0; q < 9; ++q) B[q] = Cp[q] * mdx;
+            float av[3];
+#pragma unroll
+            for (int row = 0; row < 3; ++row)
+                av[row] = fma_(-B[3 * row + 0], W.fx[0], fma_(-B[3 * row + 1], W.fx[1], fma_(-B[3 * row + 2], W.fx[2], m * v[row])));
+            const float sc = -(prm.dt * vol) * prm.inv_dx;
+            const int q = scatter_slot(slot);
+            S.rec[0][q] = make_float4(W.w[0][0], W.w[0][1], W.w[0][2], m);
+            S.rec[1][q] = make_float4(W.dw[0][0], W.dw[0][1], W.dw[0][2], sc * st6[0]);
+            S.rec[2][q] = make_float4(W.w[1][0], W.w[1][1], W.w[1][2], sc * st6[1]);
+            S.rec[3][q] = make_float4(W.dw[1][0], W.dw[1][1], W.dw[1][2], sc * st6[2]);
+            S.rec[4][q] = make_float4(W.w[2][0], W.w[2][1], W.w[2][2], sc * st6[3]);
+            S.rec[5][q] = make_float4(W.dw[2][0], W.dw[2][1], W.dw[2][2], sc * st6[4]);
+            S.rec[6][q] = make_float4(av[0], av[1], av[2], sc * st6[5]);
+            S.rec[7][q] = make_float4(B[0], B[3], B[6], 0.f);   // Bx = column 0
+            S.rec[8][q] = make_float4(B[1], B[4], B[7], 0.f);   // By
+            S.rec[9][q] = make_float4(B[2], B[5], B[8], 0.f);   // Bz
+            S.base[0][slot] = W.base[0]; S.base[1][slot] = W.base[1]; S.base[2][slot] = W.base[2];
+            S.seg_of[slot] = seg;
+        };
+        const int64_t bey = (int64_t)S.hi[1] - S.lo[1] + 1, bez = (int64_t)S.hi[2] - S.lo[2] + 1;
+        const int64_t nb = ((int64_t)S.hi[0] - S.lo[0] + 1) * bey * bez;
+        if (nb <= kScatterTile) {
+            // counting sort of the scattering particles by base cell: all the
+            // CTA's particles of one base cell form one segment, whatever their
+            // order in memory (particles drift across cell boundaries)
+            const int key = act ? (int)(((b0 - S.lo[0]) * bey + (b1 - S.lo[1])) * bez + (b2 - S.lo[2])) : 0;
+            const int rank = act ? atomicAdd(&bins[key], 1) : 0;
+            __syncthreads();
+            constexpr int kPer = kScatterTile / kScatterChunk;
+            int c[kPer], pc = 0, ne = 0;
+#pragma unroll
+            for (int u = 0; u < kPer; ++u) {
+                const int idx = kPer * t + u;
+                c[u] = idx < nb ? bins[idx] : 0;
+                pc += c[u];
+                ne += c[u] > 0 ? 1 : 0;
+            }
+            // one scan of (nonempty bins << 16 | particles): both prefix sums at once
+            int tot;
+            const int ex0 = block_excl_scan((ne << 16) | pc, &tot);
+            nact = tot & 0xFFFF;
+            nseg = tot >> 16;
+            int po = ex0 & 0xFFFF, so = ex0 >> 16;
+#pragma unroll
+            for (int u = 0; u < kPer; ++u) {
+                const int idx = kPer * t + u;
+                if (c[u] > 0) {
+                    S.seg_start[so] = po;
+                    bins[idx] = (so << 16) | po;
+                    ++so;
+                    po += c[u];
+                }
+            }
+            if (t == 0) S.seg_start[nseg] = nact;
+            __syncthreads();
+            if (act) {
+                const int e = bins[key];
+                put_record((e & 0xFFFF) + rank, e >> 16);
+            }
+        } else {
+            // a CTA spread over too many cells: compact, and let runs of equal
+            // base in memory order form the segments
+            const int k = block_excl_scan(act ? 1 : 0, &nact);
+            if (act) { S.base[0][k] = b0; S.base[1][k] = b1; S.base[2][k] = b2; }
+            __syncthreads();
+            const bool head = t < nact && (t == 0 || S.base[0][t] != S.base[0][t - 1] ||
+                                           S.base[1][t] != S.base[1][t - 1] || S.base[2][t] != S.base[2][t - 1]);
+            const int sidx = block_excl_scan(head ? 1 : 0, &nseg);
+            if (head) S.seg_start[sidx] = t;
+            if (t == 0) S.seg_start[nseg] = nact;
+            const int my_seg = head ? sidx : sidx - 1;  // segment of compacted slot t
+            __syncthreads();
+            if (act) put_record(k, 0);
+            __syncthreads();
+            if (t < nact) S.seg_of[t] = my_seg;
+        }
+    }
+    __syncthreads();  // records, segments and seg_of complete; the bins are free
     const int ox = S.lo[0], oy = S.lo[1], oz = S.lo[2];
     const int64_t ex = (int64_t)S.hi[0] - ox + 3, ey = (int64_t)S.hi[1] - oy + 3, ez = (int64_t)S.hi[2] - oz + 3;
     const bool use_tile = ex * ey * ez <= kScatterTile;
