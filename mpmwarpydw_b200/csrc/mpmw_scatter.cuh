@@ -16,8 +16,9 @@
 //      particles about 8 apart fall in different banks;
 //   3. one thread per (segment, i, j) stencil column sums its particles'
 //      contributions to the column's 3 nodes in registers, for as many complete
-//      passes over the threads as there are; the (column, particle) pairs of
-//      the columns left over are split evenly over all threads;
+//      passes over the threads as there are; each column left over is shared by
+//      a group of lanes of one warp, which combine their partial sums with
+//      shuffles before one of them adds the column;
 //   4. columns are added (shared-memory atomics) into a structure-of-arrays
 //      tile covering the CTA's stencil bounding box -- one float array per
 //      component, so the four adds of a node hit four arrays and lanes of a
@@ -46,7 +47,6 @@ struct ScatterShared {
     float4 rec[10][kScatterChunk];   // per compacted particle (swizzled slot)
     int base[3][kScatterChunk];
     int seg_start[kScatterChunk + 1];
-    int seg_of[kScatterChunk];      // segment of each compacted particle
     float tile[4][kScatterTile];     // m, m vx, m vy, m vz
     int lo[3], hi[3];
 };
@@ -108,6 +108,21 @@ struct ColumnSums {
             if (k > 0) { P01 = __fadd2_rn(P01, dz01); P2 = P2 + dz2; }
             axy[k] = __ffma2_rn(dup2(wz[k]), P01, __ffma2_rn(dup2(dwz[k]), R01, axy[k]));
             az[k] = fma_(wz[k], P2, fma_(dwz[k], R2, az[k]));
+        }
+    }
+
+    // add the sums of lane (this lane ^ o) of the warp (every lane must call)
+    __device__ __forceinline__ void shfl_add(int o)
+    {
+        constexpr unsigned kAll = 0xffffffffu;
+        m01.x += __shfl_xor_sync(kAll, m01.x, o);
+        m01.y += __shfl_xor_sync(kAll, m01.y, o);
+        m2 += __shfl_xor_sync(kAll, m2, o);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            axy[k].x += __shfl_xor_sync(kAll, axy[k].x, o);
+            axy[k].y += __shfl_xor_sync(kAll, axy[k].y, o);
+            az[k] += __shfl_xor_sync(kAll, az[k], o);
         }
     }
 
@@ -177,8 +192,8 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
     if (S.lo[0] == INT32_MAX) return;  // nothing scatters (uniform)
     int nact, nseg;
     {
-        // record of this particle, written at `slot` of segment `seg`
-        auto put_record = [&](int slot, int seg) {
+        // record of this particle, written at `slot`
+        auto put_record = [&](int slot) {
             Weights W;
             weights(xp, prm.min_bounds, prm.inv_dx, W);
             const float r = prm.rpic_damping;
@@ -213,7 +228,6 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
             S.rec[8][q] = make_float4(B[1], B[4], B[7], 0.f);   // By
             S.rec[9][q] = make_float4(B[2], B[5], B[8], 0.f);   // Bz
             S.base[0][slot] = W.base[0]; S.base[1][slot] = W.base[1]; S.base[2][slot] = W.base[2];
-            S.seg_of[slot] = seg;
         };
         const int64_t bey = (int64_t)S.hi[1] - S.lo[1] + 1, bez = (int64_t)S.hi[2] - S.lo[2] + 1;
         const int64_t nb = ((int64_t)S.hi[0] - S.lo[0] + 1) * bey * bez;
@@ -251,10 +265,7 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
             }
             if (t == 0) S.seg_start[nseg] = nact;
             __syncthreads();
-            if (act) {
-                const int e = bins[key];
-                put_record((e & 0xFFFF) + rank, e >> 16);
-            }
+            if (act) put_record((bins[key] & 0xFFFF) + rank);
         } else {
             // a CTA spread over too many cells: compact, and let runs of equal
             // base in memory order form the segments
@@ -266,14 +277,11 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
             const int sidx = block_excl_scan(head ? 1 : 0, &nseg);
             if (head) S.seg_start[sidx] = t;
             if (t == 0) S.seg_start[nseg] = nact;
-            const int my_seg = head ? sidx : sidx - 1;  // segment of compacted slot t
             __syncthreads();
-            if (act) put_record(k, 0);
-            __syncthreads();
-            if (t < nact) S.seg_of[t] = my_seg;
+            if (act) put_record(k);
         }
     }
-    __syncthreads();  // records, segments and seg_of complete; the bins are free
+    __syncthreads();  // records and segments complete; the bins are free
     const int ox = S.lo[0], oy = S.lo[1], oz = S.lo[2];
     const int64_t ex = (int64_t)S.hi[0] - ox + 3, ey = (int64_t)S.hi[1] - oy + 3, ez = (int64_t)S.hi[2] - oz + 3;
     const bool use_tile = ex * ey * ez <= kScatterTile;
@@ -283,13 +291,13 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
     }
     __syncthreads();
 
-    // Work: the pairs (stencil column ij = 3i + j of segment s, particle of s).
-    // Segment s (particles k0..k1-1, L = k1 - k0) owns pairs [9 k0, 9 k1), ordered
-    // by column, then particle; item q = 9 s + ij is one column of one segment.
-    // Complete passes over the threads take whole items (a thread sums its
-    // column's particles in registers and adds the 3 nodes once); the pairs of
-    // the items left over are then split evenly over all threads, each summing a
-    // contiguous run and adding a column whenever its run leaves one.
+    // Work: the items (segment s, stencil column ij = 3i + j), q = 9 s + ij.
+    // Complete passes over the threads take whole items: a thread sums its
+    // column's particles in registers and adds the column's 3 nodes once.  The
+    // items left over (fewer than the threads) get g lanes each (g a power of
+    // two, g x items <= threads): the g lanes of an item take its particles
+    // strided by g, sum their partial columns with warp shuffles, and one adds
+    // the column -- so no two lanes add into the same node at once.
     ColumnSums acc;
     const int items = 9 * nseg;
     const int full_items = (items / kScatterChunk) * kScatterChunk;
@@ -300,36 +308,23 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
         for (int kq = k0; kq < k1; ++kq) acc.add(S, scatter_slot(kq), ij);
         acc.emit(S, k0, ij, use_tile, ox, oy, oz, eyi, ezi, gmv, nx, ny, nz, bad);
     }
-    if (full_items < items) {
-        const int s0 = full_items / 9, ij0 = full_items - 9 * s0;
-        const int pstart = 9 * S.seg_start[s0] + ij0 * (S.seg_start[s0 + 1] - S.seg_start[s0]);
-        const int total = 9 * nact;
-        const int per = (total - pstart + kScatterChunk - 1) / kScatterChunk;
-        int g = pstart + t * per;
-        const int gend = min(total, g + per);
-        if (g < gend) {
-            int s = S.seg_of[g / 9];
-            int k0 = S.seg_start[s], L = S.seg_start[s + 1] - k0;
-            int off = g - 9 * k0;
-            int ij = off / L, r = off - ij * L;
-            acc.zero();
-            for (; g < gend; ++g) {
-                acc.add(S, scatter_slot(k0 + r), ij);
-                ++r;
-                if (r == L || g + 1 == gend) {
-                    acc.emit(S, k0, ij, use_tile, ox, oy, oz, eyi, ezi, gmv, nx, ny, nz, bad);
-                    acc.zero();
-                }
-                if (r == L) {
-                    r = 0;
-                    if (++ij == 9) {
-                        ij = 0;
-                        ++s;
-                        if (s < nseg) { k0 = S.seg_start[s]; L = S.seg_start[s + 1] - k0; }
-                    }
-                }
-            }
+    const int left = items - full_items;  // uniform, < kScatterChunk
+    if (left > 0) {
+        int lg = 0;
+        while (lg < 5 && (left << (lg + 1)) <= kScatterChunk) ++lg;
+        const int q = full_items + (t >> lg), sub = t & ((1 << lg) - 1);
+        const bool mine = q < items;
+        int k0 = 0, ij = 0;
+        acc.zero();
+        if (mine) {
+            const int s = q / 9;
+            ij = q - 9 * s;
+            k0 = S.seg_start[s];
+            const int k1 = S.seg_start[s + 1];
+            for (int kq = k0 + sub; kq < k1; kq += 1 << lg) acc.add(S, scatter_slot(kq), ij);
         }
+        for (int o = (1 << lg) >> 1; o > 0; o >>= 1) acc.shfl_add(o);  // all lanes (full-warp shuffles)
+        if (mine && sub == 0) acc.emit(S, k0, ij, use_tile, ox, oy, oz, eyi, ezi, gmv, nx, ny, nz, bad);
     }
     if (use_tile) {
         __syncthreads();
