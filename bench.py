@@ -101,14 +101,24 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------
-# algorithmic bytes per substep (elastic path; plastic-only fields are extra)
+# algorithmic bytes of one particle-substep (elastic path; plastic-only fields
+# are extra), as the substep's data flow defines them when P2G, the grid
+# update, G2P and the return map each move their own operands:
+#   P2G reads x 12, v 12, C 36, stress 24, mass 4, vol 4, labels 8      = 100
+#   G2P + return map read x 12, labels 8, F 36, 9 material floats 36,
+#   accumulated strain 4, damage 4                                        = 100
+#   writes x 12, v 12, C 36, F 36, stress 24, acc 4, damage 4, ys 4       = 132
+# per grid node: P2G result 16 W, grid pass 16 R + 12 W, G2P 12 R         =  56
 # --------------------------------------------------------------------------
-# fused G2P->stress->P2G, per particle: reads x 12, labels 8, F 36, mu lam ys
-# alpha damage 20, eta_shear eta_bulk 8, mass vol 8; writes x 12, F 36
-BYTES_G2P2G_P = (12 + 8 + 36 + 20 + 8 + 8) + (12 + 36)                            # 140
-# per grid node: the fused kernel reads v (16) and adds into mv (16); the grid
-# update reads mv (16), writes v (16) and clears mv (16)
-BYTES_GRID_NODE = {"g2p2g": 32, "grid": 48}
+SUBSTEP_BYTES_P = 332
+SUBSTEP_BYTES_NODE = 56
+GRID_PASS_BYTES_NODE = 28   # the grid update's own share of the 56
+# What the fused G2P->stress->P2G kernel must move at minimum for the same
+# work: reads x 12, labels 8, F 36, mu lam ys alpha damage 20, eta_shear
+# eta_bulk 8, mass vol 8; writes x 12, F 36 (v, C and the stress stay in
+# registers); per node it reads v 16 and adds into mv 16.
+FUSED_MIN_BYTES_P = (12 + 8 + 36 + 20 + 8 + 8) + (12 + 36)                        # 140
+FUSED_MIN_BYTES_NODE = 32
 
 
 def setup(device, sort=True):
@@ -243,9 +253,12 @@ def run_ours(a):
     K = a.steps
     dom = "g2p2g"
     dom_ms = per[dom] / kb
-    alg_dom = BYTES_G2P2G_P * N + BYTES_GRID_NODE["g2p2g"] * G
+    # one fused launch carries one substep of every particle and the substep's
+    # node traffic except the grid pass (a launch of its own)
+    alg_dom = SUBSTEP_BYTES_P * N + (SUBSTEP_BYTES_NODE - GRID_PASS_BYTES_NODE) * G
     achieved = alg_dom / (dom_ms * 1e-3) / 1e9
-    step_bytes = BYTES_G2P2G_P * N + (BYTES_GRID_NODE["g2p2g"] + BYTES_GRID_NODE["grid"]) * G
+    fused_min = FUSED_MIN_BYTES_P * N + FUSED_MIN_BYTES_NODE * G
+    step_bytes = SUBSTEP_BYTES_P * N + SUBSTEP_BYTES_NODE * G
     traffic = load_traffic(dom)
     value = N * K * world / (ms * 1e-3)
     out = {
@@ -262,6 +275,11 @@ def run_ours(a):
                      "frac": achieved / hbm, "traffic": traffic,
                      "peak_source": f"{peaks.get('source')} (MEASURED_PEAKS.json hbm_gbs)" if peaks.get("source") == "measured" else "fallback 6650 GB/s",
                      "algorithmic_bytes_per_launch": alg_dom,
+                     "bytes_per_particle": SUBSTEP_BYTES_P, "bytes_per_node": SUBSTEP_BYTES_NODE - GRID_PASS_BYTES_NODE,
+                     "fused_min_bytes_per_launch": fused_min,
+                     "fused_min_frac": fused_min / (dom_ms * 1e-3) / 1e9 / hbm,
+                     "dram_GBps": (traffic / (dom_ms * 1e-3) / 1e9) if traffic else None,
+                     "dram_frac": (traffic / (dom_ms * 1e-3) / 1e9 / hbm) if traffic else None,
                      "step_achieved_GBps": step_bytes / (ms / K * 1e-3) / 1e9,
                      "step_frac": step_bytes / (ms / K * 1e-3) / 1e9 / hbm},
         "kernel_ms_per_step": {k: v / kb for k, v in per.items()},

@@ -40,8 +40,10 @@ __device__ __forceinline__ bool gather_prepare(GatherShared &S, bool act, const 
     // one read of the status word per CTA, so the tile decision below is uniform:
     // once any CTA has reported a TMA timeout the rest of the launch gathers from
     // global memory
-    if (t == 0)
+    if (t == 0) {
         S.tma_ok = use_tma && !(status && (*reinterpret_cast<volatile uint32_t *>(status) & MPMW_ST_TIMEOUT));
+        mbar_init(&S.bar, 1);  // used only if the tile fits; the barriers below publish it
+    }
     __syncthreads();
     {
         int lo0 = act ? W.base[0] : INT32_MAX, lo1 = act ? W.base[1] : INT32_MAX, lo2 = act ? W.base[2] : INT32_MAX;
@@ -59,8 +61,6 @@ __device__ __forceinline__ bool gather_prepare(GatherShared &S, bool act, const 
     tile = S.tma_ok && (int64_t)S.hi[0] - ox + 3 <= kTileEdge && (int64_t)S.hi[1] - oy + 3 <= kTileEdge &&
            (int64_t)S.hi[2] - oz + 3 <= kTileEdge;
     if (tile) {
-        if (t == 0) mbar_init(&S.bar, 1);
-        __syncthreads();
         if (t == 0) {
             mbar_arrive_expect_tx(&S.bar, kTileBytes);
             tma_load_4d(S.tile, tmap, 0, oz, oy, ox, &S.bar);

@@ -47,6 +47,27 @@ __device__ __forceinline__ int block_excl_scan(int v, int *total)
     return r;
 }
 
+// The same scan with one barrier: every warp reads all the warp totals from
+// `wsum` (kScanThreads / 32 ints in shared memory).  The caller must not write
+// `wsum` again before its next __syncthreads().
+__device__ __forceinline__ int block_excl_scan_1bar(int v, int *total, int *wsum)
+{
+    constexpr int kWarps = kScanThreads / 32;
+    const int incl = warp_incl_scan(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 31) wsum[wid] = incl;
+    __syncthreads();
+    int before = 0, all = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+        const int s = wsum[w];
+        before += w < wid ? s : 0;
+        all += s;
+    }
+    *total = all;
+    return before + incl - v;
+}
+
 static __global__ void __launch_bounds__(kScanThreads) k_scan_blocks(const int *__restrict__ in, int *__restrict__ out,
                                                              int64_t n, int *__restrict__ block_sums)
 {

@@ -47,6 +47,7 @@ struct ScatterShared {
     float4 rec[10][kScatterChunk];   // per compacted particle (swizzled slot)
     int base[3][kScatterChunk];
     int seg_start[kScatterChunk + 1];
+    int wsum[kScatterChunk / 32];    // warp totals of the counting sort's scan
     int bins[kScatterBins];          // counting-sort bins over the box of base cells
     int lo[3], hi[3];
 };
@@ -143,7 +144,8 @@ struct ColumnSums {
     }
 };
 
-// Every thread of the CTA must call this (it synchronizes the block).
+// Every thread of the CTA must call this (it synchronizes the block), once per
+// CTA: the box bounds S.lo/S.hi are reset before the first barrier.
 // xp: position; v: velocity; C: velocity gradient (row-major); st6: symmetric
 // stress xx yy zz xy xz yz; m, vol: mass and volume.  Values of threads with
 // act == false are ignored.  Out-of-grid nodes are skipped and flagged in `bad`.
@@ -154,8 +156,8 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
 {
     const int t = threadIdx.x;
     int *bins = S.bins;
-    __syncthreads();  // S may still be in use by the caller's previous phase
-    if (t < 3) { S.lo[t] = INT32_MAX; S.hi[t] = INT32_MIN; }
+    if (t < 3) { S.lo[t] = INT32_MAX; S.hi[t] = INT32_MIN; }  // nothing before this call uses them
+    __syncthreads();  // the rest of S may still be in use by the caller's previous phase
     for (int q = t; q < kScatterBins; q += kScatterChunk) bins[q] = 0;
     // stencil base cell, as weights() computes it
     int b0 = 0, b1 = 0, b2 = 0;
@@ -164,7 +166,6 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
         b1 = (int)((xp[1] - prm.min_bounds[1]) * prm.inv_dx - 0.5f);
         b2 = (int)((xp[2] - prm.min_bounds[2]) * prm.inv_dx - 0.5f);
     }
-    __syncthreads();  // the box's initial values are in place before any warp adds its bounds
     {
         int lo0 = act ? b0 : INT32_MAX, lo1 = act ? b1 : INT32_MAX, lo2 = act ? b2 : INT32_MAX;
         int hi0 = act ? b0 : INT32_MIN, hi1 = act ? b1 : INT32_MIN, hi2 = act ? b2 : INT32_MIN;
@@ -236,7 +237,7 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
             }
             // one scan of (nonempty bins << 16 | particles): both prefix sums at once
             int tot;
-            const int ex0 = block_excl_scan((ne << 16) | pc, &tot);
+            const int ex0 = block_excl_scan_1bar((ne << 16) | pc, &tot, S.wsum);
             nact = tot & 0xFFFF;
             nseg = tot >> 16;
             int po = ex0 & 0xFFFF, so = ex0 >> 16;
