@@ -152,6 +152,13 @@ int mpmw_g2p_stress(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_
 /* Bytes of device workspace mpmw_g2p_stress / mpmw_run_substeps need for n
  * particles (a worklist of the particles whose return map takes the SVD path). */
 size_t mpmw_workspace_bytes(int64_t n);
+/* utils/mpmRoutines.py:229-312 compute_stress_from_F_trial followed by
+ * :485-569 p2g_apic_with_stress (the launches at utils/simulationRoutines.py:15-69)
+ * in one pass: F and the stress are written as mpmw_stress writes them and the
+ * scatter accumulates into grid->mv as mpmw_p2g does (the caller zeroes it).
+ * Needs mpmw_workspace_bytes(n) of workspace for the SVD-path worklist. */
+int mpmw_stress_p2g(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
+                    void *workspace, size_t ws_bytes, mpmw_stream_t stream);
 /* The middle of a fused run (utils/simulationRoutines.py:6-293 applied twice):
  * substep k's g2p (mpmRoutines.py:715-802), then substep k+1's
  * compute_stress_from_F_trial (:229-312) and p2g_apic_with_stress (:485-569),

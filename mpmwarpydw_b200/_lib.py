@@ -93,6 +93,8 @@ _SIGS = {
     "mpmw_g2p_stress": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _P, _P,
                              ctypes.c_size_t, _P]),
     "mpmw_workspace_bytes": (ctypes.c_size_t, [_I64]),
+    "mpmw_stress_p2g": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _P, _P,
+                             ctypes.c_size_t, _P]),
     "mpmw_g2p2g": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _I, _P, _P,
                         ctypes.c_size_t, _P]),
     "mpmw_vlc": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params), _P, _P]),

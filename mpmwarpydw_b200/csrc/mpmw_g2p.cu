@@ -13,6 +13,9 @@
 //   last fused step; v and C are rewritten by the final, unfused G2P of a run).
 //   SVD-path particles are listed; k_stress_p2g_list finishes their return map
 //   and scatters them with global atomics.
+// k_stress_p2g: a substep's return map (from F_trial) and its P2G in one pass,
+//   the first half of a substep whenever a workspace is given; SVD-path
+//   particles go to the same worklist and k_stress_p2g_list.
 // The worklists live in the caller's workspace (mpmw_workspace_bytes).
 #include <mutex>
 #include <unordered_map>
@@ -273,6 +276,56 @@ __global__ void __launch_bounds__(kScatterChunk, 3) k_g2p2g(mpmw_particles_t P, 
     if (bad) raise_status(status, bad);
 }
 
+// The return map of a substep and its P2G in one pass (the reference's
+// compute_stress_from_F_trial followed by p2g_apic_with_stress): F_trial -> F
+// and stress (tensor form, in registers) and the CTA-cooperative scatter.  The
+// stress is written as the unfused stress kernel writes it; particles that
+// need the SVD path are listed for k_stress_p2g_list, particles that become
+// XPBD particles write their new v and do not scatter.
+__global__ void __launch_bounds__(kScatterChunk, 3) k_stress_p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
+                                                             uint32_t *status, int *svd_list, int *svd_count)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ScatterShared &S = *reinterpret_cast<ScatterShared *>(smem_raw);
+    const int64_t n = P.n;
+    const int64_t p = (int64_t)blockIdx.x * kScatterChunk + threadIdx.x;
+    const bool act = p < n && P.active[p] == 1 && P.material[p] <= 1;
+    bool scat = false;
+    float xp[3] = {0.f, 0.f, 0.f}, v[3] = {0.f, 0.f, 0.f}, Cg[9], st6[6];
+    float m = 0.f, vol = 0.f;
+    uint32_t bad = 0;
+    if (act) {
+        float Ft[9];
+        load9(P.F_trial, n, p, Ft);
+        load9(P.C, n, p, Cg);
+        load3(P.x, n, p, xp);
+        load3(P.v, n, p, v);
+        float Fo[9], T[9];
+        const int rm = prm.stress_mode == MPMW_STRESS_AUTO ? small_strain_update<true>(P, prm.eff, p, Ft, xp, v, Fo, T)
+                                                           : 0;
+        if (rm != 0) {
+            float out[9];
+            add_viscous(T, Cg, P.eta_shear[p], P.eta_bulk[p], out);
+            store9(P.F, n, p, Fo);
+            store_sym6(P.stress, n, p, out);
+            if (rm == 2) {
+                store3(P.v, n, p, v);  // became an XPBD particle: its v changed, it does not scatter
+            } else {
+                st6[0] = out[0]; st6[1] = out[4]; st6[2] = out[8]; st6[3] = out[1]; st6[4] = out[2]; st6[5] = out[5];
+                m = P.mass[p];
+                vol = P.vol[p];
+                scat = true;
+            }
+        } else {
+            const int slot = atomicAdd(svd_count, 1);
+            svd_list[slot] = (int)p;
+        }
+    }
+    p2g_scatter(S, scat, xp, v, Cg, st6, m, vol, prm, reinterpret_cast<float4 *>(G.mv), G.dims[0], G.dims[1],
+                G.dims[2], bad);
+    if (bad) raise_status(status, bad);
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -417,6 +470,36 @@ int launch_g2p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_par
     if (store_stress) k_g2p2g<true><<<grid, kScatterChunk, smem, s>>>(p, g, prm, st, list, count, map, use_tma, use_ahead);
     else k_g2p2g<false><<<grid, kScatterChunk, smem, s>>>(p, g, prm, st, list, count, map, use_tma, use_ahead);
     MPMW_TRY_LAUNCH("k_g2p2g");
+    k_stress_p2g_list<<<148 * 4, kBlock, 0, s>>>(p, g, prm, st, list, count);
+    return check_launch("k_stress_p2g_list");
+}
+
+static bool g_stress_p2g_attr[64];
+
+int launch_stress_p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st,
+                      void *ws, size_t ws_bytes, cudaStream_t s)
+{
+    if (p.n == 0) return MPMW_OK;
+    if (!ws || ws_bytes < g2p_workspace_bytes(p.n)) {
+        set_error("stress_p2g: workspace of %zu bytes is smaller than the %zu required", ws_bytes,
+                  g2p_workspace_bytes(p.n));
+        return MPMW_E_WORKSPACE;
+    }
+    const size_t smem = sizeof(ScatterShared);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { set_error("stress_p2g: no current device"); return MPMW_E_DEVICE; }
+    if (dev >= 0 && dev < 64 && !g_stress_p2g_attr[dev]) {
+        if (cudaFuncSetAttribute(k_stress_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+            set_error("stress_p2g: cannot reserve %zu bytes of shared memory", smem);
+            return MPMW_E_DEVICE;
+        }
+        g_stress_p2g_attr[dev] = true;
+    }
+    int *count = static_cast<int *>(ws);
+    int *list = reinterpret_cast<int *>(static_cast<char *>(ws) + 256);
+    if (cudaMemsetAsync(count, 0, sizeof(int), s) != cudaSuccess) { set_error("stress_p2g: memset failed"); return MPMW_E_DEVICE; }
+    k_stress_p2g<<<grid_for(p.n, kScatterChunk), kScatterChunk, smem, s>>>(p, g, prm, st, list, count);
+    MPMW_TRY_LAUNCH("k_stress_p2g");
     k_stress_p2g_list<<<148 * 4, kBlock, 0, s>>>(p, g, prm, st, list, count);
     return check_launch("k_stress_p2g_list");
 }

@@ -15,6 +15,8 @@ int launch_g2p(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_param
 int launch_g2p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st,
                  bool store_stress, void *ws, size_t ws_bytes, cudaStream_t s);
 size_t g2p_workspace_bytes(int64_t n);
+int launch_stress_p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st,
+                      void *ws, size_t ws_bytes, cudaStream_t s);
 size_t hash_workspace_bytes(int64_t n);
 
 }  // namespace mpmw

@@ -513,6 +513,16 @@ int mpmw_g2p_stress(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_
     return launch_g2p(*p, *g, *prm, status, true, workspace, ws_bytes, as_stream(stream));
 }
 
+int mpmw_stress_p2g(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, uint32_t *status,
+                    void *workspace, size_t ws_bytes, mpmw_stream_t stream)
+{
+    MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV | kNeedCF | kNeedStress));
+    MPMW_TRY(check_grid(g));
+    MPMW_TRY(check_params(prm));
+    if (p->n > 0 && (!p->vol || !p->mass)) { set_error("stress_p2g: vol and mass are required"); return MPMW_E_ARG; }
+    return launch_stress_p2g(*p, *g, *prm, status, workspace, ws_bytes, as_stream(stream));
+}
+
 int mpmw_g2p2g(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, int store_stress,
                uint32_t *status, void *workspace, size_t ws_bytes, mpmw_stream_t stream)
 {
@@ -574,11 +584,16 @@ int mpmw_run_substeps(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpm
     // stress + P2G, each grid update also clears the accumulators and one
     // G2P->P2G kernel carries substep k's G2P, substep k+1's return map and
     // substep k+1's P2G; the last substep ends with the plain G2P.  Otherwise
-    // every substep is stress, P2G, grid update, G2P (+ VLC).
+    // every substep is stress, P2G, grid update, G2P (+ VLC).  With a
+    // workspace, each stress + P2G is one kernel (k_stress_p2g).
     const bool fuse = !prm->vlc && workspace != nullptr;
-    MPMW_TRY(launch_stress(*p, *prm, s));
-    MPMW_TRY(zero_grid(*g, s));
-    MPMW_TRY(launch_p2g(*p, *g, *prm, status, s));
+    auto stress_then_p2g = [&]() -> int {
+        MPMW_TRY(zero_grid(*g, s));
+        if (workspace) return launch_stress_p2g(*p, *g, *prm, status, workspace, ws_bytes, s);
+        MPMW_TRY(launch_stress(*p, *prm, s));
+        return launch_p2g(*p, *g, *prm, status, s);
+    };
+    MPMW_TRY(stress_then_p2g());
     for (int step = 0; step < nsteps; ++step) {
         const bool last = step == nsteps - 1;
         if (!last && fuse) {
@@ -588,11 +603,7 @@ int mpmw_run_substeps(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpm
             MPMW_TRY(launch_grid(*g, *prm, s));
             MPMW_TRY(launch_g2p(*p, *g, *prm, status, false, nullptr, 0, s));
             if (prm->vlc) MPMW_TRY(launch_vlc(*p, *g, *prm, status, s));
-            if (!last) {
-                MPMW_TRY(launch_stress(*p, *prm, s));
-                MPMW_TRY(zero_grid(*g, s));
-                MPMW_TRY(launch_p2g(*p, *g, *prm, status, s));
-            }
+            if (!last) MPMW_TRY(stress_then_p2g());
         }
     }
     return MPMW_OK;

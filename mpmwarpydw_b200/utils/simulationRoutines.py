@@ -33,10 +33,13 @@ def _structs(sim, mpm, xpbd):
 def mpmSimulationStep(sim, mpm, xpbd, device=None):
     """utils/simulationRoutines.py:6-293: zero grid, stress, P2G, grid update
     (normalise + gravity, damping if < 1, boundary condition), G2P, optional
-    volumetric locking correction."""
+    volumetric locking correction.  The stress and the P2G run as one kernel
+    (the workspace, cached on ``mpm``, holds its SVD-path worklist)."""
     P, G, prm = _structs(sim, mpm, xpbd)
     st = status_word(sim.device)
-    _lib.check(_lib.lib().mpmw_substep(P, G, prm, st.data_ptr(), stream_handle()), "mpmSimulationStep")
+    ws = workspace(mpm, sim.nPoints, sim.device)
+    _lib.check(_lib.lib().mpmw_run_substeps(P, G, prm, 1, st.data_ptr(), ws.data_ptr(), ws.numel(), stream_handle()),
+               "mpmSimulationStep")
 
 
 def run_mpm_substeps(sim, mpm, xpbd, nsteps, device=None):

@@ -258,6 +258,46 @@ def test_fused_multistep_matches_unfused(mode):
         assert rel_err(ga[k], gb[k]) <= tol, (k, rel_err(ga[k], gb[k]))
 
 
+@pytest.mark.parametrize("mode", [0, 1])
+def test_stress_p2g_matches_stress_then_p2g(mode):
+    """mpmw_stress_p2g (return map from F_trial and P2G in one kernel;
+    SVD-path particles -- all of them in mode 1 -- through the list kernel) ==
+    mpmw_stress then mpmw_p2g: F, stress, v, labels and the plastic state bit
+    for bit (the same per-particle operations), grid momentum to atomic-order
+    noise."""
+    torch = _torch()
+    from mpmwarpydw_b200 import _lib
+    from mpmwarpydw_b200.bind import (grid_from_state, params_from_states, particles_from_states, read_status,
+                                      status_word, stream_handle, workspace)
+    L = _lib.lib()
+    a = small_scene(seed=9)
+    b = small_scene(seed=9)
+    xpbd_before = int((a[0].materialLabel == 2).sum().item())
+    out = []
+    for k, (sim, mpm, xpbd) in enumerate((a, b)):
+        mpm.stress_mode = mode
+        P, G, prm = particles_from_states(sim, mpm, xpbd), grid_from_state(mpm), params_from_states(sim, mpm)
+        st = status_word(sim.device)
+        mpm._grid_mv.t.zero_()
+        if k == 0:
+            _lib.check(L.mpmw_stress(P, prm, st.data_ptr(), stream_handle()), "stress")
+            _lib.check(L.mpmw_p2g(P, G, prm, st.data_ptr(), stream_handle()), "p2g")
+        else:
+            ws = workspace(mpm, sim.nPoints, sim.device)
+            _lib.check(L.mpmw_stress_p2g(P, G, prm, st.data_ptr(), ws.data_ptr(), ws.numel(), stream_handle()),
+                       "stress_p2g")
+        torch.cuda.synchronize()
+        assert read_status(sim.device) == 0
+        out.append((gpu_fields(sim, mpm, xpbd), mpm._grid_mv.t.cpu().numpy().copy()))
+    (ga, mva), (gb, mvb) = out
+    assert int((ga["materialLabel"] == 2).sum()) > xpbd_before  # some particles became XPBD particles
+    for k in ("materialLabel", "particle_F", "particle_stress", "particle_v", "particle_damage",
+              "particle_accumulated_strain", "ys", "particle_x"):
+        assert np.array_equal(ga[k], gb[k]), k
+    assert np.abs(mva).max() > 0
+    assert rel_err(mvb, mva) <= TOL
+
+
 def _block_run(cohesion, nsteps):
     """``nsteps`` fused GPU steps of a 4,096-particle Drucker-Prager block collapse
     (the 64k block-collapse scene at reduced size) beside the FP32 and FP64
