@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(kBlock) k_stress_p2g_list(mpmw_particles_t P, 
 }
 
 template <bool Fused>
-__global__ void __launch_bounds__(kBlock) k_g2p(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
+__global__ void __launch_bounds__(kBlock, 3) k_g2p(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
                                                uint32_t *status, int *svd_list, int *svd_count,
                                                const __grid_constant__ CUtensorMap tmap, int use_tma)
 {
@@ -97,10 +97,11 @@ __global__ void __launch_bounds__(kBlock) k_g2p(mpmw_particles_t P, mpmw_grid_t 
     const int64_t n = P.n;
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool act = p < n && P.active[p] == 1 && P.material[p] <= 1;
-    float xp[3] = {0.f, 0.f, 0.f};
+    float xp[3] = {0.f, 0.f, 0.f}, Fpre[9];
     Weights W;
     if (act) {
         load3(P.x, n, p, xp);
+        load9(P.F, n, p, Fpre);  // in flight while the CTA waits for its grid tile
         weights(xp, prm.min_bounds, prm.inv_dx, W);
     }
     bool tile = false;
@@ -115,7 +116,7 @@ __global__ void __launch_bounds__(kBlock) k_g2p(mpmw_particles_t P, mpmw_grid_t 
     for (int a = 0; a < 3; ++a) xn[a] = fma_(prm.dt, nv[a], xp[a]);
     if (!(isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]))) bad |= MPMW_ST_NAN;
     float Ft[9];
-    g2p_deformation(P, prm, p, nF, Ft);
+    g2p_deformation(P, prm, p, nF, Ft, Fpre);
     store3(P.x, n, p, xn);
     store9(P.C, n, p, nC);
     if (Fused) {
