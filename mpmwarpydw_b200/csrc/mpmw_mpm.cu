@@ -312,14 +312,19 @@ __global__ void __launch_bounds__(kBlock) k_stats(mpmw_particles_t P, double *ou
 {
     const int64_t n = P.n;
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    // every field is loaded whatever the labels, so the loads of several
+    // iterations are in flight together
+#pragma unroll 4
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
-        bool act = P.active[p] == 1, xp = P.material[p] == 2;
+        const int a = P.active[p], mt = P.material[p];
+        float v3[3];
+        load3(P.v, n, p, v3);
+        const float r = P.radius[p], dmg = P.damage[p];
+        const bool act = a == 1, xp = mt == 2;
         if (act) {
-            float v3[3];
-            load3(P.v, n, p, v3);
-            acc[0] += (double)(len3(v3) / P.radius[p]);
+            acc[0] += (double)(len3(v3) / r);
             acc[1] += 1.0;
-            acc[2] += (double)P.damage[p];
+            acc[2] += (double)dmg;
         }
         if (xp) { if (act) acc[4] += 1.0; else acc[6] += 1.0; }
         else { if (act) acc[3] += 1.0; else acc[5] += 1.0; }
