@@ -96,14 +96,18 @@ __global__ void __launch_bounds__(kBlock, 3) k_g2p(mpmw_particles_t P, mpmw_grid
     __shared__ __align__(128) GatherShared S;
     const int64_t n = P.n;
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool act = p < n && P.active[p] == 1 && P.material[p] <= 1;
+    // labels, x and F are loaded together (not behind the label test)
+    int lab_a = 0, lab_m = 0;
     float xp[3] = {0.f, 0.f, 0.f}, Fpre[9];
-    Weights W;
-    if (act) {
+    if (p < n) {
+        lab_a = P.active[p];
+        lab_m = P.material[p];
         load3(P.x, n, p, xp);
         load9(P.F, n, p, Fpre);  // in flight while the CTA waits for its grid tile
-        weights(xp, prm.min_bounds, prm.inv_dx, W);
     }
+    const bool act = lab_a == 1 && lab_m <= 1;
+    Weights W;
+    if (act) weights(xp, prm.min_bounds, prm.inv_dx, W);
     bool tile = false;
     int ox = 0, oy = 0, oz = 0;
     if (!gather_prepare(S, act, W, &tmap, use_tma, status, tile, ox, oy, oz)) return;
@@ -196,13 +200,17 @@ __global__ void __launch_bounds__(kScatterChunk, 3) k_g2p2g(mpmw_particles_t P, 
 #pragma unroll 1
         for (int f = 0; f < kAheadFields; ++f) bulk_load(&AF.f[f][0], ahead_src(P, f) + p0, kScatterChunk * 4u, &S.pbar);
     }
-    const bool act = p < n && P.active[p] == 1 && P.material[p] <= 1;
+    // labels and x are loaded together (not behind the label test)
+    int lab_a = 0, lab_m = 0;
     float xp[3] = {0.f, 0.f, 0.f};
-    Weights W;
-    if (act) {
+    if (p < n) {
+        lab_a = P.active[p];
+        lab_m = P.material[p];
         load3(P.x, n, p, xp);
-        weights(xp, prm.min_bounds, prm.inv_dx, W);
     }
+    const bool act = lab_a == 1 && lab_m <= 1;
+    Weights W;
+    if (act) weights(xp, prm.min_bounds, prm.inv_dx, W);
     bool tile = false;
     int ox = 0, oy = 0, oz = 0;
     if (!gather_prepare(S.g, act, W, &tmap, use_tma, status, tile, ox, oy, oz)) {
@@ -290,17 +298,22 @@ __global__ void __launch_bounds__(kScatterChunk, 3) k_stress_p2g(mpmw_particles_
     ScatterShared &S = *reinterpret_cast<ScatterShared *>(smem_raw);
     const int64_t n = P.n;
     const int64_t p = (int64_t)blockIdx.x * kScatterChunk + threadIdx.x;
-    const bool act = p < n && P.active[p] == 1 && P.material[p] <= 1;
     bool scat = false;
-    float xp[3] = {0.f, 0.f, 0.f}, v[3] = {0.f, 0.f, 0.f}, Cg[9], st6[6];
+    float xp[3] = {0.f, 0.f, 0.f}, v[3] = {0.f, 0.f, 0.f}, Cg[9], st6[6], Ft[9];
     float m = 0.f, vol = 0.f;
     uint32_t bad = 0;
-    if (act) {
-        float Ft[9];
+    // labels and the particle's fields are loaded together (not behind the label test)
+    int lab_a = 0, lab_m = 0;
+    if (p < n) {
+        lab_a = P.active[p];
+        lab_m = P.material[p];
         load9(P.F_trial, n, p, Ft);
         load9(P.C, n, p, Cg);
         load3(P.x, n, p, xp);
         load3(P.v, n, p, v);
+    }
+    const bool act = lab_a == 1 && lab_m <= 1;
+    if (act) {
         float Fo[9], T[9];
         const int rm = prm.stress_mode == MPMW_STRESS_AUTO ? small_strain_update<true>(P, prm.eff, p, Ft, xp, v, Fo, T)
                                                            : 0;

@@ -16,10 +16,13 @@ __global__ void __launch_bounds__(kScatterChunk) k_p2g(mpmw_particles_t P, mpmw_
     ScatterShared &S = *reinterpret_cast<ScatterShared *>(smem_raw);
     const int64_t n = P.n;
     const int64_t p = (int64_t)blockIdx.x * kScatterChunk + threadIdx.x;
-    const bool act = p < n && P.active[p] == 1 && P.material[p] <= 1;
+    // labels and the particle's fields are loaded together (not behind the label test)
+    int lab_a = 0, lab_m = 0;
     float xp[3] = {0.f, 0.f, 0.f}, v[3] = {0.f, 0.f, 0.f}, C0[9], st6[6];
     float m = 0.f, vol = 0.f;
-    if (act) {
+    if (p < n) {
+        lab_a = P.active[p];
+        lab_m = P.material[p];
         load3(P.x, n, p, xp);
         load3(P.v, n, p, v);
         load9(P.C, n, p, C0);
@@ -28,6 +31,7 @@ __global__ void __launch_bounds__(kScatterChunk) k_p2g(mpmw_particles_t P, mpmw_
         m = P.mass[p];
         vol = P.vol[p];
     }
+    const bool act = lab_a == 1 && lab_m <= 1;
     uint32_t bad = 0;
     p2g_scatter(S, act, xp, v, C0, st6, m, vol, prm, reinterpret_cast<float4 *>(G.mv), G.dims[0], G.dims[1],
                 G.dims[2], bad);
