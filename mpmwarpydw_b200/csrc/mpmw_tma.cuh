@@ -54,17 +54,34 @@ __device__ __forceinline__ uint64_t globaltimer_ns()
     return t;
 }
 
-// Wait for phase `phase` of the barrier for at most kMbarWaitNs of wall time
-// (non-blocking polls with a short back-off); false if it never completed.
+// Potentially blocking test: the hardware suspends the thread until the phase
+// completes or about `hint_ns` nanoseconds pass, whichever is first.
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned phase, unsigned hint_ns)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(phase), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for phase `phase` of the barrier for at most kMbarWaitNs of wall time;
+// false if it never completed.  Each poll suspends the warp in hardware (at
+// most kMbarSuspendNs), so a warp waiting on a copy does not take issue slots
+// from the warps that compute; the wall-time bound is checked between polls.
 constexpr uint64_t kMbarWaitNs = 200ull * 1000ull * 1000ull;  // 200 ms
+constexpr unsigned kMbarSuspendNs = 20000u;                   // 20 us per poll at most
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned phase)
 {
     if (mbar_test_wait(bar, phase)) return true;
     const uint64_t t0 = globaltimer_ns();
     for (int i = 0; i < kMbarMaxPolls; ++i) {
-        if (mbar_test_wait(bar, phase)) return true;
+        if (mbar_try_wait(bar, phase, kMbarSuspendNs)) return true;
         if (globaltimer_ns() - t0 > kMbarWaitNs) return false;
-        __nanosleep(32);
     }
     return false;
 }
