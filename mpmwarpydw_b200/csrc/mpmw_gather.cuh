@@ -80,7 +80,9 @@ __device__ __forceinline__ bool gather_prepare(GatherShared &S, bool act, const 
 // components share every weight, so they are summed as float2 pairs with the
 // packed FP32 FMA (__ffma2_rn: two FMAs, each rounded once, in one
 // instruction); the z component is summed alone.  Same operations and
-// rounding as three scalar FMAs.
+// rounding as three scalar FMAs.  The moment sums (i, j, k times the weight)
+// skip the terms whose factor is exactly 0: for finite grid velocities they
+// add +-0 and leave the sum unchanged.
 __device__ __forceinline__ float2 ffma2(float w, float2 g, float2 acc) { return __ffma2_rn(make_float2(w, w), g, acc); }
 
 __device__ __forceinline__ void gather_particle(const GatherShared &S, bool tile, int ox, int oy, int oz,
@@ -115,21 +117,21 @@ __device__ __forceinline__ void gather_particle(const GatherShared &S, bool tile
                 const float2 gxy = make_float2(g.x, g.y);
                 Sv2 = ffma2(wz, gxy, Sv2); Svz = fma_(wz, g.z, Svz);
                 Tv2 = ffma2(dwz, gxy, Tv2); Tvz = fma_(dwz, g.z, Tvz);
-                Uv2 = ffma2(kwz, gxy, Uv2); Uvz = fma_(kwz, g.z, Uvz);
+                if (k > 0) { Uv2 = ffma2(kwz, gxy, Uv2); Uvz = fma_(kwz, g.z, Uvz); }  // k = 0 adds 0 * g
             }
             const float wy = W.w[1][j], dwy = W.dw[1][j], jwy = (float)j * wy;
             SS2 = ffma2(wy, Sv2, SS2); SSz = fma_(wy, Svz, SSz);
             SD2 = ffma2(dwy, Sv2, SD2); SDz = fma_(dwy, Svz, SDz);
             TS2 = ffma2(wy, Tv2, TS2); TSz = fma_(wy, Tvz, TSz);
             US2 = ffma2(wy, Uv2, US2); USz = fma_(wy, Uvz, USz);
-            SJ2 = ffma2(jwy, Sv2, SJ2); SJz = fma_(jwy, Svz, SJz);
+            if (j > 0) { SJ2 = ffma2(jwy, Sv2, SJ2); SJz = fma_(jwy, Svz, SJz); }  // j = 0 adds 0 * Sv
         }
         const float wx = W.w[0][i], dwx = W.dw[0][i], iwx = (float)i * wx;
         v2 = ffma2(wx, SS2, v2); vz = fma_(wx, SSz, vz);
         gx2 = ffma2(dwx, SS2, gx2); gxz = fma_(dwx, SSz, gxz);
         gy2 = ffma2(wx, SD2, gy2); gyz = fma_(wx, SDz, gyz);
         gz2 = ffma2(wx, TS2, gz2); gzz = fma_(wx, TSz, gzz);
-        Mi2 = ffma2(iwx, SS2, Mi2); Miz = fma_(iwx, SSz, Miz);
+        if (i > 0) { Mi2 = ffma2(iwx, SS2, Mi2); Miz = fma_(iwx, SSz, Miz); }  // i = 0 adds 0 * SS
         Mj2 = ffma2(wx, SJ2, Mj2); Mjz = fma_(wx, SJz, Mjz);
         Mk2 = ffma2(wx, US2, Mk2); Mkz = fma_(wx, USz, Mkz);
     }
