@@ -121,11 +121,15 @@ def test_p2g_matches_oracle():
     assert abs(g["grid_m"].sum(dtype=np.float64) - s.particle_mass[act].sum(dtype=np.float64)) <= 1e-5 * s.particle_mass[act].sum()
 
 
-def test_p2g_untiled_order_matches():
-    """Random particle order defeats the shared-memory tiles (global-atomic path)."""
+@pytest.mark.parametrize("n_side", [10, 24])
+def test_p2g_random_order_matches(n_side):
+    """P2G of randomly ordered particles == P2G in memory order (to atomic-order
+    noise).  At n_side 10 a CTA's 256 random particles span the scene's 125
+    base cells and take the counting sort; at n_side 24 they span 1,728 cells,
+    more than the sort's 1,024 bins, and take the compaction fallback."""
     torch = _torch()
     from mpmwarpydw_b200.utils import mpmRoutines as M
-    sim, mpm, xpbd = small_scene(seed=4)
+    sim, mpm, xpbd = small_scene(seed=4, n_side=n_side)
     perm = torch.randperm(sim.nPoints, device="cuda")
     args = [sim.activeLabel[perm].contiguous(), sim.materialLabel[perm].contiguous(), mpm.particle_stress[perm],
             sim.particle_x[perm], sim.particle_v[perm], mpm.particle_C[perm], sim.particle_vol[perm].contiguous(),
@@ -139,6 +143,57 @@ def test_p2g_untiled_order_matches():
     torch.cuda.synchronize()
     assert rel_err(gm.cpu().numpy(), mpm.grid_m.cpu().numpy()) <= TOL
     assert rel_err(gv.cpu().numpy(), mpm.grid_v_in.cpu().numpy()) <= TOL
+
+
+def test_fused_multistep_ragged_count():
+    """run_mpm_substeps(k) == k x mpmSimulationStep at 1,331 particles: a
+    partial last CTA, and a particle count that is not a multiple of 4, so the
+    fused kernel reads its particle fields without the bulk read-ahead."""
+    torch = _torch()
+    from mpmwarpydw_b200.utils import simulationRoutines as S
+    a = small_scene(seed=12, n_side=11)
+    b = small_scene(seed=12, n_side=11)
+    assert a[0].nPoints == 1331
+    for _ in range(4):
+        S.mpmSimulationStep(*a, "cuda:0")
+    S.run_mpm_substeps(*b, 4)
+    torch.cuda.synchronize()
+    ga, gb = gpu_fields(*a), gpu_fields(*b)
+    assert np.array_equal(ga["materialLabel"], gb["materialLabel"])
+    for k, tol in (("particle_x", 1e-5), ("particle_v", 1e-4), ("particle_C", 1e-4), ("particle_F", 1e-5),
+                   ("particle_F_trial", 1e-5), ("particle_stress", 1e-3), ("particle_damage", 1e-3)):
+        assert rel_err(ga[k], gb[k]) <= tol, (k, rel_err(ga[k], gb[k]))
+
+
+def test_empty_inputs_are_no_ops():
+    """Zero particles (or zero substeps): every particle entry point returns OK,
+    raises no status bit and leaves the particle fields as they were."""
+    torch = _torch()
+    from mpmwarpydw_b200 import _lib
+    from mpmwarpydw_b200.bind import (grid_from_state, params_from_states, particles_from_states, read_status,
+                                      status_word, stream_handle, workspace)
+    L = _lib.lib()
+    sim, mpm, xpbd = small_scene(seed=13)
+    before = gpu_fields(sim, mpm, xpbd)
+    P, G, prm = particles_from_states(sim, mpm, xpbd), grid_from_state(mpm), params_from_states(sim, mpm)
+    st = status_word(sim.device)
+    ws = workspace(mpm, sim.nPoints, sim.device)
+    sh = stream_handle()
+    _lib.check(L.mpmw_run_substeps(P, G, prm, 0, st.data_ptr(), ws.data_ptr(), ws.numel(), sh), "0 substeps")
+    P.n = 0
+    _lib.check(L.mpmw_stress(P, prm, st.data_ptr(), sh), "stress")
+    _lib.check(L.mpmw_p2g(P, G, prm, st.data_ptr(), sh), "p2g")
+    _lib.check(L.mpmw_stress_p2g(P, G, prm, st.data_ptr(), ws.data_ptr(), ws.numel(), sh), "stress_p2g")
+    _lib.check(L.mpmw_g2p(P, G, prm, st.data_ptr(), sh), "g2p")
+    _lib.check(L.mpmw_g2p2g(P, G, prm, 1, st.data_ptr(), ws.data_ptr(), ws.numel(), sh), "g2p2g")
+    _lib.check(L.mpmw_run_substeps(P, G, prm, 3, st.data_ptr(), ws.data_ptr(), ws.numel(), sh), "run_substeps")
+    _lib.check(L.mpmw_substep(P, G, prm, st.data_ptr(), sh), "substep")
+    torch.cuda.synchronize()
+    assert read_status(sim.device) == 0
+    after = gpu_fields(sim, mpm, xpbd)
+    for k in ("particle_x", "particle_v", "particle_C", "particle_F", "particle_F_trial", "particle_stress",
+              "materialLabel", "particle_damage"):
+        assert np.array_equal(before[k], after[k]), k
 
 
 @pytest.mark.parametrize("bc", ["friction", "friction_gradual", "restitution", "absorbing", "plane_strain_y",
