@@ -226,6 +226,7 @@ __global__ void __launch_bounds__(kScatterChunk, 3) k_g2p2g(mpmw_particles_t P, 
         mbar_wait_bounded(&S.pbar, 0);
         ahead_ok = false;
     }
+
     bool scat = false;
     float xn[3] = {0.f, 0.f, 0.f}, nv[3] = {0.f, 0.f, 0.f}, nC[9], st6[6];
     float m = 0.f, vol = 0.f;
@@ -302,8 +303,11 @@ __global__ void __launch_bounds__(kScatterChunk, 3) k_stress_p2g(mpmw_particles_
     float xp[3] = {0.f, 0.f, 0.f}, v[3] = {0.f, 0.f, 0.f}, Cg[9], st6[6], Ft[9];
     float m = 0.f, vol = 0.f;
     uint32_t bad = 0;
-    // labels and the particle's fields are loaded together (not behind the label test)
+    // labels and every field the elastic path reads are loaded together (not
+    // behind the label test, not inside the return map)
     int lab_a = 0, lab_m = 0;
+    MatScalars ms{0.f, 0.f, 0.f, 0.f, 0.f};
+    float eta_s = 0.f, eta_b = 0.f, mass = 0.f, volume = 0.f;
     if (p < n) {
         lab_a = P.active[p];
         lab_m = P.material[p];
@@ -311,23 +315,27 @@ __global__ void __launch_bounds__(kScatterChunk, 3) k_stress_p2g(mpmw_particles_
         load9(P.C, n, p, Cg);
         load3(P.x, n, p, xp);
         load3(P.v, n, p, v);
+        ms.mu = P.mu[p]; ms.lam = P.lam[p]; ms.ys = P.ys[p]; ms.alpha = P.alpha[p]; ms.D = P.damage[p];
+        eta_s = P.eta_shear[p]; eta_b = P.eta_bulk[p];
+        mass = P.mass[p]; volume = P.vol[p];
     }
     const bool act = lab_a == 1 && lab_m <= 1;
     if (act) {
         float Fo[9], T[9];
-        const int rm = prm.stress_mode == MPMW_STRESS_AUTO ? small_strain_update<true>(P, prm.eff, p, Ft, xp, v, Fo, T)
-                                                           : 0;
+        const int rm = prm.stress_mode == MPMW_STRESS_AUTO
+                           ? small_strain_update<true>(P, prm.eff, p, Ft, xp, v, Fo, T, &ms)
+                           : 0;
         if (rm != 0) {
             float out[9];
-            add_viscous(T, Cg, P.eta_shear[p], P.eta_bulk[p], out);
+            add_viscous(T, Cg, eta_s, eta_b, out);
             store9(P.F, n, p, Fo);
             store_sym6(P.stress, n, p, out);
             if (rm == 2) {
                 store3(P.v, n, p, v);  // became an XPBD particle: its v changed, it does not scatter
             } else {
                 st6[0] = out[0]; st6[1] = out[4]; st6[2] = out[8]; st6[3] = out[1]; st6[4] = out[2]; st6[5] = out[5];
-                m = P.mass[p];
-                vol = P.vol[p];
+                m = mass;
+                vol = volume;
                 scat = true;
             }
         } else {
