@@ -200,6 +200,11 @@ __global__ void __launch_bounds__(kScatterChunk, 3) k_g2p2g(mpmw_particles_t P, 
 #pragma unroll 1
         for (int f = 0; f < kAheadFields; ++f) bulk_load(&AF.f[f][0], ahead_src(P, f) + p0, kScatterChunk * 4u, &S.pbar);
     }
+    // the scatter's counting-sort bins and out-of-box flag, cleared here and
+    // published by the gather's first barrier (the scatter then needs no box
+    // reduction of its own: see below)
+    for (int q = t; q < kScatterBins; q += kScatterChunk) S.s.bins[q] = 0;
+    if (t == 0) S.s.outside = 0;
     // labels and x are loaded together (not behind the label test)
     int lab_a = 0, lab_m = 0;
     float xp[3] = {0.f, 0.f, 0.f};
@@ -281,8 +286,24 @@ __global__ void __launch_bounds__(kScatterChunk, 3) k_g2p2g(mpmw_particles_t P, 
             svd_list[atomicAdd(svd_count, 1)] = (int)p;
         }
     }
+    // A particle moves less than a cell per substep, so the gather's box of
+    // stencil bases (old positions), one cell wider on each side, holds every
+    // new base; a particle outside it sends the CTA to the scatter's
+    // compaction path.
+    ScatterBox box;
+    bool have_box = true;
+    int64_t cells = 1;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int64_t lo = (int64_t)S.g.lo[a] - 1, e = (int64_t)S.g.hi[a] - S.g.lo[a] + 3;
+        have_box = have_box && e > 0 && e <= kScatterBins && lo >= INT32_MIN;
+        box.lo[a] = have_box ? (int)lo : 0;
+        box.ext[a] = have_box ? (int)e : 1;
+        cells *= have_box ? e : 1;
+    }
+    have_box = have_box && cells <= kScatterBins;
     p2g_scatter(S.s, scat, xn, nv, nC, st6, m, vol, prm, reinterpret_cast<float4 *>(G.mv), G.dims[0], G.dims[1],
-                G.dims[2], bad);
+                G.dims[2], bad, have_box ? &box : nullptr);
     if (bad) raise_status(status, bad);
 }
 

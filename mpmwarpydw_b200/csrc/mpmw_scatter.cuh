@@ -48,6 +48,7 @@ struct ScatterShared {
     int base[3][kScatterChunk];
     int seg_start[kScatterChunk + 1];
     int wsum[kScatterChunk / 32];    // warp totals of the counting sort's scan
+    int outside;                     // a particle's base fell outside a known box
     int bins[kScatterBins];          // counting-sort bins over the box of base cells
     int lo[3], hi[3];
 };
@@ -144,6 +145,15 @@ struct ColumnSums {
     }
 };
 
+// A box of base cells that the caller knows to hold the base of every
+// scattering particle (lo and extents, at most kScatterBins cells), so the
+// scatter need not reduce one.  The caller zeroes S.bins and S.outside before
+// a barrier every thread passes before this call.  A particle found outside
+// the box sets S.outside, and the CTA then forms its segments by compaction.
+struct ScatterBox {
+    int lo[3], ext[3];
+};
+
 // Every thread of the CTA must call this (it synchronizes the block), once per
 // CTA: the box bounds S.lo/S.hi are reset before the first barrier.
 // xp: position; v: velocity; C: velocity gradient (row-major); st6: symmetric
@@ -152,13 +162,10 @@ struct ColumnSums {
 __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const float *xp, const float *v,
                                             const float *C0, const float *st6, float m, float vol,
                                             const mpmw_params_t &prm, float4 *__restrict__ gmv, int nx, int ny,
-                                            int nz, uint32_t &bad)
+                                            int nz, uint32_t &bad, const ScatterBox *known = nullptr)
 {
     const int t = threadIdx.x;
     int *bins = S.bins;
-    if (t < 3) { S.lo[t] = INT32_MAX; S.hi[t] = INT32_MIN; }  // nothing before this call uses them
-    __syncthreads();  // the rest of S may still be in use by the caller's previous phase
-    for (int q = t; q < kScatterBins; q += kScatterChunk) bins[q] = 0;
     // stencil base cell, as weights() computes it
     int b0 = 0, b1 = 0, b2 = 0;
     if (act) {
@@ -166,18 +173,54 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
         b1 = (int)((xp[1] - prm.min_bounds[1]) * prm.inv_dx - 0.5f);
         b2 = (int)((xp[2] - prm.min_bounds[2]) * prm.inv_dx - 0.5f);
     }
-    {
-        int lo0 = act ? b0 : INT32_MAX, lo1 = act ? b1 : INT32_MAX, lo2 = act ? b2 : INT32_MAX;
-        int hi0 = act ? b0 : INT32_MIN, hi1 = act ? b1 : INT32_MIN, hi2 = act ? b2 : INT32_MIN;
-        lo0 = __reduce_min_sync(0xffffffffu, lo0); lo1 = __reduce_min_sync(0xffffffffu, lo1); lo2 = __reduce_min_sync(0xffffffffu, lo2);
-        hi0 = __reduce_max_sync(0xffffffffu, hi0); hi1 = __reduce_max_sync(0xffffffffu, hi1); hi2 = __reduce_max_sync(0xffffffffu, hi2);
-        if ((t & 31) == 0) {
-            atomicMin(&S.lo[0], lo0); atomicMin(&S.lo[1], lo1); atomicMin(&S.lo[2], lo2);
-            atomicMax(&S.hi[0], hi0); atomicMax(&S.hi[1], hi1); atomicMax(&S.hi[2], hi2);
+    // the box of base cells the counting sort runs over, and each particle's
+    // bin and rank in it
+    int o0, o1, o2;
+    int64_t bey, bez, nb;
+    int key = 0, rank = 0;
+    bool use_bins;
+    if (known) {
+        o0 = known->lo[0]; o1 = known->lo[1]; o2 = known->lo[2];
+        bey = known->ext[1]; bez = known->ext[2];
+        nb = (int64_t)known->ext[0] * bey * bez;
+        if (act) {
+            const int64_t r0 = (int64_t)b0 - o0, r1 = (int64_t)b1 - o1, r2 = (int64_t)b2 - o2;
+            if (r0 >= 0 && r1 >= 0 && r2 >= 0 && r0 < known->ext[0] && r1 < bey && r2 < bez) {
+                key = (int)((r0 * bey + r1) * bez + r2);
+                rank = atomicAdd(&bins[key], 1);
+            } else {
+                S.outside = 1;
+            }
+        }
+        __syncthreads();  // bins counted, outside flag set
+        use_bins = S.outside == 0;
+    } else {
+        if (t < 3) { S.lo[t] = INT32_MAX; S.hi[t] = INT32_MIN; }  // nothing before this call uses them
+        __syncthreads();  // the rest of S may still be in use by the caller's previous phase
+        for (int q = t; q < kScatterBins; q += kScatterChunk) bins[q] = 0;
+        {
+            int lo0 = act ? b0 : INT32_MAX, lo1 = act ? b1 : INT32_MAX, lo2 = act ? b2 : INT32_MAX;
+            int hi0 = act ? b0 : INT32_MIN, hi1 = act ? b1 : INT32_MIN, hi2 = act ? b2 : INT32_MIN;
+            lo0 = __reduce_min_sync(0xffffffffu, lo0); lo1 = __reduce_min_sync(0xffffffffu, lo1); lo2 = __reduce_min_sync(0xffffffffu, lo2);
+            hi0 = __reduce_max_sync(0xffffffffu, hi0); hi1 = __reduce_max_sync(0xffffffffu, hi1); hi2 = __reduce_max_sync(0xffffffffu, hi2);
+            if ((t & 31) == 0) {
+                atomicMin(&S.lo[0], lo0); atomicMin(&S.lo[1], lo1); atomicMin(&S.lo[2], lo2);
+                atomicMax(&S.hi[0], hi0); atomicMax(&S.hi[1], hi1); atomicMax(&S.hi[2], hi2);
+            }
+        }
+        __syncthreads();
+        if (S.lo[0] == INT32_MAX) return;  // nothing scatters (uniform)
+        o0 = S.lo[0]; o1 = S.lo[1]; o2 = S.lo[2];
+        bey = (int64_t)S.hi[1] - o1 + 1;
+        bez = (int64_t)S.hi[2] - o2 + 1;
+        nb = ((int64_t)S.hi[0] - o0 + 1) * bey * bez;
+        use_bins = nb <= kScatterBins;
+        if (use_bins) {
+            key = act ? (int)(((b0 - o0) * bey + (b1 - o1)) * bez + (b2 - o2)) : 0;
+            rank = act ? atomicAdd(&bins[key], 1) : 0;
+            __syncthreads();
         }
     }
-    __syncthreads();
-    if (S.lo[0] == INT32_MAX) return;  // nothing scatters (uniform)
     int nact, nseg;
     {
         // record of this particle, written at `slot`
@@ -217,15 +260,10 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
             S.rec[9][q] = make_float4(B[2], B[5], B[8], 0.f);   // Bz
             S.base[0][slot] = W.base[0]; S.base[1][slot] = W.base[1]; S.base[2][slot] = W.base[2];
         };
-        const int64_t bey = (int64_t)S.hi[1] - S.lo[1] + 1, bez = (int64_t)S.hi[2] - S.lo[2] + 1;
-        const int64_t nb = ((int64_t)S.hi[0] - S.lo[0] + 1) * bey * bez;
-        if (nb <= kScatterBins) {
+        if (use_bins) {
             // counting sort of the scattering particles by base cell: all the
             // CTA's particles of one base cell form one segment, whatever their
             // order in memory (particles drift across cell boundaries)
-            const int key = act ? (int)(((b0 - S.lo[0]) * bey + (b1 - S.lo[1])) * bez + (b2 - S.lo[2])) : 0;
-            const int rank = act ? atomicAdd(&bins[key], 1) : 0;
-            __syncthreads();
             constexpr int kPer = kScatterBins / kScatterChunk;
             int c[kPer], pc = 0, ne = 0;
 #pragma unroll
