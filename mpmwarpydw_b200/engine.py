@@ -3,8 +3,8 @@
 ``sort_particles`` reorders every per-particle array of the three state
 objects into 4x4x4-cell block order (a one-time set-up step; the reference's
 results do not depend on particle order).  Consecutive particles then share
-grid cells, which is what the P2G kernel's shared-memory tiles and the G2P
-kernel's cached grid reads rely on.  ``sim.particle_order`` keeps, for each
+grid cells, which is what the scatter's per-CTA counting sort (long segments of
+one base cell) and the G2P kernels' grid tiles (one TMA copy per CTA) rely on.  ``sim.particle_order`` keeps, for each
 stored particle, its index in the original input so results can be written
 back in input order (:func:`original_order`).
 
