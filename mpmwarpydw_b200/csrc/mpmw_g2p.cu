@@ -177,7 +177,7 @@ __device__ __forceinline__ const float *ahead_src(const mpmw_particles_t &P, int
 // which the caller has zeroed).  StoreStress: also write the stress (the last
 // fused substep of a run).
 template <bool StoreStress>
-__global__ void __launch_bounds__(kScatterChunk, 3) k_g2p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
+__global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
                                                         uint32_t *status, int *svd_list, int *svd_count,
                                                         const __grid_constant__ CUtensorMap tmap, int use_tma,
                                                         int use_ahead)
@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(kScatterChunk, 3) k_g2p2g(mpmw_particles_t P, 
 // stress is written as the unfused stress kernel writes it; particles that
 // need the SVD path are listed for k_stress_p2g_list, particles that become
 // XPBD particles write their new v and do not scatter.
-__global__ void __launch_bounds__(kScatterChunk, 3) k_stress_p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
+__global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_stress_p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
                                                              uint32_t *status, int *svd_list, int *svd_count)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -24,11 +24,13 @@ __device__ __forceinline__ int warp_incl_scan(int v)
     return v;
 }
 
-// block-wide exclusive scan of one int per thread (blockDim.x == kScanThreads);
-// returns the exclusive value and stores the block sum in *total in every thread
+// block-wide exclusive scan of one int per thread (blockDim.x == kThreads, a
+// multiple of 32 up to 1024); returns the exclusive value and stores the block
+// sum in *total in every thread
+template <int kThreads = kScanThreads>
 __device__ __forceinline__ int block_excl_scan(int v, int *total)
 {
-    constexpr int kWarps = kScanThreads / 32;
+    constexpr int kWarps = kThreads / 32;
     __shared__ int warp_sums[kWarps + 1];
     int incl = warp_incl_scan(v);
     int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -48,11 +50,12 @@ __device__ __forceinline__ int block_excl_scan(int v, int *total)
 }
 
 // The same scan with one barrier: every warp reads all the warp totals from
-// `wsum` (kScanThreads / 32 ints in shared memory).  The caller must not write
+// `wsum` (kThreads / 32 ints in shared memory).  The caller must not write
 // `wsum` again before its next __syncthreads().
+template <int kThreads = kScanThreads>
 __device__ __forceinline__ int block_excl_scan_1bar(int v, int *total, int *wsum)
 {
-    constexpr int kWarps = kScanThreads / 32;
+    constexpr int kWarps = kThreads / 32;
     const int incl = warp_incl_scan(v);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (lane == 31) wsum[wid] = incl;

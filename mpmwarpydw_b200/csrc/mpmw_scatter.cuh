@@ -41,6 +41,7 @@
 namespace mpmw {
 
 constexpr int kScatterChunk = 256;   // particles (and threads) per CTA
+constexpr int kScatterCtasPerSm = 768 / kScatterChunk;  // resident CTAs the launch bounds aim at (80 registers)
 constexpr int kScatterBins = 1024;   // base cells of a CTA's box that the counting sort handles
 
 struct ScatterShared {
@@ -275,7 +276,7 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
             }
             // one scan of (nonempty bins << 16 | particles): both prefix sums at once
             int tot;
-            const int ex0 = block_excl_scan_1bar((ne << 16) | pc, &tot, S.wsum);
+            const int ex0 = block_excl_scan_1bar<kScatterChunk>((ne << 16) | pc, &tot, S.wsum);
             nact = tot & 0xFFFF;
             nseg = tot >> 16;
             int po = ex0 & 0xFFFF, so = ex0 >> 16;
@@ -295,12 +296,12 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
         } else {
             // a CTA spread over too many cells: compact, and let runs of equal
             // base in memory order form the segments
-            const int k = block_excl_scan(act ? 1 : 0, &nact);
+            const int k = block_excl_scan<kScatterChunk>(act ? 1 : 0, &nact);
             if (act) { S.base[0][k] = b0; S.base[1][k] = b1; S.base[2][k] = b2; }
             __syncthreads();
             const bool head = t < nact && (t == 0 || S.base[0][t] != S.base[0][t - 1] ||
                                            S.base[1][t] != S.base[1][t - 1] || S.base[2][t] != S.base[2][t - 1]);
-            const int sidx = block_excl_scan(head ? 1 : 0, &nseg);
+            const int sidx = block_excl_scan<kScatterChunk>(head ? 1 : 0, &nseg);
             if (head) S.seg_start[sidx] = t;
             if (t == 0) S.seg_start[nseg] = nact;
             __syncthreads();
