@@ -199,16 +199,24 @@ int hash_build(const float *x, int64_t n, const mpmw_hash_t &h, void *ws, size_t
 // copies (x, v) into the integrated buffers and integrates XPBD particles
 // (simulationRoutines.py:314-331 + xpbdRoutines.py:23-48)
 // flag bit0: read from the particle x/v (else from x_int/v_int);
-// flag bit1: write every particle (the wp.copy), else only integrated ones
-__global__ void k_xpbd_integrate(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int flag)
+// flag bit1: write every particle (the wp.copy), else only integrated ones.
+// xpbd_count (optional, zeroed by the caller): receives the number of
+// particles labelled XPBD, active or not.
+__global__ void k_xpbd_integrate(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int flag,
+                                 int *xpbd_count = nullptr)
 {
     const int64_t n = P.n;
     int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int mat = p < n ? P.material[p] : 0;
+    const bool integ = p < n && P.active[p] == 1 && mat == 2;
+    if (xpbd_count) {
+        const unsigned m = __ballot_sync(0xffffffffu, mat == 2);
+        if ((threadIdx.x & 31) == 0 && m) atomicAdd(xpbd_count, __popc(m));
+    }
     if (p >= n) return;
     float x0[3], v0[3];
     load3((flag & 1) ? P.x : X.x_int, n, p, x0);
     load3((flag & 1) ? P.v : X.v_int, n, p, v0);
-    bool integ = P.active[p] == 1 && P.material[p] == 2;
     if (integ) {
         float v1[3] = {v0[0] + q.gravity[0] * q.dt, v0[1] + q.gravity[1] * q.dt, v0[2] + q.gravity[2] * q.dt};
         float m = len3(v1);
@@ -277,11 +285,18 @@ __global__ void k_bound_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_pa
 // Each deltas[i] is owned by exactly one thread, so it is read-modify-written
 // without atomics; the contact-lock label writes only ever store 0 over a
 // label <= 1, which no test in this kernel distinguishes from 1.
-__global__ void k_particle_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash_t H, mpmw_xpbd_params_t q)
+// xpbd_count (optional): the step's number of particles labelled XPBD.  Every
+// pair this kernel acts on has an XPBD-labelled particle in it (the working
+// particle i may be an inactive one: the activity test is on tid), so with
+// none there is nothing to do: each particle's loop would add +0 to a delta
+// that k_bound_contacts left at +0, and set no label.
+__global__ void k_particle_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash_t H, mpmw_xpbd_params_t q,
+                                    const int *xpbd_count = nullptr)
 {
     const int64_t n = P.n;
     int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= n) return;
+    if (xpbd_count && __ldg(xpbd_count) == 0) return;
     if (P.active[tid] != 1) return;
     if (!(P.material[tid] >= 0)) return;
     int i = H.point_ids[tid];
@@ -558,14 +573,21 @@ int mpmw_xpbd_step(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_h
     if (p->n == 0) return MPMW_OK;
     cudaStream_t s = as_stream(stream);
     TRY(mpmw_hash_build(p->x, p->n, h, workspace, ws_bytes, stream));
+    // The hash build's scratch is free again: its first int counts the
+    // particles labelled XPBD, which lets the contact passes skip a step
+    // without any.
+    int *xpbd_count = static_cast<int *>(workspace);
+    if (cudaMemsetAsync(xpbd_count, 0, sizeof(int), s) != cudaSuccess) { set_error("xpbd_step: memset failed"); return MPMW_E_DEVICE; }
     // x_int <- x, v_int <- v for every particle (simulationRoutines.py:314-315), then integrate
-    TRY(mpmw_xpbd_kernel(MPMW_XK_INTEGRATE, p, x, h, q, 3, stream));
+    k_xpbd_integrate<<<grid_for(p->n), kBlock, 0, s>>>(*p, *x, *q, 3, xpbd_count);
+    TRY(check_launch("k_xpbd_integrate"));
     if (q->lock && !q->xpbd_only) TRY(mpmw_xpbd_kernel(MPMW_XK_RESET_LABELS, p, x, h, q, 0, stream));
     mpmw_xpbd_params_t qi = *q;
     if (q->xpbd_only) qi.lock = 0;
     for (int it = 0; it < q->iterations; ++it) {
         TRY(mpmw_xpbd_kernel(MPMW_XK_BOUND, p, x, h, &qi, 0, stream));
-        TRY(mpmw_xpbd_kernel(MPMW_XK_PARTICLE, p, x, h, &qi, 0, stream));
+        k_particle_contacts<<<grid_for(p->n), kBlock, 0, s>>>(*p, *x, *h, qi, xpbd_count);
+        TRY(check_launch("k_particle_contacts"));
         TRY(mpmw_xpbd_kernel(MPMW_XK_APPLY, p, x, h, &qi, it == q->iterations - 1, stream));
     }
     TRY(mpmw_xpbd_kernel(MPMW_XK_SLEEP, p, x, h, q, 1, stream));

@@ -52,6 +52,43 @@ def test_xpbd_step_matches_oracle(lock, xpbd_only):
         assert np.array_equal(a, b), (k, rel_err(a, b))
 
 
+@pytest.mark.parametrize("case", ["no_xpbd_labels", "xpbd_labels_inactive"])
+def test_xpbd_step_without_active_xpbd_particles(case):
+    """A step with no particle labelled XPBD (the contact passes then return at
+    once) is bit-exact with the oracle's full step: contact-locked labels are
+    reset, x/v pass through the integrate and impulse copies, deltas stay 0.
+    With XPBD labels on inactive particles only, the contact passes run in
+    full: the reference's kernel tests activity on the sorted slot, not on the
+    particle it works on, so inactive XPBD particles still lock MPM neighbours."""
+    import torch
+    from mpmwarpydw_b200.utils import simulationRoutines as S
+    if case == "no_xpbd_labels":
+        sim, mpm, xpbd = xpbd_scene(seed=6, frac_xpbd=0.0, lock=1)
+    else:
+        sim, mpm, xpbd = xpbd_scene(seed=7, lock=1)
+        ml = sim.materialLabel.clone()
+        al = sim.activeLabel.clone()
+        al[ml == 2] = 0
+        sim.activeLabel = al
+        assert int((ml == 2).sum().item()) > 0
+    s = to_oracle(sim, mpm, xpbd)
+    locked = (s.activeLabel == 1) & (s.materialLabel == 0)
+    assert int(locked.sum()) > 0  # contact-locked MPM particles, which the step resets
+    S.xpbdSimulationStep(sim, mpm, xpbd, "cuda:0")
+    torch.cuda.synchronize()
+    orc.xpbd_step(oracle("f32"), s)
+    g = gpu_fields(sim, mpm, xpbd)
+    assert s.numTotalXPBD == 0 and int(sim.numTotalXPBD.item()) == 0
+    if case == "no_xpbd_labels":
+        assert np.all(g["materialLabel"][locked] == 1)
+    assert np.array_equal(g["materialLabel"], s.materialLabel)
+    for k in ("particle_x", "particle_v", "particle_x_integrated", "particle_v_integrated", "particle_delta",
+              "particle_x_deltaInt", "particle_v_deltaInt", "particle_v_before_contact", "particle_cumDist_xpbd",
+              "particle_radius"):
+        a, b = g[k], getattr(s, k)
+        assert np.array_equal(a, b), (k, rel_err(a, b))
+
+
 def test_xpbd_kernels_one_by_one():
     """The reference-named per-kernel callables, in the reference's launch order."""
     import torch
