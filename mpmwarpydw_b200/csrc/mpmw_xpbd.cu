@@ -48,6 +48,18 @@ __global__ void k_hash_cells(const float *__restrict__ x, int64_t n, float inv, 
     if (point_cells) point_cells[p] = h;
 }
 
+// one bit per hash cell: set where a particle labelled XPBD lies (its cell
+// from the same positions and formula as k_hash_cells)
+__global__ void k_mark_xpbd_cells(mpmw_particles_t P, float inv, HashDims hd, unsigned *__restrict__ bits)
+{
+    const int64_t n = P.n;
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n || P.material[p] != 2) return;
+    int cx = (int)(P.x[p] * inv), cy = (int)(P.x[n + p] * inv), cz = (int)(P.x[2 * n + p] * inv);
+    int h = hash_index(hd.d, cx, cy, cz);
+    atomicOr(&bits[h >> 5], 1u << (h & 31));
+}
+
 // ---------------------------------------------------------------------------
 // stable LSD radix sort of (key, id) pairs, 7-bit digits
 // ---------------------------------------------------------------------------
@@ -290,8 +302,11 @@ __global__ void k_bound_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_pa
 // particle i may be an inactive one: the activity test is on tid), so with
 // none there is nothing to do: each particle's loop would add +0 to a delta
 // that k_bound_contacts left at +0, and set no label.
+// xpbd_cells (optional): one bit per hash cell holding an XPBD-labelled
+// particle.  A non-XPBD particle whose query box has no such cell has no pair
+// to act on and returns before walking its neighbours (same argument).
 __global__ void k_particle_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash_t H, mpmw_xpbd_params_t q,
-                                    const int *xpbd_count = nullptr)
+                                    const int *xpbd_count = nullptr, const unsigned *xpbd_cells = nullptr)
 {
     const int64_t n = P.n;
     int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -319,6 +334,16 @@ __global__ void k_particle_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash
     const float alpha = 0.f;
     float k_mu = q.dyn_friction;
     int mat_i = P.material[i];
+    if (xpbd_cells && mat_i <= 1) {
+        bool any = false;
+        for (int cz = zs; cz <= ze && !any; ++cz)
+            for (int cy = ys; cy <= ye && !any; ++cy)
+                for (int cx = xs; cx <= xe && !any; ++cx) {
+                    const int c = hash_index(hd, cx, cy, cz);
+                    any = (__ldg(&xpbd_cells[c >> 5]) >> (c & 31)) & 1u;
+                }
+        if (!any) return;
+    }
     for (int cz = zs; cz <= ze; ++cz)
         for (int cy = ys; cy <= ye; ++cy)
             for (int cx = xs; cx <= xe; ++cx) {
@@ -578,6 +603,20 @@ int mpmw_xpbd_step(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_h
     // without any.
     int *xpbd_count = static_cast<int *>(workspace);
     if (cudaMemsetAsync(xpbd_count, 0, sizeof(int), s) != cudaSuccess) { set_error("xpbd_step: memset failed"); return MPMW_E_DEVICE; }
+    // and, when it has room, one bit per hash cell holding an XPBD-labelled
+    // particle, so that particles with none near them skip the neighbour walk
+    unsigned *xpbd_cells = nullptr;
+    {
+        const int64_t ncell = (int64_t)h->dims[0] * h->dims[1] * h->dims[2];
+        const size_t bits_bytes = (size_t)((ncell + 31) / 32) * sizeof(unsigned);
+        if (ws_bytes >= 256 + bits_bytes) {
+            xpbd_cells = reinterpret_cast<unsigned *>(static_cast<char *>(workspace) + 256);
+            if (cudaMemsetAsync(xpbd_cells, 0, bits_bytes, s) != cudaSuccess) { set_error("xpbd_step: memset failed"); return MPMW_E_DEVICE; }
+            HashDims hd{{h->dims[0], h->dims[1], h->dims[2]}};
+            k_mark_xpbd_cells<<<grid_for(p->n), kBlock, 0, s>>>(*p, 1.0f / h->cell_width, hd, xpbd_cells);
+            TRY(check_launch("k_mark_xpbd_cells"));
+        }
+    }
     // x_int <- x, v_int <- v for every particle (simulationRoutines.py:314-315), then integrate
     k_xpbd_integrate<<<grid_for(p->n), kBlock, 0, s>>>(*p, *x, *q, 3, xpbd_count);
     TRY(check_launch("k_xpbd_integrate"));
@@ -586,7 +625,7 @@ int mpmw_xpbd_step(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_h
     if (q->xpbd_only) qi.lock = 0;
     for (int it = 0; it < q->iterations; ++it) {
         TRY(mpmw_xpbd_kernel(MPMW_XK_BOUND, p, x, h, &qi, 0, stream));
-        k_particle_contacts<<<grid_for(p->n), kBlock, 0, s>>>(*p, *x, *h, qi, xpbd_count);
+        k_particle_contacts<<<grid_for(p->n), kBlock, 0, s>>>(*p, *x, *h, qi, xpbd_count, xpbd_cells);
         TRY(check_launch("k_particle_contacts"));
         TRY(mpmw_xpbd_kernel(MPMW_XK_APPLY, p, x, h, &qi, it == q->iterations - 1, stream));
     }

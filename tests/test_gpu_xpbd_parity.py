@@ -89,6 +89,35 @@ def test_xpbd_step_without_active_xpbd_particles(case):
         assert np.array_equal(a, b), (k, rel_err(a, b))
 
 
+def test_xpbd_step_with_xpbd_particles_in_one_slab():
+    """XPBD particles only in a slab at one side of the block: most MPM
+    particles have no XPBD-labelled particle in their query box and skip their
+    neighbour walk (per-hash-cell presence bits).  Bit-exact with the oracle's
+    full step, contact-lock labels included."""
+    import torch
+    from mpmwarpydw_b200.utils import simulationRoutines as S
+    sim, mpm, xpbd = xpbd_scene(seed=9, frac_xpbd=0.0, lock=1)
+    x = sim.particle_x
+    ml = sim.materialLabel.clone()
+    slab = x[:, 0] < float(x[:, 0].min().item()) + 0.6
+    ml[slab] = 2
+    sim.materialLabel = ml
+    s = to_oracle(sim, mpm, xpbd)
+    S.xpbdSimulationStep(sim, mpm, xpbd, "cuda:0")
+    torch.cuda.synchronize()
+    orc.xpbd_step(oracle("f32"), s)
+    g = gpu_fields(sim, mpm, xpbd)
+    assert 0 < s.numTotalXPBD < sim.nPoints // 3
+    assert int(((s.materialLabel == 0) & ~slab.cpu().numpy()).sum()) > 0  # locks next to the slab
+    assert np.array_equal(g["materialLabel"], s.materialLabel)
+    assert int(sim.numTotalXPBD.item()) == s.numTotalXPBD and int(sim.numSleepingXPBD.item()) == s.numSleepingXPBD
+    for k in ("particle_x", "particle_v", "particle_x_integrated", "particle_v_integrated", "particle_delta",
+              "particle_x_deltaInt", "particle_v_deltaInt", "particle_v_before_contact", "particle_cumDist_xpbd",
+              "particle_radius"):
+        a, b = g[k], getattr(s, k)
+        assert np.array_equal(a, b), (k, rel_err(a, b))
+
+
 def test_xpbd_kernels_one_by_one():
     """The reference-named per-kernel callables, in the reference's launch order."""
     import torch
