@@ -316,8 +316,8 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g(mpmw
 __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_stress_p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
                                                              uint32_t *status, int *svd_list, int *svd_count)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    ScatterShared &S = *reinterpret_cast<ScatterShared *>(smem_raw);
+    extern __shared__ __align__(16) unsigned char smem_sp[];
+    ScatterShared &S = *reinterpret_cast<ScatterShared *>(smem_sp);
     const int64_t n = P.n;
     const int64_t p = (int64_t)blockIdx.x * kScatterChunk + threadIdx.x;
     bool scat = false;

@@ -441,8 +441,8 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const unsigned char *_
 {
     if (n_dev) n = min(n, (int64_t)*n_dev);
     if ((int64_t)blockIdx.x * kTcRows >= n) return;  // uniform
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    TcShared &S = *reinterpret_cast<TcShared *>(smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u));
+    extern __shared__ __align__(1024) unsigned char smem_tc[];
+    TcShared &S = *reinterpret_cast<TcShared *>(smem_tc + ((1024u - (smem_addr(smem_tc) & 1023u)) & 1023u));
     const int t = threadIdx.x, warp = t >> 5;
     const int64_t row = (int64_t)blockIdx.x * kTcRows + t;
     // weights and biases
