@@ -88,6 +88,11 @@ int mpmw_hash_build_noalloc(const float *x, int64_t n, const mpmw_hash_t *h, mpm
 /* One XPBD kernel (MPMW_XK_*). */
 int mpmw_xpbd_kernel(int which, const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_hash_t *h,
                      const mpmw_xpbd_params_t *q, int flag, mpmw_stream_t stream);
+/* Bytes of workspace mpmw_xpbd_step uses best for n points on a hash of the
+ * given dims: the hash build's scratch, and after the build a count, one bit
+ * per hash cell and per-point contact records (mpmw_hash_workspace_bytes(n)
+ * is enough; the step then skips the records). */
+size_t mpmw_xpbd_step_workspace_bytes(int64_t n, const int32_t *dims);
 /* utils/simulationRoutines.py:295-526 xpbdSimulationStep (hash build, integrate,
  * label reset, iterations x (bound, particle contacts, apply), sleep,
  * impulses + commit, swelling). */

@@ -115,6 +115,7 @@ _SIGS = {
     "mpmw_stress_surrogate": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Params), _P, _P, _F, _I,
                                    ctypes.c_uint64, _P, _P, _P, ctypes.c_size_t, _P]),
     "mpmw_hash_workspace_bytes": (ctypes.c_size_t, [_I64]),
+    "mpmw_xpbd_step_workspace_bytes": (ctypes.c_size_t, [_I64, ctypes.POINTER(ctypes.c_int32)]),
     "mpmw_hash_build": (_I, [_P, _I64, ctypes.POINTER(Hash), _P, ctypes.c_size_t, _P]),
     "mpmw_hash_build_noalloc": (_I, [_P, _I64, ctypes.POINTER(Hash), _P]),
     "mpmw_xpbd_kernel": (_I, [_I, ctypes.POINTER(Particles), ctypes.POINTER(XPBD), ctypes.POINTER(Hash),

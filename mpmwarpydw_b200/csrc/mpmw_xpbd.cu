@@ -305,8 +305,15 @@ __global__ void k_bound_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_pa
 // xpbd_cells (optional): one bit per hash cell holding an XPBD-labelled
 // particle.  A non-XPBD particle whose query box has no such cell has no pair
 // to act on and returns before walking its neighbours (same argument).
+// Rec: the neighbours' fields come from per-sorted-slot records
+// (k_contact_records) instead of by point index from the particle arrays.
+// The records hold the same values (labels as of the kernel's start, which the
+// tests here cannot tell from the live ones: the lock only writes 0 over <= 1).
+template <bool Rec>
 __global__ void k_particle_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash_t H, mpmw_xpbd_params_t q,
-                                    const int *xpbd_count = nullptr, const unsigned *xpbd_cells = nullptr)
+                                    const int *xpbd_count = nullptr, const unsigned *xpbd_cells = nullptr,
+                                    const float4 *__restrict__ recA = nullptr,
+                                    const float4 *__restrict__ recB = nullptr)
 {
     const int64_t n = P.n;
     int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -350,16 +357,30 @@ __global__ void k_particle_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash
                 int c = hash_index(hd, cx, cy, cz);
                 int b = H.cell_starts[c], e = H.cell_ends[c];
                 for (int s = b; s < e; ++s) {
-                    int index = H.point_ids[s];
-                    if (!(P.active[index] == 1 && index != i && P.mass[index] > 0.f)) continue;
-                    int mat_j = P.material[index];
-                    if (mat_i <= 1 && mat_j <= 1) continue;
-                    float xj[3];
-                    load3(X.x_int, n, index, xj);
+                    int index, mat_j;
+                    float xj[3], rad_j, mass_j;
+                    if constexpr (Rec) {
+                        const float4 ra = recA[s], rb = recB[s];
+                        index = __float_as_int(rb.w);
+                        mass_j = rb.x;
+                        if (!(__float_as_int(rb.y) == 1 && index != i && mass_j > 0.f)) continue;
+                        mat_j = __float_as_int(rb.z);
+                        if (mat_i <= 1 && mat_j <= 1) continue;
+                        xj[0] = ra.x; xj[1] = ra.y; xj[2] = ra.z;
+                        rad_j = ra.w;
+                    } else {
+                        index = H.point_ids[s];
+                        if (!(P.active[index] == 1 && index != i && P.mass[index] > 0.f)) continue;
+                        mat_j = P.material[index];
+                        if (mat_i <= 1 && mat_j <= 1) continue;
+                        load3(X.x_int, n, index, xj);
+                        rad_j = P.radius[index];
+                        mass_j = P.mass[index];
+                    }
                     float nn[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
                     float d = len3(nn);
-                    float err = (d - rad) - P.radius[index];
-                    float w2 = 1.f / P.mass[index];
+                    float err = (d - rad) - rad_j;
+                    float w2 = 1.f / mass_j;
                     float denom = w1 + w2;
                     if (err <= q.cohesion && denom > 0.f) {
                         if (q.lock == 1) {
@@ -389,6 +410,27 @@ __global__ void k_particle_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash
 #pragma unroll
     for (int a = 0; a < 3; ++a) cur[a] = cur[a] + dl[a] * q.relaxation;
     store3(X.delta, n, i, cur);
+}
+
+// The fields the contact pass reads of its neighbours, one record per sorted
+// hash slot s (point i = point_ids[s]): (x_int, radius) and (mass, active,
+// material, i), so a neighbour walk reads contiguous memory in hash order.
+__global__ void k_contact_records(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash_t H, float4 *__restrict__ recA,
+                                  float4 *__restrict__ recB)
+{
+    const int64_t n = P.n;
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int i = H.point_ids[s];
+    if (i < 0 || i >= n) {
+        recA[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+        recB[s] = make_float4(0.f, __int_as_float(0), __int_as_float(0), __int_as_float(-1));
+        return;
+    }
+    float x[3];
+    load3(X.x_int, n, i, x);
+    recA[s] = make_float4(x[0], x[1], x[2], P.radius[i]);
+    recB[s] = make_float4(P.mass[i], __int_as_float(P.active[i]), __int_as_float(P.material[i]), __int_as_float(i));
 }
 
 // xpbdRoutines.py:221-257 my_apply_particle_deltas.  x_orig = particle x,
@@ -549,6 +591,25 @@ extern "C" {
 
 size_t mpmw_hash_workspace_bytes(int64_t n) { return mpmw::hash_workspace_bytes(n < 0 ? 0 : n); }
 
+// After the hash build the step reuses its scratch: [0, 256) the count of
+// XPBD-labelled particles, then one bit per hash cell, then two float4 contact
+// records per point.  A smaller workspace drops the records (and then the bits).
+static size_t xpbd_bits_bytes(const int32_t *dims)
+{
+    const int64_t ncell = (int64_t)dims[0] * dims[1] * dims[2];
+    return (size_t)((ncell + 31) / 32) * sizeof(unsigned);
+}
+static size_t xpbd_records_offset(const int32_t *dims) { return (256 + xpbd_bits_bytes(dims) + 255) / 256 * 256; }
+
+size_t mpmw_xpbd_step_workspace_bytes(int64_t n, const int32_t *dims)
+{
+    if (n < 0) n = 0;
+    const size_t hash = mpmw::hash_workspace_bytes(n);
+    if (!dims) return hash;
+    const size_t step = xpbd_records_offset(dims) + 2 * (size_t)n * sizeof(float4);
+    return hash > step ? hash : step;
+}
+
 int mpmw_hash_build(const float *x, int64_t n, const mpmw_hash_t *h, void *workspace, size_t ws_bytes,
                     mpmw_stream_t stream)
 {
@@ -570,7 +631,7 @@ int mpmw_xpbd_kernel(int which, const mpmw_particles_t *p, const mpmw_xpbd_t *x,
     case MPMW_XK_BOUND: k_bound_contacts<<<g, kBlock, 0, s>>>(*p, *x, *q, flag); break;
     case MPMW_XK_PARTICLE:
         TRY(check_hash(h, p->n));
-        k_particle_contacts<<<g, kBlock, 0, s>>>(*p, *x, *h, *q);
+        k_particle_contacts<false><<<g, kBlock, 0, s>>>(*p, *x, *h, *q);
         break;
     case MPMW_XK_APPLY: k_apply_deltas<<<g, kBlock, 0, s>>>(*p, *x, *q, flag); break;
     case MPMW_XK_SLEEP:
@@ -617,6 +678,11 @@ int mpmw_xpbd_step(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_h
             TRY(check_launch("k_mark_xpbd_cells"));
         }
     }
+    float4 *recA = nullptr, *recB = nullptr;
+    if (xpbd_cells && ws_bytes >= xpbd_records_offset(h->dims) + 2 * (size_t)p->n * sizeof(float4)) {
+        recA = reinterpret_cast<float4 *>(static_cast<char *>(workspace) + xpbd_records_offset(h->dims));
+        recB = recA + p->n;
+    }
     // x_int <- x, v_int <- v for every particle (simulationRoutines.py:314-315), then integrate
     k_xpbd_integrate<<<grid_for(p->n), kBlock, 0, s>>>(*p, *x, *q, 3, xpbd_count);
     TRY(check_launch("k_xpbd_integrate"));
@@ -625,7 +691,14 @@ int mpmw_xpbd_step(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_h
     if (q->xpbd_only) qi.lock = 0;
     for (int it = 0; it < q->iterations; ++it) {
         TRY(mpmw_xpbd_kernel(MPMW_XK_BOUND, p, x, h, &qi, 0, stream));
-        k_particle_contacts<<<grid_for(p->n), kBlock, 0, s>>>(*p, *x, *h, qi, xpbd_count, xpbd_cells);
+        if (recA) {
+            k_contact_records<<<grid_for(p->n), kBlock, 0, s>>>(*p, *x, *h, recA, recB);
+            TRY(check_launch("k_contact_records"));
+            k_particle_contacts<true><<<grid_for(p->n), kBlock, 0, s>>>(*p, *x, *h, qi, xpbd_count, xpbd_cells,
+                                                                       recA, recB);
+        } else {
+            k_particle_contacts<false><<<grid_for(p->n), kBlock, 0, s>>>(*p, *x, *h, qi, xpbd_count, xpbd_cells);
+        }
         TRY(check_launch("k_particle_contacts"));
         TRY(mpmw_xpbd_kernel(MPMW_XK_APPLY, p, x, h, &qi, it == q->iterations - 1, stream));
     }

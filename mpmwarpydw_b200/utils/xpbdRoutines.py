@@ -9,6 +9,8 @@ arguments (CUDA tensors in the reference shapes, or state attributes).
 """
 from __future__ import annotations
 
+import ctypes
+
 import torch
 
 from .. import _lib
@@ -47,7 +49,10 @@ class HashGrid:
         if self.point_ids is None or self.point_ids.numel() < n:
             self.point_ids = torch.zeros(max(n, 1), dtype=I32, device=self.device)
             self.point_cells = torch.zeros(max(n, 1), dtype=I32, device=self.device)
-        need = int(_lib.lib().mpmw_hash_workspace_bytes(n))
+        # room for the XPBD step's contact records as well (the hash build alone
+        # needs less)
+        dims = (ctypes.c_int32 * 3)(*[int(d) for d in self.dims])
+        need = int(_lib.lib().mpmw_xpbd_step_workspace_bytes(n, dims))
         if self._ws is None or self._ws.numel() < need:
             self._ws = torch.empty(max(need, 256), dtype=torch.uint8, device=self.device)
 
