@@ -415,12 +415,15 @@ __global__ void k_particle_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash
 // The fields the contact pass reads of its neighbours, one record per sorted
 // hash slot s (point i = point_ids[s]): (x_int, radius) and (mass, active,
 // material, i), so a neighbour walk reads contiguous memory in hash order.
+// Nothing to write when the step has no XPBD-labelled particle (xpbd_count):
+// the contact pass then reads no record.
 __global__ void k_contact_records(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash_t H, float4 *__restrict__ recA,
-                                  float4 *__restrict__ recB)
+                                  float4 *__restrict__ recB, const int *xpbd_count)
 {
     const int64_t n = P.n;
     int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
+    if (xpbd_count && __ldg(xpbd_count) == 0) return;
     const int i = H.point_ids[s];
     if (i < 0 || i >= n) {
         recA[s] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -692,7 +695,7 @@ int mpmw_xpbd_step(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_h
     for (int it = 0; it < q->iterations; ++it) {
         TRY(mpmw_xpbd_kernel(MPMW_XK_BOUND, p, x, h, &qi, 0, stream));
         if (recA) {
-            k_contact_records<<<grid_for(p->n), kBlock, 0, s>>>(*p, *x, *h, recA, recB);
+            k_contact_records<<<grid_for(p->n), kBlock, 0, s>>>(*p, *x, *h, recA, recB, xpbd_count);
             TRY(check_launch("k_contact_records"));
             k_particle_contacts<true><<<grid_for(p->n), kBlock, 0, s>>>(*p, *x, *h, qi, xpbd_count, xpbd_cells,
                                                                        recA, recB);
