@@ -31,7 +31,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "MPM particle-updates/s at 4M, learned vs plain return map at <=1e-3 stress err"
+METRIC = "MPM particle-updates/s at 4M, learned vs plain return map at ≤1e-3 stress err"
 UNIT = "particle-updates/s"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
 
