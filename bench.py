@@ -146,11 +146,11 @@ def run_ours(a):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)  # before the process group, so NCCL binds this rank's GPU
+    dev = torch.device("cuda", local)
     if world > 1:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
     L = _lib.lib()
     d, sim, mpm, xpbd = setup(dev)
     N = sim.nPoints
