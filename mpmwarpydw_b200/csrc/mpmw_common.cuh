@@ -25,6 +25,15 @@ inline cudaStream_t as_stream(mpmw_stream_t s) { return reinterpret_cast<cudaStr
         if (_rc != MPMW_OK) return _rc;       \
     } while (0)
 
+// Particle indices, worklists and hash ids are 32-bit: an element count above
+// 2^31 - 1 is an argument error.  Records the message and returns true then.
+inline bool count_too_large(int64_t n, const char *what)
+{
+    if (n <= (int64_t)INT32_MAX) return false;
+    set_error("%s: count %lld exceeds the maximum of %d", what, (long long)n, (int)INT32_MAX);
+    return true;
+}
+
 inline unsigned grid_for(int64_t n, int block = kBlock)
 {
     int64_t b = (n + block - 1) / block;

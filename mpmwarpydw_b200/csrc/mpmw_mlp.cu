@@ -566,6 +566,7 @@ extern "C" {
 int mpmw_dp_samples(int64_t n, uint64_t seed, float *x, float *y, mpmw_stream_t stream)
 {
     if (n < 0 || (n > 0 && (!x || !y))) { set_error("dp_samples: bad arguments"); return MPMW_E_ARG; }
+    if (count_too_large(n, "dp_samples")) return MPMW_E_ARG;
     if (n == 0) return MPMW_OK;
     k_dp_samples<<<grid_for(n), kBlock, 0, as_stream(stream)>>>(n, seed, x, y);
     return check_launch("k_dp_samples");
@@ -574,6 +575,7 @@ int mpmw_dp_samples(int64_t n, uint64_t seed, float *x, float *y, mpmw_stream_t 
 int mpmw_mlp_forward(const float *params, const float *x, int64_t n, float *y, mpmw_stream_t stream)
 {
     if (!params || n < 0 || (n > 0 && (!x || !y))) { set_error("mlp_forward: bad arguments"); return MPMW_E_ARG; }
+    if (count_too_large(n, "mlp_forward")) return MPMW_E_ARG;
     if (n == 0) return MPMW_OK;
     { int rc_ = set_smem_attrs(); if (rc_ != MPMW_OK) return rc_; }
     const unsigned g = (unsigned)((n + kTile - 1) / kTile);
@@ -619,6 +621,7 @@ int mpmw_mlp_infer_tc(const void *packed, const float *params, const float *x, i
                       uint32_t *status, mpmw_stream_t stream)
 {
     if (!packed || !params || n < 0 || (n > 0 && (!x || !y))) { set_error("mlp_infer_tc: bad arguments"); return MPMW_E_ARG; }
+    if (count_too_large(n, "mlp_infer_tc")) return MPMW_E_ARG;
     if ((reinterpret_cast<uintptr_t>(packed) & 15u) != 0) { set_error("mlp_infer_tc: packed must be 16-byte aligned"); return MPMW_E_ARG; }
     if (n == 0) return MPMW_OK;
     { int rc_ = set_smem_attrs(); if (rc_ != MPMW_OK) return rc_; }

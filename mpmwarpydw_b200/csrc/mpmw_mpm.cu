@@ -354,6 +354,7 @@ static int check_particles(const mpmw_particles_t *p, unsigned need)
 {
     if (!p) { set_error("particles is NULL"); return MPMW_E_ARG; }
     if (p->n < 0) { set_error("negative particle count"); return MPMW_E_ARG; }
+    if (count_too_large(p->n, "particles")) return MPMW_E_ARG;
     if (p->n == 0) return MPMW_OK;
     if ((need & kNeedLabels) && (!p->active || !p->material)) {
         set_error("particles: active and material labels are required");
@@ -445,6 +446,7 @@ int mpmw_mu_lam_bulk(int64_t n, const float *E, const float *nu, float *mu, floa
                      mpmw_stream_t stream)
 {
     if (n < 0 || (n > 0 && (!E || !nu || !mu || !lam || !bulk))) { set_error("mu_lam_bulk: bad arguments"); return MPMW_E_ARG; }
+    if (count_too_large(n, "mu_lam_bulk")) return MPMW_E_ARG;
     if (n == 0) return MPMW_OK;
     k_mu_lam_bulk<<<grid_for(n), kBlock, 0, as_stream(stream)>>>(n, E, nu, mu, lam, bulk);
     return check_launch("k_mu_lam_bulk");
@@ -454,6 +456,7 @@ int mpmw_geostatic_F(int64_t n, const float *x, float *F, const float *mu, const
                      float gravity, float z_top, float K0, int planestrain, mpmw_stream_t stream)
 {
     if (n < 0 || (n > 0 && (!x || !F || !mu || !lam || !density))) { set_error("geostatic_F: bad arguments"); return MPMW_E_ARG; }
+    if (count_too_large(n, "geostatic_F")) return MPMW_E_ARG;
     if (n == 0) return MPMW_OK;
     k_geostatic_F<<<grid_for(n), kBlock, 0, as_stream(stream)>>>(n, x, F, mu, lam, density, gravity, z_top, K0, planestrain);
     return check_launch("k_geostatic_F");
@@ -629,6 +632,7 @@ int mpmw_creep(const mpmw_particles_t *p, const float *ys_base, float dt, float 
         set_error("creep: bad arguments");
         return MPMW_E_ARG;
     }
+    if (count_too_large(p->n, "creep")) return MPMW_E_ARG;
     if (p->n == 0) return MPMW_OK;
     k_creep<<<grid_for(p->n), kBlock, 0, as_stream(stream)>>>(*p, ys_base, dt, base_creep, damage_creep, damage_exponent);
     return check_launch("k_creep");
@@ -637,6 +641,7 @@ int mpmw_creep(const mpmw_particles_t *p, const float *ys_base, float dt, float 
 int mpmw_stats(const mpmw_particles_t *p, double *out, mpmw_stream_t stream)
 {
     if (!p || p->n < 0 || !out) { set_error("stats: bad arguments"); return MPMW_E_ARG; }
+    if (count_too_large(p->n, "stats")) return MPMW_E_ARG;
     if (p->n > 0 && (!p->active || !p->material || !p->v || !p->radius || !p->damage)) {
         set_error("stats: active, material, v, radius and damage are required");
         return MPMW_E_ARG;

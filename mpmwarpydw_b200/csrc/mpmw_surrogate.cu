@@ -311,6 +311,7 @@ int mpmw_stress_surrogate(const mpmw_particles_t *p, const mpmw_params_t *prm, c
 {
     if (!p || !prm || !packed || !mlp_params || !stats) { set_error("stress_surrogate: NULL argument"); return MPMW_E_ARG; }
     if (p->n < 0) { set_error("stress_surrogate: negative particle count"); return MPMW_E_ARG; }
+    if (count_too_large(p->n, "stress_surrogate")) return MPMW_E_ARG;
     if (p->n == 0) return MPMW_OK;
     if (!p->x || !p->v || !p->C || !p->F || !p->F_trial || !p->stress || !p->active || !p->material || !p->mu ||
         !p->lam || !p->ys || !p->alpha || !p->damage || !p->acc_strain || !p->strain_criteria || !p->hardening ||

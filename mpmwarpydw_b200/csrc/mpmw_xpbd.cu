@@ -565,6 +565,7 @@ static int check_xpbd_args(const mpmw_particles_t *p, const mpmw_xpbd_t *x, cons
 {
     if (!p || !x || !q) { set_error("xpbd: NULL argument"); return MPMW_E_ARG; }
     if (p->n < 0) { set_error("xpbd: negative particle count"); return MPMW_E_ARG; }
+    if (count_too_large(p->n, "xpbd")) return MPMW_E_ARG;
     if (p->n == 0) return MPMW_OK;
     if (!p->x || !p->v || !p->active || !p->material || !p->mass || !p->radius) {
         set_error("xpbd: x, v, active, material, mass and radius are required");
@@ -616,6 +617,7 @@ size_t mpmw_xpbd_step_workspace_bytes(int64_t n, const int32_t *dims)
 int mpmw_hash_build(const float *x, int64_t n, const mpmw_hash_t *h, void *workspace, size_t ws_bytes,
                     mpmw_stream_t stream)
 {
+    if (count_too_large(n, "hash_build")) return MPMW_E_ARG;
     TRY(check_hash(h, n));
     if (n < 0 || (n > 0 && (!x || !workspace))) { set_error("hash_build: bad arguments"); return MPMW_E_ARG; }
     return mpmw::hash_build(x, n, *h, workspace, ws_bytes, as_stream(stream));

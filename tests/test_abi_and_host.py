@@ -35,6 +35,33 @@ def test_argument_errors_are_reported_not_raised():
     assert rc == 1  # null grid buffers are rejected before the enum
 
 
+def test_particle_counts_beyond_32_bits_are_rejected():
+    """Particle indices, worklists and hash ids are 32-bit: a count above
+    2^31 - 1 is an argument error, reported before any device work."""
+    from mpmwarpydw_b200 import _lib
+    L = _lib.lib()
+    big = 2 ** 31
+    P = _lib.Particles(); P.n = big
+    G = _lib.Grid(); G.dims[0] = G.dims[1] = G.dims[2] = 4
+    prm = _lib.Params()
+    rc = L.mpmw_substep(ctypes.byref(P), ctypes.byref(G), ctypes.byref(prm), None, None)
+    assert rc == 1 and b"2147483647" in L.mpmw_last_error()
+    out = (ctypes.c_double * 7)()  # never written: the count is rejected first
+    rc = L.mpmw_stats(ctypes.byref(P), out, None)
+    assert rc == 1 and b"2147483647" in L.mpmw_last_error()
+    X, q, H = _lib.XPBD(), _lib.XPBDParams(), _lib.Hash()
+    for i in range(3):
+        H.dims[i] = 8
+    H.cell_width = 1.0
+    rc = L.mpmw_xpbd_step(ctypes.byref(P), ctypes.byref(X), ctypes.byref(H), ctypes.byref(q), None, 0, None)
+    assert rc == 1 and b"2147483647" in L.mpmw_last_error()
+    rc = L.mpmw_hash_build(None, big, ctypes.byref(H), None, 0, None)
+    assert rc == 1 and b"2147483647" in L.mpmw_last_error()
+    f = (ctypes.c_float * 1)()  # never read: the count is rejected first
+    rc = L.mpmw_mu_lam_bulk(big, f, f, f, f, f, None)
+    assert rc == 1 and b"2147483647" in L.mpmw_last_error()
+
+
 def test_getargs_merge_rules(tmp_path):
     from mpmwarpydw_b200.utils.getArgs import get_args
     cfg = tmp_path / "c.json"
