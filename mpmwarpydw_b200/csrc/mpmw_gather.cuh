@@ -85,9 +85,12 @@ __device__ __forceinline__ bool gather_prepare(GatherShared &S, bool act, const 
 // add +-0 and leave the sum unchanged.
 __device__ __forceinline__ float2 ffma2(float w, float2 g, float2 acc) { return __ffma2_rn(make_float2(w, w), g, acc); }
 
-__device__ __forceinline__ void gather_particle(const GatherShared &S, bool tile, int ox, int oy, int oz,
-                                                const Weights &W, const mpmw_grid_t &G, float inv_dx, float *nv,
-                                                float *nF, float *nC, uint32_t &bad)
+// Tile: the CTA's grid tile is in shared memory (a uniform choice, made once
+// per CTA, so the 27 node reads compile without a branch each).
+template <bool Tile>
+__device__ __forceinline__ void gather_particle_t(const GatherShared &S, int ox, int oy, int oz, const Weights &W,
+                                                  const mpmw_grid_t &G, float inv_dx, float *nv, float *nF, float *nC,
+                                                  uint32_t &bad)
 {
     const int nx = G.dims[0], ny = G.dims[1], nz = G.dims[2];
     const float4 *__restrict__ gv = reinterpret_cast<const float4 *>(G.v);
@@ -110,7 +113,7 @@ __device__ __forceinline__ void gather_particle(const GatherShared &S, bool tile
             for (int k = 0; k < 3; ++k) {
                 const int iz = W.base[2] + k;
                 float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (tile) g = S.tile[tb + (i * kTileEdge + j) * kTileEdge + k];
+                if (Tile) g = S.tile[tb + (i * kTileEdge + j) * kTileEdge + k];
                 else if (inside || (ix >= 0 && iy >= 0 && iz >= 0 && ix < nx && iy < ny && iz < nz))
                     g = __ldg(&gv[((int64_t)ix * ny + iy) * nz + iz]);
                 const float wz = W.w[2][k], dwz = W.dw[2][k], kwz = (float)k * wz;
@@ -148,6 +151,14 @@ __device__ __forceinline__ void gather_particle(const GatherShared &S, bool tile
         nC[3 * r + 1] = c4 * fma_(-W.fx[1], nv[r], Mj[r]);
         nC[3 * r + 2] = c4 * fma_(-W.fx[2], nv[r], Mk[r]);
     }
+}
+
+__device__ __forceinline__ void gather_particle(const GatherShared &S, bool tile, int ox, int oy, int oz,
+                                                const Weights &W, const mpmw_grid_t &G, float inv_dx, float *nv,
+                                                float *nF, float *nC, uint32_t &bad)
+{
+    if (tile) gather_particle_t<true>(S, ox, oy, oz, W, G, inv_dx, nv, nF, nC, bad);
+    else gather_particle_t<false>(S, ox, oy, oz, W, G, inv_dx, nv, nF, nC, bad);
 }
 
 // F_trial = (I + dt grad v) F = F + dt (grad v F); optional covariance update.

@@ -11,9 +11,12 @@
 //      particles that drift across cell boundaries between global sorts do not
 //      fragment the segments.  A CTA whose box has more than kScatterBins cells
 //      compacts instead, and runs of equal base in memory order form segments;
-//   2. each particle stores its B-spline weights and per-particle constants
-//      (10 float4) in shared memory at its sorted slot, swizzled so that
-//      particles about 8 apart fall in different banks;
+//   2. each particle stores its B-spline weights and per-particle constants in
+//      shared memory at its sorted slot: 8 float4 (swizzled so that particles
+//      about 8 apart fall in different banks) laid out as the packed FP32 FMA
+//      wants its operand pairs (z weights duplicated, stress and momentum
+//      components side by side), and its x and y weights as (w, dw) pairs that
+//      a column (i, j) indexes directly;
 //   3. one thread per (segment, i, j) stencil column sums its particles'
 //      contributions to the column's 3 nodes in registers, for as many complete
 //      passes over the threads as there are; each column left over is shared by
@@ -44,8 +47,14 @@ constexpr int kScatterChunk = 256;   // particles (and threads) per CTA
 constexpr int kScatterCtasPerSm = 768 / kScatterChunk;  // resident CTAs the launch bounds aim at (80 registers)
 constexpr int kScatterBins = 1024;   // base cells of a CTA's box that the counting sort handles
 
+constexpr int kScatterRec = 8;       // float4 records per particle
+
 struct ScatterShared {
-    float4 rec[10][kScatterChunk];   // per compacted particle (swizzled slot)
+    float4 rec[kScatterRec][kScatterChunk];  // per compacted particle (swizzled slot)
+    // x and y weights of slot q: (wx_i, dwx_i) at 7q + i, (wy_j, dwy_j) at
+    // 7q + 3 + j.  The odd stride puts the lanes that read one particle for
+    // different columns in different banks.
+    float2 wxy[kScatterChunk * 7];
     int base[3][kScatterChunk];
     int seg_start[kScatterChunk + 1];
     int wsum[kScatterChunk / 32];    // warp totals of the counting sort's scan
@@ -55,8 +64,6 @@ struct ScatterShared {
 };
 
 __device__ __forceinline__ int scatter_slot(int k) { return k ^ ((k >> 3) & 7); }
-
-__device__ __forceinline__ float sel3(const float4 &r, int i) { return i == 0 ? r.x : (i == 1 ? r.y : r.z); }
 
 // Register sums of one stencil column (i, j) of one segment: the 3 nodes
 // k = 0..2 of (m, m vx, m vy, m vz).  The x and y momentum components (and
@@ -77,40 +84,44 @@ struct ColumnSums {
         for (int k = 0; k < 3; ++k) { axy[k] = make_float2(0.f, 0.f); az[k] = 0.f; }
     }
 
-    // add the contribution of the particle in record slot q to column ij
+    // add the contribution of the particle in record slot q to column ij.
+    // Record (see put_record): rec[0] = (wz0 wz0 wz1 wz1), rec[1] = (wz2 wz2
+    // dwz0 dwz0), rec[2] = (dwz1 dwz1 dwz2 dwz2), rec[3] = (s00 s01 s01 s11),
+    // rec[4] = (s02 s12 s22 m), rec[5] = (a0 a1 Bx0 Bx1), rec[6] = (By0 By1
+    // Bz0 Bz1), rec[7] = (a2 Bx2 By2 Bz2).
     template <class Shared>
-    __device__ __forceinline__ void add(const Shared &S, int q, int ij)
+    __device__ __forceinline__ void add(const Shared &S, int q, int i, int j, float2 fi2, float2 fj2)
     {
-        const int i = ij / 3, j = ij - 3 * (ij / 3);
-        const float fi = (float)i, fj = (float)j;
-        const float4 r0 = S.rec[0][q], r1 = S.rec[1][q], r2 = S.rec[2][q], r3 = S.rec[3][q], r4 = S.rec[4][q],
-                     r5 = S.rec[5][q], r6 = S.rec[6][q], r7 = S.rec[7][q], r8 = S.rec[8][q], r9 = S.rec[9][q];
-        const float wxi = sel3(r0, i), dwxi = sel3(r1, i), wyj = sel3(r2, j), dwyj = sel3(r3, j);
-        const float mm = r0.w;
-        const float s00 = r1.w, s11 = r2.w, s22 = r3.w, s01 = r4.w, s02 = r5.w, s12 = r6.w;
-        const float wxy = wxi * wyj, g0 = dwxi * wyj, g1 = wxi * dwyj, wm = wxy * mm;
+        const float2 xw = S.wxy[7 * q + i], yw = S.wxy[7 * q + 3 + j];
+        const float wxi = xw.x, dwxi = xw.y, wyj = yw.x, dwyj = yw.y;
+        const float4 z0 = S.rec[0][q], z1 = S.rec[1][q], z2 = S.rec[2][q], sa = S.rec[3][q], sb = S.rec[4][q],
+                     u0 = S.rec[5][q], u1 = S.rec[6][q], u2 = S.rec[7][q];
+        const float wxy = wxi * wyj, g0 = dwxi * wyj, g1 = wxi * dwyj, wm = wxy * sb.w;
+        const float2 wxy2 = dup2(wxy);
         // A = a + i Bx + j By
-        const float2 A01 = __ffma2_rn(dup2(fj), make_float2(r8.x, r8.y),
-                                      __ffma2_rn(dup2(fi), make_float2(r7.x, r7.y), make_float2(r6.x, r6.y)));
-        const float A2 = fma_(fj, r8.z, fma_(fi, r7.z, r6.z));
+        const float2 A01 = __ffma2_rn(fj2, make_float2(u1.x, u1.y),
+                                      __ffma2_rn(fi2, make_float2(u0.z, u0.w), make_float2(u0.x, u0.y)));
+        const float A2 = fma_(fj2.x, u2.z, fma_(fi2.x, u2.y, u2.x));
         // Q = S (g0, g1, 0), R = wxy S[:,2]
-        const float2 Q01 = __ffma2_rn(make_float2(s00, s01), dup2(g0), __fmul2_rn(make_float2(s01, s11), dup2(g1)));
-        const float Q2 = fma_(s02, g0, s12 * g1);
-        const float2 R01 = __fmul2_rn(dup2(wxy), make_float2(s02, s12));
-        const float R2 = wxy * s22;
+        const float2 Q01 = __ffma2_rn(make_float2(sa.x, sa.y), dup2(g0), __fmul2_rn(make_float2(sa.z, sa.w), dup2(g1)));
+        const float Q2 = fma_(sb.x, g0, sb.y * g1);
+        const float2 R01 = __fmul2_rn(wxy2, make_float2(sb.x, sb.y));
+        const float R2 = wxy * sb.z;
         // P_k = wxy (A + k Bz) + Q
-        float2 P01 = __ffma2_rn(dup2(wxy), A01, Q01);
+        float2 P01 = __ffma2_rn(wxy2, A01, Q01);
         float P2 = fma_(wxy, A2, Q2);
-        const float2 dz01 = __fmul2_rn(dup2(wxy), make_float2(r9.x, r9.y));
-        const float dz2 = wxy * r9.z;
-        m01 = __ffma2_rn(make_float2(r4.x, r4.y), dup2(wm), m01);
-        m2 = fma_(r4.z, wm, m2);
-        const float wz[3] = {r4.x, r4.y, r4.z}, dwz[3] = {r5.x, r5.y, r5.z};
+        const float2 dz01 = __fmul2_rn(wxy2, make_float2(u1.z, u1.w));
+        const float dz2 = wxy * u2.w;
+        m01.x = fma_(z0.x, wm, m01.x);
+        m01.y = fma_(z0.z, wm, m01.y);
+        m2 = fma_(z1.x, wm, m2);
+        const float2 wz[3] = {make_float2(z0.x, z0.y), make_float2(z0.z, z0.w), make_float2(z1.x, z1.y)};
+        const float2 dwz[3] = {make_float2(z1.z, z1.w), make_float2(z2.x, z2.y), make_float2(z2.z, z2.w)};
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             if (k > 0) { P01 = __fadd2_rn(P01, dz01); P2 = P2 + dz2; }
-            axy[k] = __ffma2_rn(dup2(wz[k]), P01, __ffma2_rn(dup2(dwz[k]), R01, axy[k]));
-            az[k] = fma_(wz[k], P2, fma_(dwz[k], R2, az[k]));
+            axy[k] = __ffma2_rn(wz[k], P01, __ffma2_rn(dwz[k], R01, axy[k]));
+            az[k] = fma_(wz[k].x, P2, fma_(dwz[k].x, R2, az[k]));
         }
     }
 
@@ -249,16 +260,22 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
                 av[row] = fma_(-B[3 * row + 0], W.fx[0], fma_(-B[3 * row + 1], W.fx[1], fma_(-B[3 * row + 2], W.fx[2], m * v[row])));
             const float sc = -(prm.dt * vol) * prm.inv_dx;
             const int q = scatter_slot(slot);
-            S.rec[0][q] = make_float4(W.w[0][0], W.w[0][1], W.w[0][2], m);
-            S.rec[1][q] = make_float4(W.dw[0][0], W.dw[0][1], W.dw[0][2], sc * st6[0]);
-            S.rec[2][q] = make_float4(W.w[1][0], W.w[1][1], W.w[1][2], sc * st6[1]);
-            S.rec[3][q] = make_float4(W.dw[1][0], W.dw[1][1], W.dw[1][2], sc * st6[2]);
-            S.rec[4][q] = make_float4(W.w[2][0], W.w[2][1], W.w[2][2], sc * st6[3]);
-            S.rec[5][q] = make_float4(W.dw[2][0], W.dw[2][1], W.dw[2][2], sc * st6[4]);
-            S.rec[6][q] = make_float4(av[0], av[1], av[2], sc * st6[5]);
-            S.rec[7][q] = make_float4(B[0], B[3], B[6], 0.f);   // Bx = column 0
-            S.rec[8][q] = make_float4(B[1], B[4], B[7], 0.f);   // By
-            S.rec[9][q] = make_float4(B[2], B[5], B[8], 0.f);   // Bz
+            const float s00 = sc * st6[0], s11 = sc * st6[1], s22 = sc * st6[2], s01 = sc * st6[3],
+                        s02 = sc * st6[4], s12 = sc * st6[5];
+            // Bx = column 0 of B (B[0], B[3], B[6]), By = column 1, Bz = column 2
+            S.rec[0][q] = make_float4(W.w[2][0], W.w[2][0], W.w[2][1], W.w[2][1]);
+            S.rec[1][q] = make_float4(W.w[2][2], W.w[2][2], W.dw[2][0], W.dw[2][0]);
+            S.rec[2][q] = make_float4(W.dw[2][1], W.dw[2][1], W.dw[2][2], W.dw[2][2]);
+            S.rec[3][q] = make_float4(s00, s01, s01, s11);
+            S.rec[4][q] = make_float4(s02, s12, s22, m);
+            S.rec[5][q] = make_float4(av[0], av[1], B[0], B[3]);
+            S.rec[6][q] = make_float4(B[1], B[4], B[2], B[5]);
+            S.rec[7][q] = make_float4(av[2], B[6], B[7], B[8]);
+#pragma unroll
+            for (int e = 0; e < 3; ++e) {
+                S.wxy[7 * q + e] = make_float2(W.w[0][e], W.dw[0][e]);
+                S.wxy[7 * q + 3 + e] = make_float2(W.w[1][e], W.dw[1][e]);
+            }
             S.base[0][slot] = W.base[0]; S.base[1][slot] = W.base[1]; S.base[2][slot] = W.base[2];
         };
         if (use_bins) {
@@ -322,9 +339,11 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
     const int full_items = (items / kScatterChunk) * kScatterChunk;
     for (int q = t; q < full_items; q += kScatterChunk) {
         const int s = q / 9, ij = q - 9 * s;
+        const int i = ij / 3, j = ij - 3 * (ij / 3);
+        const float2 fi2 = dup2((float)i), fj2 = dup2((float)j);
         const int k0 = S.seg_start[s], k1 = S.seg_start[s + 1];
         acc.zero();
-        for (int kq = k0; kq < k1; ++kq) acc.add(S, scatter_slot(kq), ij);
+        for (int kq = k0; kq < k1; ++kq) acc.add(S, scatter_slot(kq), i, j, fi2, fj2);
         acc.emit(S, k0, ij, gmv, nx, ny, nz, bad);
     }
     const int left = items - full_items;  // uniform, < kScatterChunk
@@ -340,7 +359,9 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
             ij = q - 9 * s;
             k0 = S.seg_start[s];
             const int k1 = S.seg_start[s + 1];
-            for (int kq = k0 + sub; kq < k1; kq += 1 << lg) acc.add(S, scatter_slot(kq), ij);
+            const int i = ij / 3, j = ij - 3 * (ij / 3);
+            const float2 fi2 = dup2((float)i), fj2 = dup2((float)j);
+            for (int kq = k0 + sub; kq < k1; kq += 1 << lg) acc.add(S, scatter_slot(kq), i, j, fi2, fj2);
         }
         for (int o = (1 << lg) >> 1; o > 0; o >>= 1) acc.shfl_add(o);  // all lanes (full-warp shuffles)
         if (mine && sub == 0) acc.emit(S, k0, ij, gmv, nx, ny, nz, bad);
