@@ -241,11 +241,18 @@ __device__ __forceinline__ void p2g_scatter(ScatterShared &S, bool act, const fl
             weights(xp, prm.min_bounds, prm.inv_dx, W);
             const float r = prm.rpic_damping;
             float Cp[9];
+            if (r == 0.f) {
+                // (1 - 0) C + 0 (C - C^T) = C for finite C (up to the sign of an
+                // exact zero): a uniform shortcut for the undamped default
 #pragma unroll
-            for (int aa = 0; aa < 3; ++aa)
+                for (int q = 0; q < 9; ++q) Cp[q] = C0[q];
+            } else {
 #pragma unroll
-                for (int bb = 0; bb < 3; ++bb)
-                    Cp[3 * aa + bb] = (1.f - r) * C0[3 * aa + bb] + (r / 2.f) * (C0[3 * aa + bb] - C0[3 * bb + aa]);
+                for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+                    for (int bb = 0; bb < 3; ++bb)
+                        Cp[3 * aa + bb] = (1.f - r) * C0[3 * aa + bb] + (r / 2.f) * (C0[3 * aa + bb] - C0[3 * bb + aa]);
+            }
             if (r < -0.001f) {
 #pragma unroll
                 for (int q = 0; q < 9; ++q) Cp[q] = 0.f;
