@@ -88,37 +88,78 @@ __global__ void __launch_bounds__(kBlock) k_stress_p2g_list(mpmw_particles_t P, 
     if (bad) raise_status(status, bad);
 }
 
+// Shared memory of k_g2p: the grid tile, F of the CTA's particles (read ahead
+// by bulk copies) and the positions, parked while the gather runs so that fewer
+// registers stay live across it.
+struct G2PShared {
+    GatherShared g;
+    float F[9][kBlock];
+    float xpark[3][kBlock];
+    uint64_t pbar;
+};
+
 template <bool Fused>
 __global__ void __launch_bounds__(kBlock, 3) k_g2p(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
                                                uint32_t *status, int *svd_list, int *svd_count,
-                                               const __grid_constant__ CUtensorMap tmap, int use_tma)
+                                               const __grid_constant__ CUtensorMap tmap, int use_tma, int use_ahead)
 {
-    __shared__ __align__(128) GatherShared S;
+    __shared__ __align__(128) G2PShared S;
     const int64_t n = P.n;
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    // labels, x and F are loaded together (not behind the label test)
+    const int t = threadIdx.x;
+    const int64_t p0 = (int64_t)blockIdx.x * blockDim.x;
+    const int64_t p = p0 + t;
+    // F read ahead into shared memory by bulk copies (full CTAs; the host checks
+    // the 16-byte alignment they need), in flight while the CTA waits for its tile
+    const bool ahead = use_ahead && p0 + kBlock <= n;
+    if (ahead && t == 0) {
+        mbar_init(&S.pbar, 1);
+        mbar_arrive_expect_tx(&S.pbar, 9u * kBlock * 4u);
+#pragma unroll 1
+        for (int f = 0; f < 9; ++f) bulk_load(&S.F[f][0], P.F + (int64_t)f * n + p0, kBlock * 4u, &S.pbar);
+    }
+    // labels and x are loaded together (not behind the label test)
     int lab_a = 0, lab_m = 0;
-    float xp[3] = {0.f, 0.f, 0.f}, Fpre[9];
+    float xp[3] = {0.f, 0.f, 0.f};
     if (p < n) {
         lab_a = P.active[p];
         lab_m = P.material[p];
         load3(P.x, n, p, xp);
-        load9(P.F, n, p, Fpre);  // in flight while the CTA waits for its grid tile
     }
     const bool act = lab_a == 1 && lab_m <= 1;
     Weights W;
     if (act) weights(xp, prm.min_bounds, prm.inv_dx, W);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) S.xpark[a][t] = xp[a];
     bool tile = false;
     int ox = 0, oy = 0, oz = 0;
-    if (!gather_prepare(S, act, W, &tmap, use_tma, status, tile, ox, oy, oz)) return;
+    if (!gather_prepare(S.g, act, W, &tmap, use_tma, status, tile, ox, oy, oz)) {
+        // no active particle: the read-ahead must still land before the CTA exits
+        if (ahead && !mbar_wait_bounded(&S.pbar, 0)) raise_status(status, MPMW_ST_TIMEOUT);
+        return;  // uniform
+    }
+    // every active thread waits for the read-ahead, so the CTA outlives the copies
     if (!act) return;
     uint32_t bad = 0;
     float nv[3], nF[9], nC[9];
-    gather_particle(S, tile, ox, oy, oz, W, G, prm.inv_dx, nv, nF, nC, bad);
+    gather_particle(S.g, tile, ox, oy, oz, W, G, prm.inv_dx, nv, nF, nC, bad);
     float xn[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) xn[a] = fma_(prm.dt, nv[a], xp[a]);
+    for (int a = 0; a < 3; ++a) xn[a] = fma_(prm.dt, nv[a], S.xpark[a][t]);
     if (!(isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]))) bad |= MPMW_ST_NAN;
+    float Fpre[9];
+    bool ahead_ok = ahead;
+    if (ahead && !mbar_wait_bounded(&S.pbar, 0)) {
+        // report, wait once more for the copies in flight, and read global memory
+        bad |= MPMW_ST_TIMEOUT;
+        mbar_wait_bounded(&S.pbar, 0);
+        ahead_ok = false;
+    }
+    if (ahead_ok) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Fpre[k] = S.F[k][t];
+    } else {
+        load9(P.F, n, p, Fpre);
+    }
     float Ft[9];
     g2p_deformation(P, prm, p, nF, Ft, Fpre);
     store3(P.x, n, p, xn);
@@ -155,6 +196,10 @@ struct AheadFields {
     float f[kAheadFields][kScatterChunk];
 };
 static_assert(sizeof(AheadFields) <= sizeof(ScatterShared::rec), "read-ahead fits the record area");
+// the particle positions are parked in the record area behind the read-ahead
+// fields while the gather runs (fewer registers live across it)
+static_assert((kAheadFields + 3) * kScatterChunk * sizeof(float) <= sizeof(ScatterShared::rec),
+              "parked positions fit the record area");
 
 __device__ __forceinline__ const float *ahead_src(const mpmw_particles_t &P, int field)
 {
@@ -216,6 +261,9 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g(mpmw
     const bool act = lab_a == 1 && lab_m <= 1;
     Weights W;
     if (act) weights(xp, prm.min_bounds, prm.inv_dx, W);
+    float(*xpark)[kScatterChunk] = &AF.f[0] + kAheadFields;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) xpark[a][t] = xp[a];
     bool tile = false;
     int ox = 0, oy = 0, oz = 0;
     if (!gather_prepare(S.g, act, W, &tmap, use_tma, status, tile, ox, oy, oz)) {
@@ -239,7 +287,7 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g(mpmw
         float nF[9];
         gather_particle(S.g, tile, ox, oy, oz, W, G, prm.inv_dx, nv, nF, nC, bad);
 #pragma unroll
-        for (int a = 0; a < 3; ++a) xn[a] = fma_(prm.dt, nv[a], xp[a]);
+        for (int a = 0; a < 3; ++a) xn[a] = fma_(prm.dt, nv[a], xpark[a][t]);
         if (!(isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]))) bad |= MPMW_ST_NAN;
         float Ft[9];
         {
@@ -454,8 +502,10 @@ int launch_g2p(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_param
     CUtensorMap map;
     int use_tma = cached_grid_map(g, &map) ? 1 : 0;
     if (!use_tma) memset(&map, 0, sizeof(map));
+    // the F read-ahead needs each row's chunk start 16-byte aligned
+    const int use_ahead = p.F && p.n % 4 == 0 && (reinterpret_cast<uintptr_t>(p.F) & 15u) == 0 ? 1 : 0;
     if (!fused) {
-        k_g2p<false><<<grid_for(p.n), kBlock, 0, s>>>(p, g, prm, st, nullptr, nullptr, map, use_tma);
+        k_g2p<false><<<grid_for(p.n), kBlock, 0, s>>>(p, g, prm, st, nullptr, nullptr, map, use_tma, use_ahead);
         return check_launch("k_g2p");
     }
     if (!ws || ws_bytes < g2p_workspace_bytes(p.n)) {
@@ -466,7 +516,7 @@ int launch_g2p(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_param
     int *count = static_cast<int *>(ws);
     int *list = reinterpret_cast<int *>(static_cast<char *>(ws) + 256);
     if (cudaMemsetAsync(count, 0, sizeof(int), s) != cudaSuccess) { set_error("g2p_stress: memset failed"); return MPMW_E_DEVICE; }
-    k_g2p<true><<<grid_for(p.n), kBlock, 0, s>>>(p, g, prm, st, list, count, map, use_tma);
+    k_g2p<true><<<grid_for(p.n), kBlock, 0, s>>>(p, g, prm, st, list, count, map, use_tma, use_ahead);
     MPMW_TRY_LAUNCH("k_g2p<fused>");
     k_stress_list<<<148 * 4, kBlock, 0, s>>>(p, prm.eff, list, count);
     return check_launch("k_stress_list");
