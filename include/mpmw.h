@@ -191,6 +191,32 @@ int mpmw_substep(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_par
 int mpmw_run_substeps(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm, int nsteps,
                       uint32_t *status, void *workspace, size_t ws_bytes, mpmw_stream_t stream);
 
+/* ---- batched independent scenes (parameter sweeps) ----------------------- */
+#define MPMW_BATCH_MAX_SCENES 192  /* scenes per batch (their grid tensor maps travel as a kernel parameter) */
+/* Many independent scenes stepped together, each kernel one launch over all of
+ * them (runMPMYDW.py:666-682 steps of independent scenes; the batching has no
+ * reference counterpart).  The scenes' particles are concatenated in the SoA
+ * arrays of *p: scene s owns particles [offsets[s], offsets[s+1]), every offset
+ * a multiple of 256 (a scene is padded with inactive particles, active = 0),
+ * offsets[0] = 0 and offsets[nscenes] = p->n.  grids[s] and prms[s] are scene
+ * s's grid and parameters; VLC must be off.
+ *
+ * Bytes of workspace for such a batch: the SVD worklist of
+ * mpmw_workspace_bytes(n) plus the scene table. */
+size_t mpmw_batch_workspace_bytes(const mpmw_grid_t *grids, int nscenes, int64_t n);
+/* Checks the batch (1 <= nscenes <= MPMW_BATCH_MAX_SCENES) and writes its scene
+ * table (each scene's grid and parameters; each CTA's scene) into the
+ * workspace; the library keeps the scenes' grid tensor maps for the run.
+ * Synchronizes `stream`; run it again after changing a grid, a parameter or
+ * the offsets. */
+int mpmw_batch_prepare(const mpmw_particles_t *p, const mpmw_grid_t *grids, const mpmw_params_t *prms,
+                       const int64_t *offsets, int nscenes, void *workspace, size_t ws_bytes, mpmw_stream_t stream);
+/* nsteps substeps of every scene of the batch prepared in this workspace: per
+ * scene the same result as mpmw_run_substeps on that scene alone.  No host
+ * synchronization (capturable in a CUDA graph). */
+int mpmw_batch_run_substeps(const mpmw_particles_t *p, int nsteps, uint32_t *status, void *workspace,
+                            size_t ws_bytes, mpmw_stream_t stream);
+
 /* utils/mpmRoutines.py:1446-1475 deactivate_and_teleport_xpbd_below_datum */
 int mpmw_teleport(const mpmw_particles_t *p, float z_datum, float teleport_distance, mpmw_stream_t stream);
 /* utils/mpmRoutines.py:3-21 creep_by_damage_with_baseline */

@@ -168,22 +168,33 @@ def particles_struct(n, **f) -> _lib.Particles:
     return P
 
 
+# mpmw_particles_t field -> (state object: 0 sim, 1 mpm, 2 xpbd; its attribute)
+PARTICLE_FIELDS = (
+    ("x", 0, "particle_x"), ("v", 0, "particle_v"),
+    ("C", 1, "particle_C"), ("F", 1, "particle_F"), ("F_trial", 1, "particle_F_trial"),
+    ("stress", 1, "particle_stress"), ("cov", 1, "particle_cov"),
+    ("vol", 0, "particle_vol"), ("mass", 0, "particle_mass"), ("density", 0, "particle_density"),
+    ("radius", 0, "particle_radius"),
+    ("mu", 1, "mu"), ("lam", 1, "lam"), ("ys", 1, "ys"), ("alpha", 1, "alpha"),
+    ("hardening", 1, "hardening"), ("softening", 1, "softening"), ("strain_criteria", 1, "strainCriteria"),
+    ("eta_shear", 1, "eta_shear"), ("eta_bulk", 1, "eta_bulk"),
+    ("acc_strain", 1, "particle_accumulated_strain"), ("damage", 1, "particle_damage"),
+    ("active", 0, "activeLabel"), ("material", 0, "materialLabel"),
+    ("x_pc", 2, "particle_x_initial_xpbd"), ("v_pc", 2, "particle_v_initial_xpbd"),
+)
+
+
+def particle_storage(sim, mpm=None, xpbd=None) -> dict:
+    """The state objects' SoA storage tensors by mpmw_particles_t field name
+    (None where the state object or the array is absent)."""
+    objs = (sim, mpm, xpbd)
+    return {name: (getattr(objs[w], "_s_" + attr, None) if objs[w] is not None else None)
+            for name, w, attr in PARTICLE_FIELDS}
+
+
 def particles_from_states(sim, mpm=None, xpbd=None) -> _lib.Particles:
     """Zero-copy C view of the state objects' SoA storage."""
-    g = lambda o, a: (getattr(o, "_s_" + a, None) if o is not None else None)  # noqa: E731
-    return particles_struct(
-        sim.nPoints,
-        x=g(sim, "particle_x"), v=g(sim, "particle_v"),
-        C=g(mpm, "particle_C"), F=g(mpm, "particle_F"), F_trial=g(mpm, "particle_F_trial"),
-        stress=g(mpm, "particle_stress"), cov=g(mpm, "particle_cov"),
-        vol=g(sim, "particle_vol"), mass=g(sim, "particle_mass"), density=g(sim, "particle_density"),
-        radius=g(sim, "particle_radius"),
-        mu=g(mpm, "mu"), lam=g(mpm, "lam"), ys=g(mpm, "ys"), alpha=g(mpm, "alpha"),
-        hardening=g(mpm, "hardening"), softening=g(mpm, "softening"), strain_criteria=g(mpm, "strainCriteria"),
-        eta_shear=g(mpm, "eta_shear"), eta_bulk=g(mpm, "eta_bulk"),
-        acc_strain=g(mpm, "particle_accumulated_strain"), damage=g(mpm, "particle_damage"),
-        active=g(sim, "activeLabel"), material=g(sim, "materialLabel"),
-        x_pc=g(xpbd, "particle_x_initial_xpbd"), v_pc=g(xpbd, "particle_v_initial_xpbd"))
+    return particles_struct(sim.nPoints, **particle_storage(sim, mpm, xpbd))
 
 
 def grid_struct(dims, mv=None, v=None, cell_div=None, cell_vol=None) -> _lib.Grid:

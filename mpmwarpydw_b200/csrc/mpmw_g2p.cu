@@ -17,11 +17,14 @@
 //   the first half of a substep whenever a workspace is given; SVD-path
 //   particles go to the same worklist and k_stress_p2g_list.
 // The worklists live in the caller's workspace (mpmw_workspace_bytes).
+#include <memory>
 #include <mutex>
 #include <unordered_map>
+#include <vector>
 
 #include "mpmw_common.cuh"
 #include "mpmw_gather.cuh"
+#include "mpmw_grid.cuh"
 #include "mpmw_internal.cuh"
 #include "mpmw_math.cuh"
 #include "mpmw_scatter.cuh"
@@ -60,31 +63,36 @@ __global__ void __launch_bounds__(kBlock) k_stress_list(mpmw_particles_t P, floa
     }
 }
 
+// SVD-path stress + P2G scatter of one particle listed by k_g2p2g
+__device__ __forceinline__ void stress_p2g_one(const mpmw_particles_t &P, const mpmw_grid_t &G,
+                                               const mpmw_params_t &prm, int64_t p, uint32_t &bad)
+{
+    const int64_t n = P.n;
+    float Ft[9], Cg[9], Fo[9], out[9];
+    load9(P.F_trial, n, p, Ft);
+    load9(P.C, n, p, Cg);
+    stress_particle<false>(P, prm.eff, MPMW_STRESS_SVD, p, Ft, Cg, nullptr, nullptr, Fo, out);
+    store9(P.F, n, p, Fo);
+    store_sym6(P.stress, n, p, out);
+    if (P.material[p] <= 1) {
+        float xp[3], v[3];
+        load3(P.x, n, p, xp);
+        load3(P.v, n, p, v);
+        const float st6[6] = {out[0], out[4], out[8], out[1], out[2], out[5]};
+        p2g_scatter_one(xp, v, Cg, st6, P.mass[p], P.vol[p], prm, reinterpret_cast<float4 *>(G.mv), G.dims[0],
+                        G.dims[1], G.dims[2], bad);
+    }
+}
+
 // SVD-path stress + P2G scatter for the particles listed by k_g2p2g
 __global__ void __launch_bounds__(kBlock) k_stress_p2g_list(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
                                                            uint32_t *status, const int *__restrict__ list,
                                                            const int *__restrict__ count)
 {
     const int cnt = *count;
-    const int64_t n = P.n;
     uint32_t bad = 0;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += gridDim.x * blockDim.x) {
-        const int64_t p = list[q];
-        float Ft[9], Cg[9], Fo[9], out[9];
-        load9(P.F_trial, n, p, Ft);
-        load9(P.C, n, p, Cg);
-        stress_particle<false>(P, prm.eff, MPMW_STRESS_SVD, p, Ft, Cg, nullptr, nullptr, Fo, out);
-        store9(P.F, n, p, Fo);
-        store_sym6(P.stress, n, p, out);
-        if (P.material[p] <= 1) {
-            float xp[3], v[3];
-            load3(P.x, n, p, xp);
-            load3(P.v, n, p, v);
-            const float st6[6] = {out[0], out[4], out[8], out[1], out[2], out[5]};
-            p2g_scatter_one(xp, v, Cg, st6, P.mass[p], P.vol[p], prm, reinterpret_cast<float4 *>(G.mv), G.dims[0],
-                            G.dims[1], G.dims[2], bad);
-        }
-    }
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += gridDim.x * blockDim.x)
+        stress_p2g_one(P, G, prm, list[q], bad);
     if (bad) raise_status(status, bad);
 }
 
@@ -98,15 +106,15 @@ struct G2PShared {
     uint64_t pbar;
 };
 
+// G2P of the CTA whose particles start at p0 (a multiple of kBlock).
 template <bool Fused>
-__global__ void __launch_bounds__(kBlock, 3) k_g2p(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
-                                               uint32_t *status, int *svd_list, int *svd_count,
-                                               const __grid_constant__ CUtensorMap tmap, int use_tma, int use_ahead)
+__device__ __forceinline__ void g2p_body(const mpmw_particles_t &P, const mpmw_grid_t &G, const mpmw_params_t &prm,
+                                         uint32_t *status, int *svd_list, int *svd_count, const CUtensorMap *tmap,
+                                         int use_tma, int use_ahead, int64_t p0)
 {
     __shared__ __align__(128) G2PShared S;
     const int64_t n = P.n;
     const int t = threadIdx.x;
-    const int64_t p0 = (int64_t)blockIdx.x * blockDim.x;
     const int64_t p = p0 + t;
     // F read ahead into shared memory by bulk copies (full CTAs; the host checks
     // the 16-byte alignment they need), in flight while the CTA waits for its tile
@@ -132,7 +140,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_g2p(mpmw_particles_t P, mpmw_grid
     for (int a = 0; a < 3; ++a) S.xpark[a][t] = xp[a];
     bool tile = false;
     int ox = 0, oy = 0, oz = 0;
-    if (!gather_prepare(S.g, act, W, &tmap, use_tma, status, tile, ox, oy, oz)) {
+    if (!gather_prepare(S.g, act, W, tmap, use_tma, status, tile, ox, oy, oz)) {
         // no active particle: the read-ahead must still land before the CTA exits
         if (ahead && !mbar_wait_bounded(&S.pbar, 0)) raise_status(status, MPMW_ST_TIMEOUT);
         return;  // uniform
@@ -182,6 +190,15 @@ __global__ void __launch_bounds__(kBlock, 3) k_g2p(mpmw_particles_t P, mpmw_grid
     if (bad) raise_status(status, bad);
 }
 
+template <bool Fused>
+__global__ void __launch_bounds__(kBlock, 3) k_g2p(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
+                                               uint32_t *status, int *svd_list, int *svd_count,
+                                               const __grid_constant__ CUtensorMap tmap, int use_tma, int use_ahead)
+{
+    g2p_body<Fused>(P, G, prm, status, svd_list, svd_count, &tmap, use_tma, use_ahead,
+                    (int64_t)blockIdx.x * blockDim.x);
+}
+
 struct G2P2GShared {
     GatherShared g;
     ScatterShared s;
@@ -219,13 +236,13 @@ __device__ __forceinline__ const float *ahead_src(const mpmw_particles_t &P, int
 }
 
 // G2P of substep k, return map of substep k+1, P2G of substep k+1 (into grid.mv,
-// which the caller has zeroed).  StoreStress: also write the stress (the last
+// which the caller has zeroed) for the CTA whose particles start at p0 (a
+// multiple of kScatterChunk).  StoreStress: also write the stress (the last
 // fused substep of a run).
 template <bool StoreStress>
-__global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
-                                                        uint32_t *status, int *svd_list, int *svd_count,
-                                                        const __grid_constant__ CUtensorMap tmap, int use_tma,
-                                                        int use_ahead)
+__device__ __forceinline__ void g2p2g_body(const mpmw_particles_t &P, const mpmw_grid_t &G, const mpmw_params_t &prm,
+                                           uint32_t *status, int *svd_list, int *svd_count, const CUtensorMap *tmap,
+                                           int use_tma, int use_ahead, int64_t p0)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     // the TMA destination (S.g.tile) must be 128-byte aligned: round the base up
@@ -233,7 +250,6 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g(mpmw
     G2P2GShared &S = *reinterpret_cast<G2P2GShared *>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
     const int64_t n = P.n;
     const int t = threadIdx.x;
-    const int64_t p0 = (int64_t)blockIdx.x * blockDim.x;
     const int64_t p = p0 + t;
     // read-ahead of the particle fields used after the gather (full CTAs only;
     // the host checks the 16-byte alignment the bulk copies need)
@@ -266,7 +282,7 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g(mpmw
     for (int a = 0; a < 3; ++a) xpark[a][t] = xp[a];
     bool tile = false;
     int ox = 0, oy = 0, oz = 0;
-    if (!gather_prepare(S.g, act, W, &tmap, use_tma, status, tile, ox, oy, oz)) {
+    if (!gather_prepare(S.g, act, W, tmap, use_tma, status, tile, ox, oy, oz)) {
         // no active particle: the read-ahead must still land before the CTA exits
         if (ahead && !mbar_wait_bounded(&S.pbar, 0)) raise_status(status, MPMW_ST_TIMEOUT);
         return;  // uniform
@@ -355,19 +371,31 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g(mpmw
     if (bad) raise_status(status, bad);
 }
 
+template <bool StoreStress>
+__global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
+                                                        uint32_t *status, int *svd_list, int *svd_count,
+                                                        const __grid_constant__ CUtensorMap tmap, int use_tma,
+                                                        int use_ahead)
+{
+    g2p2g_body<StoreStress>(P, G, prm, status, svd_list, svd_count, &tmap, use_tma, use_ahead,
+                            (int64_t)blockIdx.x * blockDim.x);
+}
+
 // The return map of a substep and its P2G in one pass (the reference's
 // compute_stress_from_F_trial followed by p2g_apic_with_stress): F_trial -> F
 // and stress (tensor form, in registers) and the CTA-cooperative scatter.  The
 // stress is written as the unfused stress kernel writes it; particles that
 // need the SVD path are listed for k_stress_p2g_list, particles that become
 // XPBD particles write their new v and do not scatter.
-__global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_stress_p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
-                                                             uint32_t *status, int *svd_list, int *svd_count)
+// (for the CTA whose particles start at p0, a multiple of kScatterChunk)
+__device__ __forceinline__ void stress_p2g_body(const mpmw_particles_t &P, const mpmw_grid_t &G,
+                                                const mpmw_params_t &prm, uint32_t *status, int *svd_list,
+                                                int *svd_count, int64_t p0)
 {
     extern __shared__ __align__(16) unsigned char smem_sp[];
     ScatterShared &S = *reinterpret_cast<ScatterShared *>(smem_sp);
     const int64_t n = P.n;
-    const int64_t p = (int64_t)blockIdx.x * kScatterChunk + threadIdx.x;
+    const int64_t p = p0 + threadIdx.x;
     bool scat = false;
     float xp[3] = {0.f, 0.f, 0.f}, v[3] = {0.f, 0.f, 0.f}, Cg[9], st6[6], Ft[9];
     float m = 0.f, vol = 0.f;
@@ -415,6 +443,12 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_stress_p2g
     p2g_scatter(S, scat, xp, v, Cg, st6, m, vol, prm, reinterpret_cast<float4 *>(G.mv), G.dims[0], G.dims[1],
                 G.dims[2], bad);
     if (bad) raise_status(status, bad);
+}
+
+__global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_stress_p2g(mpmw_particles_t P, mpmw_grid_t G, mpmw_params_t prm,
+                                                             uint32_t *status, int *svd_list, int *svd_count)
+{
+    stress_p2g_body(P, G, prm, status, svd_list, svd_count, (int64_t)blockIdx.x * kScatterChunk);
 }
 
 // ---------------------------------------------------------------------------
@@ -480,7 +514,7 @@ static bool cached_grid_map(const mpmw_grid_t &g, CUtensorMap *out)
     if (it != g_maps.end()) { *out = it->second; return true; }
     CUtensorMap m;
     if (!grid_tensor_map(g.v, g.dims, &m)) return false;
-    if (g_maps.size() > 64) g_maps.clear();
+    if (g_maps.size() > 512) g_maps.clear();
     g_maps.emplace(key, m);
     *out = m;
     return true;
@@ -524,6 +558,20 @@ int launch_g2p(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_param
 
 static bool g_g2p2g_attr[64];
 
+// the read-ahead bulk copies of k_g2p2g need every field's chunk start 16-byte aligned
+static bool g2p2g_ahead_ok(const mpmw_particles_t &p)
+{
+    if (p.n % 4 != 0) return false;
+    for (int f = 0; f < kAheadFields; ++f) {
+        const float *base = f < 9 ? p.F + (int64_t)f * p.n
+                                  : (f == 9 ? p.mu : f == 10 ? p.lam : f == 11 ? p.ys : f == 12 ? p.alpha
+                                     : f == 13 ? p.damage : f == 14 ? p.eta_shear : f == 15 ? p.eta_bulk
+                                     : f == 16 ? p.mass : p.vol);
+        if (!base || (reinterpret_cast<uintptr_t>(base) & 15u) != 0) return false;
+    }
+    return true;
+}
+
 int launch_g2p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st,
                  bool store_stress, void *ws, size_t ws_bytes, cudaStream_t s)
 {
@@ -550,15 +598,7 @@ int launch_g2p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_par
     int *count = static_cast<int *>(ws);
     int *list = reinterpret_cast<int *>(static_cast<char *>(ws) + 256);
     if (cudaMemsetAsync(count, 0, sizeof(int), s) != cudaSuccess) { set_error("g2p2g: memset failed"); return MPMW_E_DEVICE; }
-    // the read-ahead bulk copies need every field's chunk start 16-byte aligned
-    int use_ahead = (p.n % 4 == 0) ? 1 : 0;
-    for (int f = 0; f < kAheadFields && use_ahead; ++f) {
-        const float *base = f < 9 ? p.F + (int64_t)f * p.n
-                                  : (f == 9 ? p.mu : f == 10 ? p.lam : f == 11 ? p.ys : f == 12 ? p.alpha
-                                     : f == 13 ? p.damage : f == 14 ? p.eta_shear : f == 15 ? p.eta_bulk
-                                     : f == 16 ? p.mass : p.vol);
-        if (!base || (reinterpret_cast<uintptr_t>(base) & 15u) != 0) use_ahead = 0;
-    }
+    const int use_ahead = g2p2g_ahead_ok(p) ? 1 : 0;
     const unsigned grid = grid_for(p.n, kScatterChunk);
     if (store_stress) k_g2p2g<true><<<grid, kScatterChunk, smem, s>>>(p, g, prm, st, list, count, map, use_tma, use_ahead);
     else k_g2p2g<false><<<grid, kScatterChunk, smem, s>>>(p, g, prm, st, list, count, map, use_tma, use_ahead);
@@ -595,6 +635,297 @@ int launch_stress_p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpm
     MPMW_TRY_LAUNCH("k_stress_p2g");
     k_stress_p2g_list<<<148 * 4, kBlock, 0, s>>>(p, g, prm, st, list, count);
     return check_launch("k_stress_p2g_list");
+}
+
+// ---------------------------------------------------------------------------
+// batched scenes: one launch per kernel over many independent scenes
+// ---------------------------------------------------------------------------
+// The scenes' particles are concatenated in one set of SoA arrays (scene s owns
+// the CTA-aligned particle range [offsets[s], offsets[s+1])); each scene keeps
+// its own grid, parameters and grid tensor map.  mpmw_batch_prepare writes a
+// table into the workspace: per scene its grid and parameters (128 B), and per
+// CTA its scene, for the particle kernels and for the grid-node kernels.  A
+// particle CTA reads its scene index once and one warp stages the scene's
+// record in shared memory.  The tensor maps travel as a __grid_constant__
+// kernel parameter (the usual home of a TMA descriptor: no proxy fence).
+struct BatchScene {
+    mpmw_grid_t grid;
+    mpmw_params_t prm;
+};
+static_assert(sizeof(BatchScene) % 4 == 0 && sizeof(BatchScene) <= 32 * 4 * 2, "a scene record is staged by one warp");
+
+struct BatchMaps {
+    CUtensorMap tmap[MPMW_BATCH_MAX_SCENES];
+};
+static_assert(sizeof(BatchMaps) + sizeof(mpmw_particles_t) + 128 <= 32764, "the maps fit the kernel parameter space");
+
+struct BatchRef {  // kernel argument: pointers into the prepared workspace
+    const BatchScene *scene;
+    const int *pcta_scene;  // particle CTA -> scene
+    const int *ncta_scene;  // grid-node CTA -> scene
+    const int *ncta_first;  // scene -> its first grid-node CTA
+    int use_tma;
+};
+
+// Every thread of the CTA calls it: scene index of this particle CTA, and the
+// scene's record copied into `rec` (published by the barrier).
+__device__ __forceinline__ int stage_scene(const BatchRef &R, BatchScene &rec)
+{
+    const int s = R.pcta_scene[blockIdx.x];
+    constexpr int kWords = (int)(sizeof(BatchScene) / 4);
+    if (threadIdx.x < kWords)
+        reinterpret_cast<uint32_t *>(&rec)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&R.scene[s])[threadIdx.x];
+    __syncthreads();
+    return s;
+}
+
+// Grid-node CTAs of the batch cover kBatchNodesPerCta nodes of one scene each
+// (kBatchNodesPerThread per thread, kBlock apart), so the scene lookup is paid
+// once per 2048 nodes.
+constexpr int kBatchNodesPerThread = 8;
+constexpr int kBatchNodesPerCta = kBlock * kBatchNodesPerThread;
+
+__global__ void __launch_bounds__(kBlock) k_zero_grid_batch(const BatchRef R)
+{
+    const int s = R.ncta_scene[blockIdx.x];
+    const mpmw_grid_t G = R.scene[s].grid;
+    const int64_t total = (int64_t)G.dims[0] * G.dims[1] * G.dims[2];
+    const int64_t g0 = (int64_t)(blockIdx.x - R.ncta_first[s]) * kBatchNodesPerCta + threadIdx.x;
+#pragma unroll
+    for (int u = 0; u < kBatchNodesPerThread; ++u) {
+        const int64_t g = g0 + (int64_t)u * kBlock;
+        if (g < total) reinterpret_cast<float4 *>(G.mv)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_grid_update_batch(const BatchRef R, int zero_mv)
+{
+    const int s = R.ncta_scene[blockIdx.x];
+    const BatchScene B = R.scene[s];
+    const int64_t g0 = (int64_t)(blockIdx.x - R.ncta_first[s]) * kBatchNodesPerCta + threadIdx.x;
+#pragma unroll 2
+    for (int u = 0; u < kBatchNodesPerThread; ++u) grid_update_node(B.grid, B.prm, zero_mv, g0 + (int64_t)u * kBlock);
+}
+
+__global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_stress_p2g_batch(
+    mpmw_particles_t P, const BatchRef R, uint32_t *status, int *svd_list, int *svd_count)
+{
+    __shared__ BatchScene B;
+    stage_scene(R, B);
+    stress_p2g_body(P, B.grid, B.prm, status, svd_list, svd_count, (int64_t)blockIdx.x * kScatterChunk);
+}
+
+template <bool StoreStress>
+__global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g_batch(
+    mpmw_particles_t P, const BatchRef R, const __grid_constant__ BatchMaps M, uint32_t *status, int *svd_list,
+    int *svd_count, int use_ahead)
+{
+    __shared__ BatchScene B;
+    const int s = stage_scene(R, B);
+    g2p2g_body<StoreStress>(P, B.grid, B.prm, status, svd_list, svd_count, &M.tmap[s], R.use_tma, use_ahead,
+                            (int64_t)blockIdx.x * kScatterChunk);
+}
+
+__global__ void __launch_bounds__(kBlock, 3) k_g2p_batch(mpmw_particles_t P, const BatchRef R,
+                                                     const __grid_constant__ BatchMaps M, uint32_t *status,
+                                                     int use_ahead)
+{
+    static_assert(kBlock == kScatterChunk, "particle CTAs of the batched G2P and P2G kernels coincide");
+    __shared__ BatchScene B;
+    const int s = stage_scene(R, B);
+    g2p_body<false>(P, B.grid, B.prm, status, nullptr, nullptr, &M.tmap[s], R.use_tma, use_ahead,
+                    (int64_t)blockIdx.x * kBlock);
+}
+
+__global__ void __launch_bounds__(kBlock) k_stress_p2g_list_batch(mpmw_particles_t P, const BatchRef R,
+                                                                 uint32_t *status, const int *__restrict__ list,
+                                                                 const int *__restrict__ count)
+{
+    const int cnt = *count;
+    uint32_t bad = 0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += gridDim.x * blockDim.x) {
+        const int64_t p = list[q];
+        const BatchScene &B = R.scene[R.pcta_scene[p / kScatterChunk]];
+        stress_p2g_one(P, B.grid, B.prm, p, bad);
+    }
+    if (bad) raise_status(status, bad);
+}
+
+namespace {
+// Workspace layout of a batch: SVD worklist count (256 B) and list (n ints),
+// then the scene records, then the three CTA tables.
+struct BatchLayout {
+    size_t scenes, pcta, ncta, nfirst, total;
+};
+size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+BatchLayout batch_layout(int64_t n, int nscenes, int64_t nctas)
+{
+    BatchLayout L;
+    L.scenes = g2p_workspace_bytes(n);
+    L.pcta = L.scenes + round256((size_t)nscenes * sizeof(BatchScene));
+    L.ncta = L.pcta + round256((size_t)(n / kScatterChunk) * sizeof(int));
+    L.nfirst = L.ncta + round256((size_t)nctas * sizeof(int));
+    L.total = L.nfirst + round256((size_t)(nscenes + 1) * sizeof(int));
+    return L;
+}
+int64_t scene_node_ctas(const mpmw_grid_t &g)
+{
+    return grid_for((int64_t)g.dims[0] * g.dims[1] * g.dims[2], kBatchNodesPerCta);
+}
+int64_t batch_node_ctas(const mpmw_grid_t *grids, int nscenes)
+{
+    int64_t c = 0;
+    for (int k = 0; k < nscenes; ++k) c += scene_node_ctas(grids[k]);
+    return c;
+}
+// what a prepared workspace holds, for mpmw_batch_run_substeps
+struct BatchPrepared {
+    int64_t n;
+    int nscenes, pctas, nctas, use_tma, use_ahead, use_ahead_g2p;
+    BatchLayout L;
+    std::shared_ptr<BatchMaps> maps;
+};
+std::mutex g_batch_mu;
+std::unordered_map<const void *, BatchPrepared> g_batches;
+}  // namespace
+
+size_t batch_workspace_bytes(const mpmw_grid_t *grids, int nscenes, int64_t n)
+{
+    return batch_layout(n, nscenes, batch_node_ctas(grids, nscenes)).total;
+}
+
+// Writes the scene table into the workspace (synchronizes the stream) and
+// remembers the batch's launch sizes.  The caller has checked the arguments.
+int prepare_batch(const mpmw_particles_t &p, const mpmw_grid_t *grids, const mpmw_params_t *prms,
+                  const int64_t *offsets, int nscenes, void *ws, size_t ws_bytes, cudaStream_t s)
+{
+    const int64_t nctas = batch_node_ctas(grids, nscenes);
+    const BatchLayout L = batch_layout(p.n, nscenes, nctas);
+    if (nscenes > MPMW_BATCH_MAX_SCENES) {
+        set_error("batch: %d scenes (at most %d per batch)", nscenes, MPMW_BATCH_MAX_SCENES);
+        return MPMW_E_ARG;
+    }
+    if (reinterpret_cast<uintptr_t>(ws) & 15u) { set_error("batch: the workspace must be 16-byte aligned"); return MPMW_E_ARG; }
+    if (ws_bytes < L.total) {
+        set_error("batch: workspace of %zu bytes is smaller than the %zu required", ws_bytes, L.total);
+        return MPMW_E_WORKSPACE;
+    }
+    const size_t tbytes = L.total - L.scenes;
+    std::vector<unsigned char> host(tbytes, 0);
+    BatchScene *sc = reinterpret_cast<BatchScene *>(host.data());
+    int *pcta = reinterpret_cast<int *>(host.data() + (L.pcta - L.scenes));
+    int *ncta = reinterpret_cast<int *>(host.data() + (L.ncta - L.scenes));
+    int *nfirst = reinterpret_cast<int *>(host.data() + (L.nfirst - L.scenes));
+    auto maps = std::make_shared<BatchMaps>();
+    memset(maps.get(), 0, sizeof(BatchMaps));
+    int use_tma = 1, c = 0;
+    for (int k = 0; k < nscenes; ++k) {
+        if (!cached_grid_map(grids[k], &maps->tmap[k])) use_tma = 0;
+        sc[k].grid = grids[k];
+        sc[k].prm = prms[k];
+        for (int64_t b = offsets[k] / kScatterChunk; b < offsets[k + 1] / kScatterChunk; ++b) pcta[b] = k;
+        nfirst[k] = c;
+        const int nc = (int)scene_node_ctas(grids[k]);
+        for (int b = 0; b < nc; ++b) ncta[c + b] = k;
+        c += nc;
+    }
+    nfirst[nscenes] = c;
+    unsigned char *dst = static_cast<unsigned char *>(ws) + L.scenes;
+    if (cudaMemcpyAsync(dst, host.data(), tbytes, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        set_error("batch: copying the scene table failed");
+        return MPMW_E_DEVICE;
+    }
+    BatchPrepared bp;
+    bp.n = p.n;
+    bp.nscenes = nscenes;
+    bp.pctas = (int)(p.n / kScatterChunk);
+    bp.nctas = (int)nctas;
+    bp.use_tma = use_tma;
+    bp.use_ahead = g2p2g_ahead_ok(p) ? 1 : 0;
+    bp.use_ahead_g2p = p.F && p.n % 4 == 0 && (reinterpret_cast<uintptr_t>(p.F) & 15u) == 0 ? 1 : 0;
+    bp.L = L;
+    bp.maps = maps;
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    if (g_batches.size() > 256) g_batches.clear();
+    g_batches[ws] = bp;
+    return MPMW_OK;
+}
+
+static bool g_batch_attr[64];
+
+// The fused schedule of mpmw_run_substeps over every scene of a batch that
+// prepare_batch wrote into this workspace.
+int launch_batch_substeps(const mpmw_particles_t &p, int nsteps, uint32_t *st, void *ws, size_t ws_bytes,
+                          cudaStream_t s)
+{
+    BatchPrepared bp;
+    {
+        std::lock_guard<std::mutex> lk(g_batch_mu);
+        auto it = g_batches.find(ws);
+        if (it == g_batches.end()) { set_error("batch: the workspace was not prepared (mpmw_batch_prepare)"); return MPMW_E_ARG; }
+        bp = it->second;
+    }
+    if (bp.n != p.n || ws_bytes < bp.L.total) {
+        set_error("batch: the workspace was prepared for %lld particles in %zu bytes", (long long)bp.n, bp.L.total);
+        return MPMW_E_ARG;
+    }
+    if (nsteps == 0 || p.n == 0) return MPMW_OK;
+    const size_t smem = sizeof(G2P2GShared) + 128;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { set_error("batch: no current device"); return MPMW_E_DEVICE; }
+    if (dev >= 0 && dev < 64 && !g_batch_attr[dev]) {
+        if (cudaFuncSetAttribute(k_g2p2g_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+            cudaFuncSetAttribute(k_g2p2g_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+            cudaFuncSetAttribute(k_stress_p2g_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(ScatterShared)) != cudaSuccess) {
+            set_error("batch: cannot reserve %zu bytes of shared memory", smem);
+            return MPMW_E_DEVICE;
+        }
+        g_batch_attr[dev] = true;
+    }
+    unsigned char *base = static_cast<unsigned char *>(ws);
+    BatchRef R;
+    R.scene = reinterpret_cast<const BatchScene *>(base + bp.L.scenes);
+    R.pcta_scene = reinterpret_cast<const int *>(base + bp.L.pcta);
+    R.ncta_scene = reinterpret_cast<const int *>(base + bp.L.ncta);
+    R.ncta_first = reinterpret_cast<const int *>(base + bp.L.nfirst);
+    R.use_tma = bp.use_tma;
+    int *count = static_cast<int *>(ws);
+    int *list = reinterpret_cast<int *>(base + 256);
+    const unsigned pctas = (unsigned)bp.pctas, nctas = (unsigned)bp.nctas;
+    auto reset_count = [&]() -> int {
+        if (cudaMemsetAsync(count, 0, sizeof(int), s) != cudaSuccess) { set_error("batch: memset failed"); return MPMW_E_DEVICE; }
+        return MPMW_OK;
+    };
+    // prologue: every grid cleared, substep 1's return map and P2G
+    k_zero_grid_batch<<<nctas, kBlock, 0, s>>>(R);
+    MPMW_TRY_LAUNCH("k_zero_grid_batch");
+    if (reset_count() != MPMW_OK) return MPMW_E_DEVICE;
+    k_stress_p2g_batch<<<pctas, kScatterChunk, sizeof(ScatterShared), s>>>(p, R, st, list, count);
+    MPMW_TRY_LAUNCH("k_stress_p2g_batch");
+    k_stress_p2g_list_batch<<<148 * 4, kBlock, 0, s>>>(p, R, st, list, count);
+    MPMW_TRY_LAUNCH("k_stress_p2g_list_batch");
+    for (int step = 0; step < nsteps; ++step) {
+        if (step < nsteps - 1) {
+            k_grid_update_batch<<<nctas, kBlock, 0, s>>>(R, 1);
+            MPMW_TRY_LAUNCH("k_grid_update_batch");
+            if (reset_count() != MPMW_OK) return MPMW_E_DEVICE;
+            if (step + 1 == nsteps - 1)
+                k_g2p2g_batch<true><<<pctas, kScatterChunk, smem, s>>>(p, R, *bp.maps, st, list, count, bp.use_ahead);
+            else
+                k_g2p2g_batch<false><<<pctas, kScatterChunk, smem, s>>>(p, R, *bp.maps, st, list, count, bp.use_ahead);
+            MPMW_TRY_LAUNCH("k_g2p2g_batch");
+            k_stress_p2g_list_batch<<<148 * 4, kBlock, 0, s>>>(p, R, st, list, count);
+            MPMW_TRY_LAUNCH("k_stress_p2g_list_batch");
+        } else {
+            k_grid_update_batch<<<nctas, kBlock, 0, s>>>(R, 0);
+            MPMW_TRY_LAUNCH("k_grid_update_batch");
+            k_g2p_batch<<<pctas, kBlock, 0, s>>>(p, R, *bp.maps, st, bp.use_ahead_g2p);
+            MPMW_TRY_LAUNCH("k_g2p_batch");
+        }
+    }
+    return MPMW_OK;
 }
 
 }  // namespace mpmw

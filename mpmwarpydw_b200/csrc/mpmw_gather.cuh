@@ -31,7 +31,8 @@ struct GatherShared {
 
 // Phase 1 (every thread of the CTA calls it): CTA bounding box of the active
 // particles' stencil bases and, when it fits, the TMA load of the grid tile.
-// Returns false (uniformly) when the CTA has no active particle.
+// Returns false (uniformly) when the CTA has no active particle.  tmap is a
+// kernel parameter (or an element of one).
 __device__ __forceinline__ bool gather_prepare(GatherShared &S, bool act, const Weights &W, const CUtensorMap *tmap,
                                                int use_tma, uint32_t *status, bool &tile, int &ox, int &oy, int &oz)
 {

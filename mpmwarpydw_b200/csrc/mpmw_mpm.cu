@@ -8,6 +8,7 @@
 #include <cstring>
 
 #include "mpmw_common.cuh"
+#include "mpmw_grid.cuh"
 #include "mpmw_internal.cuh"
 #include "mpmw_math.cuh"
 
@@ -33,117 +34,11 @@ int check_launch(const char *what)
     return MPMW_OK;
 }
 
-// ---------------------------------------------------------------------------
-// grid update: normalisation + gravity + damping + boundary condition
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ float coulomb(float v, float mu, float dt, float g)
-{
-    if (fabsf(v) < 1e-12f) return 0.f;
-    float dvf = (mu * g) * dt;
-    float s = v < 0.f ? -1.f : 1.f;
-    return s * rmax(fabsf(v) - dvf, 0.f);
-}
-
-__device__ __forceinline__ void apply_bc(int bc, const int *idx, const int *dim, float *o, float mu, float rest,
-                                         float dt, float g, int pad)
-{
-    float v[3] = {o[0], o[1], o[2]};
-    if (bc == MPMW_BC_FRICTION || bc == MPMW_BC_RESTITUTION) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const int t0 = (a + 1) % 3, t1 = (a + 2) % 3;
-#pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                bool hit = side == 0 ? (idx[a] <= pad && v[a] < 0.f) : (idx[a] >= dim[a] - pad && v[a] > 0.f);
-                if (!hit) continue;
-                float w[3];
-                w[a] = bc == MPMW_BC_FRICTION ? 0.f : -rest * v[a];
-                w[t0] = coulomb(v[t0], mu, dt, g);
-                w[t1] = coulomb(v[t1], mu, dt, g);
-                o[0] = w[0]; o[1] = w[1]; o[2] = w[2];
-            }
-        }
-    } else if (bc == MPMW_BC_FRICTION_GRADUAL) {
-        const float padf = (float)pad;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const int t0 = (a + 1) % 3, t1 = (a + 2) % 3;
-            float fade = 0.f;
-            bool hit = false;
-            if (idx[a] < pad && v[a] < 0.f) { fade = (float)idx[a] / padf; hit = true; }
-            else if (idx[a] >= dim[a] - pad && v[a] > 0.f) { fade = (float)(dim[a] - 1 - idx[a]) / padf; hit = true; }
-            if (!hit) continue;
-            float fm = mu * (1.f - fade);
-            float w[3];
-            w[t0] = coulomb(v[t0], fm, dt, g);
-            w[t1] = coulomb(v[t1], fm, dt, g);
-            w[a] = 0.f * (1.f - fade) + v[a] * fade;
-            o[0] = w[0]; o[1] = w[1]; o[2] = w[2];
-        }
-    } else if (bc == MPMW_BC_ABSORBING) {
-        const float padf = (float)pad;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-#pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                bool hit = side == 0 ? (idx[a] < 3) : (idx[a] >= dim[a] - 3);
-                if (!hit) continue;
-                float lf = side == 0 ? (padf - (float)idx[a]) / padf : (padf - (float)(dim[a] - 1 - idx[a])) / padf;
-                float damp = 0.f * lf + 1.f * (1.f - lf);
-                o[0] = v[0] * damp; o[1] = v[1] * damp; o[2] = v[2] * damp;
-            }
-        }
-    } else if (bc == MPMW_BC_PLANE_STRAIN_Y) {
-        const int ix = idx[0], iy = idx[1], iz = idx[2];
-        if (ix <= pad && v[0] < 0.f) { o[0] = 0.f; o[1] = coulomb(v[1], mu, dt, g); o[2] = coulomb(v[2], mu, dt, g); }
-        if (ix >= dim[0] - pad && v[0] > 0.f) { o[0] = 0.f; o[1] = coulomb(v[1], mu, dt, g); o[2] = coulomb(v[2], mu, dt, g); }
-        if (iy <= pad) { v[0] = o[0]; v[1] = o[1]; v[2] = o[2]; o[0] = v[0]; o[1] = 0.f; o[2] = v[2]; }
-        if (iy >= dim[1] - pad) { v[0] = o[0]; v[1] = o[1]; v[2] = o[2]; o[0] = v[0]; o[1] = 0.f; o[2] = v[2]; }
-        if (iz <= pad && v[2] < 0.f) { float a0 = coulomb(v[0], mu, dt, g), a1 = coulomb(v[1], mu, dt, g); o[0] = a0; o[1] = a1; o[2] = 0.f; }
-        if (iz >= dim[2] - pad && v[2] > 0.f) { float a0 = coulomb(v[0], mu, dt, g), a1 = coulomb(v[1], mu, dt, g); o[0] = a0; o[1] = a1; o[2] = 0.f; }
-    } else if (bc == MPMW_BC_PLANE_STRAIN_Y_GLOBAL) {
-        const int ix = idx[0], iz = idx[2];
-        o[1] = 0.f;
-        v[0] = o[0]; v[1] = o[1]; v[2] = o[2];
-        if (ix <= pad && v[0] < 0.f) { o[0] = 0.f; o[1] = 0.f; o[2] = coulomb(v[2], mu, dt, g); }
-        if (ix >= dim[0] - pad && v[0] > 0.f) { o[0] = 0.f; o[1] = 0.f; o[2] = coulomb(v[2], mu, dt, g); }
-        if (iz <= pad && v[2] < 0.f) { o[0] = coulomb(v[0], mu, dt, g); o[1] = 0.f; o[2] = 0.f; }
-        if (iz >= dim[2] - pad && v[2] > 0.f) { o[0] = coulomb(v[0], mu, dt, g); o[1] = 0.f; o[2] = 0.f; }
-    }
-}
-
 // zero_mv: also clear the accumulators after reading them (for the fused
 // G2P->P2G kernel, which scatters the next substep into them)
 __global__ void __launch_bounds__(kBlock) k_grid_update(mpmw_grid_t G, mpmw_params_t prm, int zero_mv)
 {
-    const int nx = G.dims[0], ny = G.dims[1], nz = G.dims[2];
-    const int64_t total = (int64_t)nx * ny * nz;
-    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= total) return;
-    const float4 a = reinterpret_cast<const float4 *>(G.mv)[g];
-    if (zero_mv) reinterpret_cast<float4 *>(G.mv)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
-    float o[3] = {0.f, 0.f, 0.f};
-    if (a.x > 1e-15f) {
-        float inv = 1.f / a.x;
-        o[0] = a.y * inv + prm.dt * prm.gravity[0];
-        o[1] = a.z * inv + prm.dt * prm.gravity[1];
-        o[2] = a.w * inv + prm.dt * prm.gravity[2];
-    }
-    if (prm.grid_v_damping_scale < 1.f) {
-        o[0] = o[0] * prm.grid_v_damping_scale;
-        o[1] = o[1] * prm.grid_v_damping_scale;
-        o[2] = o[2] * prm.grid_v_damping_scale;
-    }
-    if (prm.boundary_condition >= 0) {
-        int iz = (int)(g % nz);
-        int64_t r = g / nz;
-        int iy = (int)(r % ny), ix = (int)(r / ny);
-        int idx[3] = {ix, iy, iz}, dim[3] = {nx, ny, nz};
-        float gm = fabsf(prm.gravity[2]);
-        apply_bc(prm.boundary_condition, idx, dim, o, prm.bound_friction, prm.bound_restitution, prm.dt, gm,
-                 prm.boundary_padding);
-    }
-    reinterpret_cast<float4 *>(G.v)[g] = make_float4(o[0], o[1], o[2], 0.f);
+    grid_update_node(G, prm, zero_mv, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // single grid operations with the reference kernels' exact write sets:
@@ -171,9 +66,9 @@ __global__ void __launch_bounds__(kBlock) k_grid_op(mpmw_grid_t G, mpmw_params_t
     } else {
         float4 t = v4[g];
         float o[3] = {t.x, t.y, t.z};
-        int iz = (int)(g % nz);
-        int64_t r = g / nz;
-        int iy = (int)(r % ny), ix = (int)(r / ny);
+        const int gi = (int)g;  // grids hold at most 2^31 - 1 nodes
+        int iz = gi % nz, r = gi / nz;
+        int iy = r % ny, ix = r / ny;
         int idx[3] = {ix, iy, iz}, dim[3] = {nx, ny, nz};
         apply_bc(prm.boundary_condition, idx, dim, o, prm.bound_friction, prm.bound_restitution, prm.dt,
                  fabsf(prm.gravity[2]), prm.boundary_padding);
@@ -615,6 +510,48 @@ int mpmw_run_substeps(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpm
         }
     }
     return MPMW_OK;
+}
+
+size_t mpmw_batch_workspace_bytes(const mpmw_grid_t *grids, int nscenes, int64_t n)
+{
+    if (!grids || nscenes < 1 || n < 0) return 0;
+    for (int k = 0; k < nscenes; ++k)
+        if (grids[k].dims[0] <= 0 || grids[k].dims[1] <= 0 || grids[k].dims[2] <= 0) return 0;
+    return batch_workspace_bytes(grids, nscenes, n);
+}
+
+int mpmw_batch_prepare(const mpmw_particles_t *p, const mpmw_grid_t *grids, const mpmw_params_t *prms,
+                       const int64_t *offsets, int nscenes, void *workspace, size_t ws_bytes, mpmw_stream_t stream)
+{
+    MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV | kNeedCF | kNeedStress));
+    if (!grids || !prms || !offsets) { set_error("batch: grids, prms and offsets are required"); return MPMW_E_ARG; }
+    if (nscenes < 1) { set_error("batch: %d scenes (at least 1)", nscenes); return MPMW_E_ARG; }
+    if (p->n > 0 && (!p->vol || !p->mass)) { set_error("batch: vol and mass are required"); return MPMW_E_ARG; }
+    if (offsets[0] != 0 || offsets[nscenes] != p->n) {
+        set_error("batch: offsets must run from 0 to the particle count %lld", (long long)p->n);
+        return MPMW_E_ARG;
+    }
+    for (int k = 0; k < nscenes; ++k) {
+        MPMW_TRY(check_grid(&grids[k]));
+        MPMW_TRY(check_params(&prms[k]));
+        if (offsets[k + 1] <= offsets[k] || offsets[k] % 256 != 0) {
+            set_error("batch: scene %d: offsets must increase and be multiples of 256", k);
+            return MPMW_E_ARG;
+        }
+        if (prms[k].vlc) { set_error("batch: scene %d: volumetric locking correction is not batched", k); return MPMW_E_ARG; }
+        if (prms[k].update_cov && !p->cov) { set_error("batch: scene %d: update_cov needs cov", k); return MPMW_E_ARG; }
+    }
+    if (!workspace) { set_error("batch: workspace is NULL"); return MPMW_E_WORKSPACE; }
+    return prepare_batch(*p, grids, prms, offsets, nscenes, workspace, ws_bytes, as_stream(stream));
+}
+
+int mpmw_batch_run_substeps(const mpmw_particles_t *p, int nsteps, uint32_t *status, void *workspace,
+                            size_t ws_bytes, mpmw_stream_t stream)
+{
+    MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV | kNeedCF | kNeedStress));
+    if (nsteps < 0) { set_error("nsteps must be >= 0"); return MPMW_E_ARG; }
+    if (!workspace) { set_error("batch: workspace is NULL"); return MPMW_E_WORKSPACE; }
+    return launch_batch_substeps(*p, nsteps, status, workspace, ws_bytes, as_stream(stream));
 }
 
 int mpmw_teleport(const mpmw_particles_t *p, float z_datum, float teleport_distance, mpmw_stream_t stream)

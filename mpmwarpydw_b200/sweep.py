@@ -1,10 +1,15 @@
 """Batched parameter sweeps: many independent scenes of uneven size.
 
-Each scene keeps its own state objects and grid.  ``SceneBatch`` advances all
-of them together: every scene's ``mpmw_run_substeps`` call goes to its own
-CUDA stream, and the whole batch step is captured once into a CUDA graph
-(fork/join across the scene streams) that is replayed, so one graph launch
-runs every scene's substeps concurrently on the GPU.
+Two ways to step a batch:
+
+- ``ConcatBatch`` concatenates the scenes' particles (each scene padded with
+  inactive particles to a multiple of 256) into one set of SoA arrays, keeps
+  each scene's grid, and steps every scene with one launch per kernel
+  (``mpmw_batch_run_substeps``): a CTA finds its scene in a table passed as a
+  kernel parameter.  The batch step can be captured as a CUDA graph.
+- ``SceneBatch`` keeps each scene's own state objects and gives every
+  scene's ``mpmw_run_substeps`` call its own CUDA stream; the whole batch step
+  is captured once into a CUDA graph (fork/join across the scene streams).
 
 Across GPUs the scenes shard with no data-path exchange: :func:`partition`
 assigns scenes to ranks by particle count (longest first, each to the least
@@ -105,6 +110,151 @@ class SceneBatch:
             mom = (m[:, None] * v).sum(0).double().cpu().tolist()
             out.append(SceneResult(i, sim.nPoints, int(act.sum().item()),
                                    float(mpm.particle_damage[act].double().mean().item()) if act.any() else 0.0,
+                                   tuple(mom), float(v.abs().max().item())))
+        return out
+
+
+_CHUNK = 256  # particles per CTA: scene offsets are multiples of this
+
+
+class ConcatBatch:
+    """Independent scenes stepped by one launch per kernel over concatenated
+    particle arrays (``mpmw_batch_run_substeps``).
+
+    ``fields[name]`` holds every scene's particles of that mpmw_particles_t
+    field; scene i owns columns ``offsets[i]:offsets[i] + counts[i]`` (the
+    rest of its 256-aligned range is inactive padding).  The per-scene state
+    objects built from the domains keep their grids, which the batch steps in
+    place; :meth:`sync_scenes` copies the particle results back into them."""
+
+    def __init__(self, scenes, device="cuda:0", sort=True):
+        import ctypes
+
+        from . import _lib, domains
+        from .bind import grid_from_state, params_from_states, particle_storage, particles_struct, status_word
+        from .engine import sort_particles
+        if not scenes:
+            raise ValueError("a batch needs at least one scene")
+        self.device = torch.device(device)
+        self.states = []
+        for d in scenes:
+            sim, mpm, xpbd = domains.build(d, device=self.device)
+            if sort:
+                sort_particles(sim, mpm, xpbd)
+            self.states.append((sim, mpm, xpbd))
+        self.counts = [s[0].nPoints for s in self.states]
+        offs = [0]
+        for c in self.counts:
+            offs.append(offs[-1] + -(-c // _CHUNK) * _CHUNK)
+        self.offsets = offs
+        self.total = offs[-1]
+        per = [particle_storage(*st) for st in self.states]
+        self.fields = {}
+        self._aos = {}  # field -> values per particle of a flat per-particle (AoS) array, e.g. cov (6)
+        for name in per[0]:
+            parts = [p[name] for p in per]
+            if all(t is None for t in parts):
+                self.fields[name] = None
+                continue
+            if any(t is None for t in parts):
+                raise ValueError(f"field {name} is present in some scenes only")
+            t0, c0 = parts[0], self.counts[0]
+            k = t0.numel() // c0 if t0.dim() == 1 and t0.numel() != c0 else 0
+            self._aos[name] = k
+            cols = []
+            for t, c, o0, o1 in zip(parts, self.counts, offs[:-1], offs[1:]):
+                if k:  # AoS: k values per particle, padding appended row by row
+                    t = t.view(c, k)
+                cols.append(t)
+                if o1 - o0 > c:  # inactive padding (active label 0)
+                    shape = (o1 - o0 - c, k) if k else (*t.shape[:-1], o1 - o0 - c)
+                    cols.append(torch.zeros(*shape, dtype=t.dtype, device=t.device))
+            cat = torch.cat(cols, dim=0 if k else -1)
+            self.fields[name] = (cat.reshape(-1) if k else cat).contiguous()
+        self.P = particles_struct(self.total, **self.fields)
+        n = len(self.states)
+        self.grids = (_lib.Grid * n)(*[grid_from_state(mpm) for _, mpm, _ in self.states])
+        self.prms = (_lib.Params * n)(*[params_from_states(sim, mpm) for sim, mpm, _ in self.states])
+        self.offs = (ctypes.c_int64 * (n + 1))(*offs)
+        L = _lib.lib()
+        self.ws = torch.empty(int(L.mpmw_batch_workspace_bytes(self.grids, n, self.total)), dtype=torch.uint8,
+                              device=self.device)
+        self.status = status_word(self.device)
+        self.graph = None
+        self.graph_steps = 0
+        self.prepare()
+        torch.cuda.synchronize(self.device)
+
+    def prepare(self):
+        """(Re)write the scene table (grids, parameters, tensor maps) into the
+        workspace; needed again after a scene's parameters change."""
+        import ctypes
+
+        from . import _lib
+        from .bind import stream_handle
+        _lib.check(_lib.lib().mpmw_batch_prepare(ctypes.byref(self.P), self.grids, self.prms, self.offs,
+                                                 len(self.states), self.ws.data_ptr(), self.ws.numel(),
+                                                 stream_handle(torch.cuda.current_stream(self.device))),
+                   "batch_prepare")
+
+    @property
+    def particles(self):
+        return sum(self.counts)
+
+    def step(self, k: int):
+        """k substeps of every scene, one launch per kernel."""
+        import ctypes
+
+        from . import _lib
+        from .bind import stream_handle
+        _lib.check(_lib.lib().mpmw_batch_run_substeps(ctypes.byref(self.P), int(k), self.status.data_ptr(),
+                                                      self.ws.data_ptr(), self.ws.numel(),
+                                                      stream_handle(torch.cuda.current_stream(self.device))),
+                   "batch_run_substeps")
+
+    def capture(self, k: int):
+        """Capture one batch step of k substeps into a CUDA graph.  The eager
+        warm-up needed before capture advances every scene by k."""
+        self.step(k)
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        cap = torch.cuda.Stream(device=self.device)
+        cap.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.graph(g, stream=cap):
+            self.step(k)
+        self.graph, self.graph_steps = g, k
+        return g
+
+    def replay(self):
+        self.graph.replay()
+
+    def scene_field(self, i: int, name: str):
+        """Scene i's part of a concatenated field (a view): columns of a SoA
+        field, rows (particle, k) of an AoS one."""
+        t = self.fields[name]
+        o, c = self.offsets[i], self.counts[i]
+        k = self._aos[name]
+        return t.view(-1, k)[o:o + c] if k else t[..., o:o + c]
+
+    def sync_scenes(self):
+        """Copy every scene's particle state back into its state objects."""
+        from .bind import particle_storage
+        for i, st in enumerate(self.states):
+            for name, dst in particle_storage(*st).items():
+                if dst is not None:
+                    src = self.scene_field(i, name)
+                    dst.copy_(src.reshape(dst.shape) if self._aos[name] else src)
+
+    def results(self):
+        out = []
+        for i, c in enumerate(self.counts):
+            act = self.scene_field(i, "active") == 1
+            v = self.scene_field(i, "v")            # (3, n)
+            m = self.scene_field(i, "mass")
+            d = self.scene_field(i, "damage")
+            mom = (m[None, :] * v).sum(1).double().cpu().tolist()
+            out.append(SceneResult(i, c, int(act.sum().item()),
+                                   float(d[act].double().mean().item()) if act.any() else 0.0,
                                    tuple(mom), float(v.abs().max().item())))
         return out
 

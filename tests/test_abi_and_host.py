@@ -125,3 +125,48 @@ def test_block_sort_key_groups_blocks():
     k = block_sort_key(x, (0, 0, 0), 1.0, (8, 8, 8))
     # particles 0 and 2 share block (0,0,0); particle 3 is in block (0,0,1); particle 1 in block (1,0,0)
     assert k[0] // 64 == k[2] // 64 and k[0] < k[2] < k[3] < k[1]
+
+
+def test_batch_arguments_are_checked_before_any_device_work():
+    """mpmw_batch_prepare rejects a bad scene table with MPMW_E_ARG (and a short
+    workspace with MPMW_E_WORKSPACE) before it touches a device, and
+    mpmw_batch_run_substeps refuses a workspace that was never prepared: the
+    pointers below are host addresses that no kernel ever sees."""
+    from mpmwarpydw_b200 import _lib
+    L = _lib.lib()
+    buf = (ctypes.c_float * 128)()
+    addr = ctypes.addressof(buf) + (-ctypes.addressof(buf)) % 256  # 256-byte aligned host address
+    P = _lib.Particles(); P.n = 512
+    for f in ("x", "v", "C", "F", "F_trial", "stress", "vol", "mass", "density", "mu", "lam", "ys", "alpha",
+              "hardening", "softening", "strain_criteria", "eta_shear", "eta_bulk", "acc_strain", "damage",
+              "active", "material", "x_pc", "v_pc"):
+        setattr(P, f, addr)
+    grids = (_lib.Grid * 2)()
+    prms = (_lib.Params * 2)()
+    for g in grids:
+        g.dims[0] = g.dims[1] = g.dims[2] = 4
+        g.mv = g.v = addr
+    for p in prms:
+        p.boundary_condition = -1
+
+    def prepare(offsets, nscenes=2, ws=None, ws_bytes=0):
+        offs = (ctypes.c_int64 * len(offsets))(*offsets)
+        return L.mpmw_batch_prepare(ctypes.byref(P), grids, prms, offs, nscenes, ws, ws_bytes, None)
+
+    need = L.mpmw_batch_workspace_bytes(grids, 2, 512)
+    assert need > L.mpmw_workspace_bytes(512)  # worklist plus the scene table
+    assert prepare([0, 100, 512]) == 1 and b"multiples of 256" in L.mpmw_last_error()
+    assert prepare([0, 256, 500]) == 1 and b"particle count" in L.mpmw_last_error()
+    assert prepare([0, 512, 512]) == 1 and b"increase" in L.mpmw_last_error()
+    assert prepare([0], nscenes=0) == 1 and b"scenes" in L.mpmw_last_error()
+    prms[1].vlc = 1
+    assert prepare([0, 256, 512]) == 1 and b"locking" in L.mpmw_last_error()
+    prms[1].vlc = 0
+    assert prepare([0, 256, 512]) == 4 and b"workspace" in L.mpmw_last_error()
+    assert prepare([0, 256, 512], ws=addr + 16, ws_bytes=need) == 1 and b"aligned" in L.mpmw_last_error()
+    assert prepare([0, 256, 512], ws=addr, ws_bytes=need - 256) == 4 and b"workspace" in L.mpmw_last_error()
+    grids[1].dims[2] = 0
+    assert prepare([0, 256, 512]) == 1 and b"dims" in L.mpmw_last_error()
+    assert L.mpmw_batch_workspace_bytes(grids, 2, 512) == 0
+    rc = L.mpmw_batch_run_substeps(ctypes.byref(P), 3, None, addr, need, None)
+    assert rc == 1 and b"not prepared" in L.mpmw_last_error()

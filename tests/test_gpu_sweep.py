@@ -38,3 +38,40 @@ def test_batch_graph_equals_scenes_one_by_one():
             assert rel_err(a.cpu().numpy(), c.cpu().numpy()) <= 1e-5
     res = b.results()
     assert [r.particles for r in res] == [d.n for d in scenes]
+
+
+def test_concatenated_batch_equals_scenes_one_by_one():
+    """One launch per kernel over the concatenated scenes (mpmw_batch_run_substeps,
+    eager and graph-replayed) gives each scene the state of stepping it alone."""
+    import torch
+
+    from mpmwarpydw_b200 import domains
+    from mpmwarpydw_b200.engine import sort_particles
+    from mpmwarpydw_b200.sweep import ConcatBatch
+    from mpmwarpydw_b200.utils.simulationRoutines import run_mpm_substeps
+    scenes = _scenes()
+    b = ConcatBatch(scenes)
+    assert all(o % 256 == 0 for o in b.offsets) and b.offsets[-1] == b.total
+    b.step(4)             # eager
+    b.capture(3)          # eager warm-up (3 substeps) + capture
+    b.replay()            # 3 more: 10 in all
+    torch.cuda.synchronize()
+    from mpmwarpydw_b200.bind import read_status
+    assert read_status("cuda:0") == 0
+    b.sync_scenes()
+    for i, d in enumerate(scenes):
+        sim, mpm, xpbd = domains.build(d, device="cuda:0")
+        sort_particles(sim, mpm, xpbd)
+        for k in (4, 3, 3):
+            run_mpm_substeps(sim, mpm, xpbd, k)
+        torch.cuda.synchronize()
+        bs, bm, _ = b.states[i]
+        assert np.array_equal(sim.materialLabel.cpu().numpy(), bs.materialLabel.cpu().numpy())
+        for a, c in ((sim.particle_x, bs.particle_x), (sim.particle_v, bs.particle_v), (mpm.particle_F, bm.particle_F),
+                     (mpm.particle_C, bm.particle_C), (mpm.particle_stress, bm.particle_stress)):
+            assert rel_err(a.cpu().numpy(), c.cpu().numpy()) <= 1e-5
+        # the padding stays inactive and untouched
+        pad = b.fields["active"][b.offsets[i] + b.counts[i]:b.offsets[i + 1]]
+        assert int(pad.abs().sum().item()) == 0
+    res = b.results()
+    assert [r.particles for r in res] == [d.n for d in scenes]
