@@ -163,7 +163,7 @@ def test_batch_arguments_are_checked_before_any_device_work():
     assert prepare([0, 256, 512]) == 1 and b"locking" in L.mpmw_last_error()
     prms[1].vlc = 0
     assert prepare([0, 256, 512]) == 4 and b"workspace" in L.mpmw_last_error()
-    assert prepare([0, 256, 512], ws=addr + 16, ws_bytes=need) == 1 and b"aligned" in L.mpmw_last_error()
+    assert prepare([0, 256, 512], ws=addr + 4, ws_bytes=need) == 1 and b"aligned" in L.mpmw_last_error()
     assert prepare([0, 256, 512], ws=addr, ws_bytes=need - 256) == 4 and b"workspace" in L.mpmw_last_error()
     grids[1].dims[2] = 0
     assert prepare([0, 256, 512]) == 1 and b"dims" in L.mpmw_last_error()
