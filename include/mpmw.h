@@ -201,8 +201,8 @@ int mpmw_run_substeps(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpm
  * offsets[0] = 0 and offsets[nscenes] = p->n.  grids[s] and prms[s] are scene
  * s's grid and parameters; VLC must be off.
  *
- * Bytes of workspace for such a batch: the SVD worklist of
- * mpmw_workspace_bytes(n) plus the scene table. */
+ * Bytes of workspace for such a batch: the SVD worklist (n ints), a worklist
+ * count per scene and the scene table. */
 size_t mpmw_batch_workspace_bytes(const mpmw_grid_t *grids, int nscenes, int64_t n);
 /* Checks the batch (1 <= nscenes <= MPMW_BATCH_MAX_SCENES) and writes its scene
  * table (each scene's grid and parameters; each CTA's scene) into the
@@ -216,6 +216,12 @@ int mpmw_batch_prepare(const mpmw_particles_t *p, const mpmw_grid_t *grids, cons
  * synchronization (capturable in a CUDA graph). */
 int mpmw_batch_run_substeps(const mpmw_particles_t *p, int nsteps, uint32_t *status, void *workspace,
                             size_t ws_bytes, mpmw_stream_t stream);
+/* The same for the scenes [first_scene, last_scene) of the prepared batch.
+ * Disjoint ranges use disjoint particles, grids and worklists, so they may run
+ * concurrently on different streams (how many ranges suits a batch best is
+ * measured by sweep.ConcatBatch.tune). */
+int mpmw_batch_run_range(const mpmw_particles_t *p, int first_scene, int last_scene, int nsteps, uint32_t *status,
+                         void *workspace, size_t ws_bytes, mpmw_stream_t stream);
 
 /* utils/mpmRoutines.py:1446-1475 deactivate_and_teleport_xpbd_below_datum */
 int mpmw_teleport(const mpmw_particles_t *p, float z_datum, float teleport_distance, mpmw_stream_t stream);

@@ -106,6 +106,7 @@ _SIGS = {
     "mpmw_batch_prepare": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params),
                                 ctypes.POINTER(_I64), _I, _P, ctypes.c_size_t, _P]),
     "mpmw_batch_run_substeps": (_I, [ctypes.POINTER(Particles), _I, _P, _P, ctypes.c_size_t, _P]),
+    "mpmw_batch_run_range": (_I, [ctypes.POINTER(Particles), _I, _I, _I, _P, _P, ctypes.c_size_t, _P]),
     "mpmw_teleport": (_I, [ctypes.POINTER(Particles), _F, _F, _P]),
     "mpmw_creep": (_I, [ctypes.POINTER(Particles), _P, _F, _F, _F, _F, _P]),
     "mpmw_stats": (_I, [ctypes.POINTER(Particles), _P, _P]),

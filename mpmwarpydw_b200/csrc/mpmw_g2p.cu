@@ -664,6 +664,8 @@ struct BatchRef {  // kernel argument: pointers into the prepared workspace
     const int *pcta_scene;  // particle CTA -> scene
     const int *ncta_scene;  // grid-node CTA -> scene
     const int *ncta_first;  // scene -> its first grid-node CTA
+    int pcta_base;          // this launch covers particle CTAs pcta_base + blockIdx.x (a range of scenes)
+    int ncta_base;          // ... and grid-node CTAs ncta_base + blockIdx.x
     int use_tma;
 };
 
@@ -671,7 +673,7 @@ struct BatchRef {  // kernel argument: pointers into the prepared workspace
 // scene's record copied into `rec` (published by the barrier).
 __device__ __forceinline__ int stage_scene(const BatchRef &R, BatchScene &rec)
 {
-    const int s = R.pcta_scene[blockIdx.x];
+    const int s = R.pcta_scene[R.pcta_base + blockIdx.x];
     constexpr int kWords = (int)(sizeof(BatchScene) / 4);
     if (threadIdx.x < kWords)
         reinterpret_cast<uint32_t *>(&rec)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&R.scene[s])[threadIdx.x];
@@ -687,10 +689,11 @@ constexpr int kBatchNodesPerCta = kBlock * kBatchNodesPerThread;
 
 __global__ void __launch_bounds__(kBlock) k_zero_grid_batch(const BatchRef R)
 {
-    const int s = R.ncta_scene[blockIdx.x];
+    const int b = R.ncta_base + blockIdx.x;
+    const int s = R.ncta_scene[b];
     const mpmw_grid_t G = R.scene[s].grid;
     const int64_t total = (int64_t)G.dims[0] * G.dims[1] * G.dims[2];
-    const int64_t g0 = (int64_t)(blockIdx.x - R.ncta_first[s]) * kBatchNodesPerCta + threadIdx.x;
+    const int64_t g0 = (int64_t)(b - R.ncta_first[s]) * kBatchNodesPerCta + threadIdx.x;
 #pragma unroll
     for (int u = 0; u < kBatchNodesPerThread; ++u) {
         const int64_t g = g0 + (int64_t)u * kBlock;
@@ -700,11 +703,25 @@ __global__ void __launch_bounds__(kBlock) k_zero_grid_batch(const BatchRef R)
 
 __global__ void __launch_bounds__(kBlock) k_grid_update_batch(const BatchRef R, int zero_mv)
 {
-    const int s = R.ncta_scene[blockIdx.x];
+    const int b = R.ncta_base + blockIdx.x;
+    const int s = R.ncta_scene[b];
     const BatchScene B = R.scene[s];
-    const int64_t g0 = (int64_t)(blockIdx.x - R.ncta_first[s]) * kBatchNodesPerCta + threadIdx.x;
-#pragma unroll 2
-    for (int u = 0; u < kBatchNodesPerThread; ++u) grid_update_node(B.grid, B.prm, zero_mv, g0 + (int64_t)u * kBlock);
+    const int64_t g0 = (int64_t)(b - R.ncta_first[s]) * kBatchNodesPerCta + threadIdx.x;
+    const int64_t total = (int64_t)B.grid.dims[0] * B.grid.dims[1] * B.grid.dims[2];
+    // every node's accumulators are loaded before any store: the stores go
+    // through pointers the compiler cannot tell apart from the loads, so
+    // interleaving them would pay one memory latency per node
+    float4 a[kBatchNodesPerThread];
+#pragma unroll
+    for (int u = 0; u < kBatchNodesPerThread; ++u) {
+        const int64_t g = g0 + (int64_t)u * kBlock;
+        a[u] = g < total ? reinterpret_cast<const float4 *>(B.grid.mv)[g] : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < kBatchNodesPerThread; ++u) {
+        const int64_t g = g0 + (int64_t)u * kBlock;
+        if (g < total) grid_update_apply(B.grid, B.prm, zero_mv, g, a[u]);
+    }
 }
 
 __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_stress_p2g_batch(
@@ -712,7 +729,8 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_stress_p2g
 {
     __shared__ BatchScene B;
     stage_scene(R, B);
-    stress_p2g_body(P, B.grid, B.prm, status, svd_list, svd_count, (int64_t)blockIdx.x * kScatterChunk);
+    stress_p2g_body(P, B.grid, B.prm, status, svd_list, svd_count,
+                    (int64_t)(R.pcta_base + blockIdx.x) * kScatterChunk);
 }
 
 template <bool StoreStress>
@@ -723,7 +741,7 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g_batc
     __shared__ BatchScene B;
     const int s = stage_scene(R, B);
     g2p2g_body<StoreStress>(P, B.grid, B.prm, status, svd_list, svd_count, &M.tmap[s], R.use_tma, use_ahead,
-                            (int64_t)blockIdx.x * kScatterChunk);
+                            (int64_t)(R.pcta_base + blockIdx.x) * kScatterChunk);
 }
 
 __global__ void __launch_bounds__(kBlock, 3) k_g2p_batch(mpmw_particles_t P, const BatchRef R,
@@ -734,7 +752,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_g2p_batch(mpmw_particles_t P, con
     __shared__ BatchScene B;
     const int s = stage_scene(R, B);
     g2p_body<false>(P, B.grid, B.prm, status, nullptr, nullptr, &M.tmap[s], R.use_tma, use_ahead,
-                    (int64_t)blockIdx.x * kBlock);
+                    (int64_t)(R.pcta_base + blockIdx.x) * kBlock);
 }
 
 __global__ void __launch_bounds__(kBlock) k_stress_p2g_list_batch(mpmw_particles_t P, const BatchRef R,
@@ -752,16 +770,20 @@ __global__ void __launch_bounds__(kBlock) k_stress_p2g_list_batch(mpmw_particles
 }
 
 namespace {
-// Workspace layout of a batch: SVD worklist count (256 B) and list (n ints),
-// then the scene records, then the three CTA tables.
+// Workspace layout of a batch: the SVD worklist (n ints; a range of scenes
+// lists its particles in its own part, from the range's first particle on),
+// one worklist count per scene (a range uses its first scene's), the scene
+// records, then the three CTA tables.
 struct BatchLayout {
-    size_t scenes, pcta, ncta, nfirst, total;
+    size_t list, counts, scenes, pcta, ncta, nfirst, total;
 };
 size_t round256(size_t b) { return (b + 255) / 256 * 256; }
 BatchLayout batch_layout(int64_t n, int nscenes, int64_t nctas)
 {
     BatchLayout L;
-    L.scenes = g2p_workspace_bytes(n);
+    L.list = 0;
+    L.counts = round256((size_t)n * sizeof(int));
+    L.scenes = L.counts + round256((size_t)nscenes * sizeof(int));
     L.pcta = L.scenes + round256((size_t)nscenes * sizeof(BatchScene));
     L.ncta = L.pcta + round256((size_t)(n / kScatterChunk) * sizeof(int));
     L.nfirst = L.ncta + round256((size_t)nctas * sizeof(int));
@@ -784,6 +806,7 @@ struct BatchPrepared {
     int nscenes, pctas, nctas, use_tma, use_ahead, use_ahead_g2p;
     BatchLayout L;
     std::shared_ptr<BatchMaps> maps;
+    std::vector<int> pfirst, nfirst;  // first particle / grid-node CTA of each scene (+ the totals)
 };
 std::mutex g_batch_mu;
 std::unordered_map<const void *, BatchPrepared> g_batches;
@@ -846,6 +869,9 @@ int prepare_batch(const mpmw_particles_t &p, const mpmw_grid_t *grids, const mpm
     bp.use_ahead_g2p = p.F && p.n % 4 == 0 && (reinterpret_cast<uintptr_t>(p.F) & 15u) == 0 ? 1 : 0;
     bp.L = L;
     bp.maps = maps;
+    bp.pfirst.resize(nscenes + 1);
+    bp.nfirst.assign(nfirst, nfirst + nscenes + 1);
+    for (int k = 0; k <= nscenes; ++k) bp.pfirst[k] = (int)(offsets[k] / kScatterChunk);
     std::lock_guard<std::mutex> lk(g_batch_mu);
     if (g_batches.size() > 256) g_batches.clear();
     g_batches[ws] = bp;
@@ -854,10 +880,12 @@ int prepare_batch(const mpmw_particles_t &p, const mpmw_grid_t *grids, const mpm
 
 static bool g_batch_attr[64];
 
-// The fused schedule of mpmw_run_substeps over every scene of a batch that
-// prepare_batch wrote into this workspace.
-int launch_batch_substeps(const mpmw_particles_t &p, int nsteps, uint32_t *st, void *ws, size_t ws_bytes,
-                          cudaStream_t s)
+// The fused schedule of mpmw_run_substeps over the scenes [first, last) of a
+// batch that prepare_batch wrote into this workspace (last < 0: to the end).
+// Disjoint scene ranges touch disjoint particles, grids and worklists, so they
+// may run concurrently on different streams.
+int launch_batch_substeps(const mpmw_particles_t &p, int first, int last, int nsteps, uint32_t *st, void *ws,
+                          size_t ws_bytes, cudaStream_t s)
 {
     BatchPrepared bp;
     {
@@ -868,6 +896,11 @@ int launch_batch_substeps(const mpmw_particles_t &p, int nsteps, uint32_t *st, v
     }
     if (bp.n != p.n || ws_bytes < bp.L.total) {
         set_error("batch: the workspace was prepared for %lld particles in %zu bytes", (long long)bp.n, bp.L.total);
+        return MPMW_E_ARG;
+    }
+    if (last < 0) last = bp.nscenes;
+    if (first < 0 || first >= last || last > bp.nscenes) {
+        set_error("batch: scene range [%d, %d) outside the %d prepared scenes", first, last, bp.nscenes);
         return MPMW_E_ARG;
     }
     if (nsteps == 0 || p.n == 0) return MPMW_OK;
@@ -890,10 +923,13 @@ int launch_batch_substeps(const mpmw_particles_t &p, int nsteps, uint32_t *st, v
     R.pcta_scene = reinterpret_cast<const int *>(base + bp.L.pcta);
     R.ncta_scene = reinterpret_cast<const int *>(base + bp.L.ncta);
     R.ncta_first = reinterpret_cast<const int *>(base + bp.L.nfirst);
+    R.pcta_base = bp.pfirst[first];
+    R.ncta_base = bp.nfirst[first];
     R.use_tma = bp.use_tma;
-    int *count = static_cast<int *>(ws);
-    int *list = reinterpret_cast<int *>(base + 256);
-    const unsigned pctas = (unsigned)bp.pctas, nctas = (unsigned)bp.nctas;
+    int *count = reinterpret_cast<int *>(base + bp.L.counts) + first;
+    int *list = reinterpret_cast<int *>(base + bp.L.list) + (int64_t)bp.pfirst[first] * kScatterChunk;
+    const unsigned pctas = (unsigned)(bp.pfirst[last] - bp.pfirst[first]);
+    const unsigned nctas = (unsigned)(bp.nfirst[last] - bp.nfirst[first]);
     auto reset_count = [&]() -> int {
         if (cudaMemsetAsync(count, 0, sizeof(int), s) != cudaSuccess) { set_error("batch: memset failed"); return MPMW_E_DEVICE; }
         return MPMW_OK;

@@ -84,15 +84,13 @@ __device__ __forceinline__ void apply_bc(int bc, const int *idx, const int *dim,
     }
 }
 
-// One node g of the grid update (g beyond the grid returns).  zero_mv: also
-// clear the accumulators after reading them (for the fused G2P->P2G kernel,
-// which scatters the next substep into them).
-__device__ __forceinline__ void grid_update_node(const mpmw_grid_t &G, const mpmw_params_t &prm, int zero_mv, int64_t g)
+// The grid update of node g (inside the grid) whose accumulators (m, m v)
+// were read as `a`.  zero_mv: also clear the accumulators (for the fused
+// G2P->P2G kernel, which scatters the next substep into them).
+__device__ __forceinline__ void grid_update_apply(const mpmw_grid_t &G, const mpmw_params_t &prm, int zero_mv,
+                                                  int64_t g, const float4 a)
 {
-    const int nx = G.dims[0], ny = G.dims[1], nz = G.dims[2];
-    const int64_t total = (int64_t)nx * ny * nz;
-    if (g >= total) return;
-    const float4 a = reinterpret_cast<const float4 *>(G.mv)[g];
+    const int ny = G.dims[1], nz = G.dims[2];
     if (zero_mv) reinterpret_cast<float4 *>(G.mv)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
     float o[3] = {0.f, 0.f, 0.f};
     if (a.x > 1e-15f) {
@@ -112,12 +110,19 @@ __device__ __forceinline__ void grid_update_node(const mpmw_grid_t &G, const mpm
         const int gi = (int)g;
         const int iz = gi % nz, r = gi / nz;
         const int iy = r % ny, ix = r / ny;
-        int idx[3] = {ix, iy, iz}, dim[3] = {nx, ny, nz};
+        int idx[3] = {ix, iy, iz}, dim[3] = {G.dims[0], ny, nz};
         float gm = fabsf(prm.gravity[2]);
         apply_bc(prm.boundary_condition, idx, dim, o, prm.bound_friction, prm.bound_restitution, prm.dt, gm,
                  prm.boundary_padding);
     }
     reinterpret_cast<float4 *>(G.v)[g] = make_float4(o[0], o[1], o[2], 0.f);
+}
+
+// One node g of the grid update (g beyond the grid returns).
+__device__ __forceinline__ void grid_update_node(const mpmw_grid_t &G, const mpmw_params_t &prm, int zero_mv, int64_t g)
+{
+    if (g >= (int64_t)G.dims[0] * G.dims[1] * G.dims[2]) return;
+    grid_update_apply(G, prm, zero_mv, g, reinterpret_cast<const float4 *>(G.mv)[g]);
 }
 
 }  // namespace mpmw

@@ -551,7 +551,17 @@ int mpmw_batch_run_substeps(const mpmw_particles_t *p, int nsteps, uint32_t *sta
     MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV | kNeedCF | kNeedStress));
     if (nsteps < 0) { set_error("nsteps must be >= 0"); return MPMW_E_ARG; }
     if (!workspace) { set_error("batch: workspace is NULL"); return MPMW_E_WORKSPACE; }
-    return launch_batch_substeps(*p, nsteps, status, workspace, ws_bytes, as_stream(stream));
+    return launch_batch_substeps(*p, 0, -1, nsteps, status, workspace, ws_bytes, as_stream(stream));
+}
+
+int mpmw_batch_run_range(const mpmw_particles_t *p, int first_scene, int last_scene, int nsteps, uint32_t *status,
+                         void *workspace, size_t ws_bytes, mpmw_stream_t stream)
+{
+    MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV | kNeedCF | kNeedStress));
+    if (nsteps < 0) { set_error("nsteps must be >= 0"); return MPMW_E_ARG; }
+    if (!workspace) { set_error("batch: workspace is NULL"); return MPMW_E_WORKSPACE; }
+    return launch_batch_substeps(*p, first_scene, last_scene, nsteps, status, workspace, ws_bytes,
+                                 as_stream(stream));
 }
 
 int mpmw_teleport(const mpmw_particles_t *p, float z_datum, float teleport_distance, mpmw_stream_t stream)

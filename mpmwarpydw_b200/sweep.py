@@ -115,6 +115,24 @@ class SceneBatch:
 
 
 _CHUNK = 256  # particles per CTA: scene offsets are multiples of this
+_TUNED = {}   # (scenes, log2 particles) -> group count chosen by ConcatBatch.tune
+
+
+def scene_groups(counts, groups: int):
+    """Split scenes 0..len(counts)-1 into ``groups`` contiguous ranges of
+    roughly equal particle count: a list of (first, last) pairs."""
+    n = len(counts)
+    groups = max(1, min(int(groups), n))
+    total = float(sum(counts))
+    out, first, acc = [], 0, 0
+    for i, c in enumerate(counts):
+        acc += c
+        left_scenes, left_groups = n - i - 1, groups - len(out) - 1
+        if left_groups > 0 and (acc >= total * (len(out) + 1) / groups or left_scenes == left_groups):
+            out.append((first, i + 1))
+            first = i + 1
+    out.append((first, n))
+    return out
 
 
 class ConcatBatch:
@@ -182,6 +200,9 @@ class ConcatBatch:
         self.status = status_word(self.device)
         self.graph = None
         self.graph_steps = 0
+        self.groups = 1
+        self.tuning = {}
+        self._streams = []
         self.prepare()
         torch.cuda.synchronize(self.device)
 
@@ -201,16 +222,56 @@ class ConcatBatch:
     def particles(self):
         return sum(self.counts)
 
-    def step(self, k: int):
-        """k substeps of every scene, one launch per kernel."""
+    def step(self, k: int, groups=None):
+        """k substeps of every scene.  The scenes run as ``groups`` contiguous
+        ranges (default: ``self.groups``), each range one launch per kernel
+        on its own stream; 1 group is a single launch per kernel."""
         import ctypes
 
         from . import _lib
         from .bind import stream_handle
-        _lib.check(_lib.lib().mpmw_batch_run_substeps(ctypes.byref(self.P), int(k), self.status.data_ptr(),
-                                                      self.ws.data_ptr(), self.ws.numel(),
-                                                      stream_handle(torch.cuda.current_stream(self.device))),
-                   "batch_run_substeps")
+        L = _lib.lib()
+        ranges = scene_groups(self.counts, self.groups if groups is None else groups)
+        cur = torch.cuda.current_stream(self.device)
+        if len(ranges) == 1:
+            _lib.check(L.mpmw_batch_run_substeps(ctypes.byref(self.P), int(k), self.status.data_ptr(),
+                                                 self.ws.data_ptr(), self.ws.numel(), stream_handle(cur)),
+                       "batch_run_substeps")
+            return
+        while len(self._streams) < len(ranges):
+            self._streams.append(torch.cuda.Stream(device=self.device))
+        for (a, b), st in zip(ranges, self._streams):
+            st.wait_stream(cur)
+            _lib.check(L.mpmw_batch_run_range(ctypes.byref(self.P), a, b, int(k), self.status.data_ptr(),
+                                              self.ws.data_ptr(), self.ws.numel(), stream_handle(st)),
+                       "batch_run_range")
+        for st in self._streams[:len(ranges)]:
+            cur.wait_stream(st)
+
+    def tune(self, k: int = 5, candidates=None, reuse: bool = True):
+        """Pick the number of scene groups (streams) that steps this batch
+        fastest: each candidate runs k substeps to warm up and k timed (so the
+        tuning advances every scene by 2 k substeps per candidate).  The choice
+        is kept in ``self.groups`` and, per batch shape, for later batches."""
+        import math
+        key = (len(self.counts), int(round(math.log2(max(1, self.particles)))))
+        if reuse and key in _TUNED:
+            self.groups = _TUNED[key]
+            return self.groups
+        n = len(self.counts)
+        cands = sorted({c for c in (candidates or (1, 2, 4, 8, 16, 32, n)) if 1 <= c <= n})
+        for g in cands:
+            self.step(k, g)
+            torch.cuda.synchronize(self.device)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            self.step(k, g)
+            e1.record()
+            torch.cuda.synchronize(self.device)
+            self.tuning[g] = self.particles * k / (e0.elapsed_time(e1) * 1e-3)
+        self.groups = max(self.tuning, key=self.tuning.get)
+        _TUNED[key] = self.groups
+        return self.groups
 
     def capture(self, k: int):
         """Capture one batch step of k substeps into a CUDA graph.  The eager
@@ -265,8 +326,9 @@ def run_sharded(scenes, steps: int, chunk: int = 50, device=None, group=None, ru
     SceneResult in scene order, other ranks return None.
 
     ``runner(my_scenes, steps, chunk, device) -> list[SceneResult]`` runs one
-    rank's share (default: a SceneBatch replaying a captured graph of ``chunk``
-    substeps); the result indices are the positions within ``my_scenes``."""
+    rank's share (default: a tuned ConcatBatch replaying a captured graph of
+    ``chunk`` substeps); the result indices are the positions within
+    ``my_scenes``."""
     import torch.distributed as dist
     world = dist.get_world_size(group) if dist.is_initialized() else 1
     rank = dist.get_rank(group) if dist.is_initialized() else 0
@@ -286,15 +348,19 @@ def run_sharded(scenes, steps: int, chunk: int = 50, device=None, group=None, ru
     return sorted(allr, key=lambda r: r.index)
 
 
-def _run_batch(scenes, steps, chunk, device):
+def _run_batch(scenes, steps, chunk, device, tune_k: int = 5):
     if not scenes:
         return []
     dev = device or torch.device("cuda", torch.cuda.current_device())
-    b = SceneBatch(scenes, device=dev)
+    b = ConcatBatch(scenes, device=dev)
     done = 0
-    if steps >= 2 * chunk:
+    n_cands = len({c for c in (1, 2, 4, 8, 16, 32, len(scenes)) if 1 <= c <= len(scenes)})
+    if steps >= 2 * tune_k * n_cands + 2 * chunk:
+        b.tune(tune_k, reuse=False)
+        done = 2 * tune_k * len(b.tuning)
+    if steps - done >= 2 * chunk:
         b.capture(chunk)
-        done = chunk
+        done += chunk
         while done + chunk <= steps:
             b.replay()
             done += chunk

@@ -170,3 +170,21 @@ def test_batch_arguments_are_checked_before_any_device_work():
     assert L.mpmw_batch_workspace_bytes(grids, 2, 512) == 0
     rc = L.mpmw_batch_run_substeps(ctypes.byref(P), 3, None, addr, need, None)
     assert rc == 1 and b"not prepared" in L.mpmw_last_error()
+
+
+def test_scene_groups_are_contiguous_balanced_and_never_empty():
+    """The batch's scene ranges (one stream each) cover every scene once, in
+    order, with min(groups, scenes) non-empty ranges of similar particle count."""
+    import random
+
+    from mpmwarpydw_b200.sweep import scene_groups
+    rng = random.Random(5)
+    for _ in range(200):
+        counts = [rng.randint(1, 1000) for _ in range(rng.randint(1, 40))]
+        g = rng.randint(1, 50)
+        r = scene_groups(counts, g)
+        assert len(r) == min(g, len(counts))
+        assert r[0][0] == 0 and r[-1][1] == len(counts)
+        assert all(a < b for a, b in r) and all(r[i][1] == r[i + 1][0] for i in range(len(r) - 1))
+    # equal scenes split evenly
+    assert scene_groups([10] * 8, 4) == [(0, 2), (2, 4), (4, 6), (6, 8)]

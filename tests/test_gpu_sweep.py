@@ -52,7 +52,8 @@ def test_concatenated_batch_equals_scenes_one_by_one():
     scenes = _scenes()
     b = ConcatBatch(scenes)
     assert all(o % 256 == 0 for o in b.offsets) and b.offsets[-1] == b.total
-    b.step(4)             # eager
+    b.step(4)             # eager, one launch per kernel
+    b.groups = 2          # two scene ranges on two streams from here on
     b.capture(3)          # eager warm-up (3 substeps) + capture
     b.replay()            # 3 more: 10 in all
     torch.cuda.synchronize()
