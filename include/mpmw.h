@@ -235,6 +235,44 @@ int mpmw_creep(const mpmw_particles_t *p, const float *ys_base, float dt, float 
  * active MPM, active XPBD, inactive MPM, inactive XPBD (countParticlesByType). */
 int mpmw_stats(const mpmw_particles_t *p, double *out, mpmw_stream_t stream);
 
+/* ---- phase-1 loop on the device (runMPMYDW.py:656-727) ------------------ */
+/* The reference driver runs substeps while counter < nSteps and (counter <
+ * minSteps or residual > residualThreshold), ending early when the mean
+ * damage stalls, and reads the residual back to the host every substep.  A
+ * loop object runs that test on the device: one CUDA graph whose while-node
+ * body is `chunk` fused substeps (mpmw_run_substeps), the statistics
+ * (mpmw_stats) and a decision kernel, so a launch runs chunk after chunk with
+ * no host round trip until the phase ends or `segment_left` runs out.  The
+ * decision is the driver's check made every `chunk` substeps, in double
+ * precision: counter += chunk; residual = sum|v|/r / active; the damage
+ * stall counter grows by chunk when mean damage rose by less than
+ * stall_threshold * chunk and counter > min_steps, else resets; the phase
+ * ends early when stall >= stall_steps and counter > min_steps. */
+typedef struct mpmw_loop_state { /* device memory, 8-byte aligned */
+    int counter;       /* substeps run in the phase */
+    int stall;         /* substeps of stalled damage */
+    int stopped_early; /* 1 once the damage stall ended the phase */
+    int segment_left;  /* substeps this launch may still run (set by the caller, multiple of chunk) */
+    double residual;   /* sum |v|/r / active at the last check (1e10 before any) */
+    double prev_damage;/* mean damage over active at the last check */
+    double stats[7];   /* mpmw_stats of the last check */
+} mpmw_loop_state_t;
+typedef struct mpmw_loop_params {
+    int chunk, n_steps, min_steps, stall_steps;
+    double residual_threshold, stall_threshold;
+} mpmw_loop_params_t;
+typedef struct mpmw_loop mpmw_loop_t;
+/* Builds the graph on `stream` (captured, nothing runs).  The structs, the
+ * workspace (mpmw_workspace_bytes(n)) and `state` are baked in: keep them alive
+ * and unchanged while the loop exists. */
+int mpmw_loop_create(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm,
+                     const mpmw_loop_params_t *lp, mpmw_loop_state_t *state, uint32_t *status, void *workspace,
+                     size_t ws_bytes, mpmw_loop_t **out, mpmw_stream_t stream);
+/* Runs chunks while the phase continues and state->segment_left >= chunk (at
+ * least one chunk: launch only when that holds). */
+int mpmw_loop_launch(mpmw_loop_t *loop, mpmw_stream_t stream);
+void mpmw_loop_destroy(mpmw_loop_t *loop);
+
 #ifdef __cplusplus
 }
 #endif

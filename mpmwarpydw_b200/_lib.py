@@ -80,6 +80,20 @@ class XPBDParams(ctypes.Structure):
 XK = dict(INTEGRATE=0, RESET_LABELS=1, BOUND=2, PARTICLE=3, APPLY=4, SLEEP=5, IMPULSES=6, SWELL=7)
 
 
+class LoopState(ctypes.Structure):
+    """mpmw_loop_state_t (include/mpmw.h)."""
+    _fields_ = [("counter", ctypes.c_int), ("stall", ctypes.c_int), ("stopped_early", ctypes.c_int),
+                ("segment_left", ctypes.c_int), ("residual", ctypes.c_double), ("prev_damage", ctypes.c_double),
+                ("stats", ctypes.c_double * 7)]
+
+
+class LoopParams(ctypes.Structure):
+    """mpmw_loop_params_t (include/mpmw.h)."""
+    _fields_ = [("chunk", ctypes.c_int), ("n_steps", ctypes.c_int), ("min_steps", ctypes.c_int),
+                ("stall_steps", ctypes.c_int), ("residual_threshold", ctypes.c_double),
+                ("stall_threshold", ctypes.c_double)]
+
+
 _SIGS = {
     "mpmw_last_error": (ctypes.c_char_p, []),
     "mpmw_version": (_I, []),
@@ -107,6 +121,11 @@ _SIGS = {
                                 ctypes.POINTER(_I64), _I, _P, ctypes.c_size_t, _P]),
     "mpmw_batch_run_substeps": (_I, [ctypes.POINTER(Particles), _I, _P, _P, ctypes.c_size_t, _P]),
     "mpmw_batch_run_range": (_I, [ctypes.POINTER(Particles), _I, _I, _I, _P, _P, ctypes.c_size_t, _P]),
+    "mpmw_loop_create": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params),
+                              ctypes.POINTER(LoopParams), _P, _P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p),
+                              _P]),
+    "mpmw_loop_launch": (_I, [_P, _P]),
+    "mpmw_loop_destroy": (None, [_P]),
     "mpmw_teleport": (_I, [ctypes.POINTER(Particles), _F, _F, _P]),
     "mpmw_creep": (_I, [ctypes.POINTER(Particles), _P, _F, _F, _F, _F, _P]),
     "mpmw_stats": (_I, [ctypes.POINTER(Particles), _P, _P]),

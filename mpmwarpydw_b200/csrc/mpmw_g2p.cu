@@ -557,6 +557,34 @@ int launch_g2p(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_param
 }
 
 static bool g_g2p2g_attr[64];
+static bool g_stress_p2g_attr[64];
+
+// Opts the fused kernels into their shared memory (once per device).  Also
+// called before a graph capture, so that no attribute call runs inside one.
+int reserve_fused_smem()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { set_error("no current device"); return MPMW_E_DEVICE; }
+    if (dev < 0 || dev >= 64) return MPMW_OK;
+    if (!g_g2p2g_attr[dev]) {
+        const int smem = (int)(sizeof(G2P2GShared) + 128);
+        if (cudaFuncSetAttribute(k_g2p2g<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+            cudaFuncSetAttribute(k_g2p2g<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) {
+            set_error("g2p2g: cannot reserve %d bytes of shared memory", smem);
+            return MPMW_E_DEVICE;
+        }
+        g_g2p2g_attr[dev] = true;
+    }
+    if (!g_stress_p2g_attr[dev]) {
+        const int smem = (int)sizeof(ScatterShared);
+        if (cudaFuncSetAttribute(k_stress_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) {
+            set_error("stress_p2g: cannot reserve %d bytes of shared memory", smem);
+            return MPMW_E_DEVICE;
+        }
+        g_stress_p2g_attr[dev] = true;
+    }
+    return MPMW_OK;
+}
 
 // the read-ahead bulk copies of k_g2p2g need every field's chunk start 16-byte aligned
 static bool g2p2g_ahead_ok(const mpmw_particles_t &p)
@@ -582,16 +610,7 @@ int launch_g2p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_par
         return MPMW_E_WORKSPACE;
     }
     const size_t smem = sizeof(G2P2GShared) + 128;  // + alignment slack (see k_g2p2g)
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) { set_error("g2p2g: no current device"); return MPMW_E_DEVICE; }
-    if (dev >= 0 && dev < 64 && !g_g2p2g_attr[dev]) {
-        if (cudaFuncSetAttribute(k_g2p2g<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-            cudaFuncSetAttribute(k_g2p2g<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
-            set_error("g2p2g: cannot reserve %zu bytes of shared memory", smem);
-            return MPMW_E_DEVICE;
-        }
-        g_g2p2g_attr[dev] = true;
-    }
+    if (const int rc_ = reserve_fused_smem()) return rc_;
     CUtensorMap map;
     int use_tma = cached_grid_map(g, &map) ? 1 : 0;
     if (!use_tma) memset(&map, 0, sizeof(map));
@@ -607,8 +626,6 @@ int launch_g2p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_par
     return check_launch("k_stress_p2g_list");
 }
 
-static bool g_stress_p2g_attr[64];
-
 int launch_stress_p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st,
                       void *ws, size_t ws_bytes, cudaStream_t s)
 {
@@ -619,15 +636,7 @@ int launch_stress_p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpm
         return MPMW_E_WORKSPACE;
     }
     const size_t smem = sizeof(ScatterShared);
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) { set_error("stress_p2g: no current device"); return MPMW_E_DEVICE; }
-    if (dev >= 0 && dev < 64 && !g_stress_p2g_attr[dev]) {
-        if (cudaFuncSetAttribute(k_stress_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
-            set_error("stress_p2g: cannot reserve %zu bytes of shared memory", smem);
-            return MPMW_E_DEVICE;
-        }
-        g_stress_p2g_attr[dev] = true;
-    }
+    if (const int rc_ = reserve_fused_smem()) return rc_;
     int *count = static_cast<int *>(ws);
     int *list = reinterpret_cast<int *>(static_cast<char *>(ws) + 256);
     if (cudaMemsetAsync(count, 0, sizeof(int), s) != cudaSuccess) { set_error("stress_p2g: memset failed"); return MPMW_E_DEVICE; }

@@ -147,3 +147,69 @@ class SubstepGraphCache:
             self._graphs.pop(next(iter(self._graphs)))  # oldest first
         # the capture's warm-up run is this call's k substeps
         self._graphs[key] = SubstepGraph(sim, mpm, xpbd, k, warmup=True)
+
+
+class DeviceLoop:
+    """Phase-1 substeps with the driver's stop test on the device
+    (runMPMYDW.py:656-727; ``mpmw_loop_*``).
+
+    One CUDA graph whose while node runs ``chunk`` fused substeps, the
+    statistics and the driver's check (residual, damage stall) until the phase
+    ends or the segment's substep budget runs out, with no host round trip in
+    between.  The graph bakes in the particle, grid and parameter structs: make
+    a new loop when a parameter (dt, gravity) changes."""
+
+    def __init__(self, sim, mpm, xpbd, chunk, n_steps, residual_threshold, stall_threshold, stall_steps, min_steps):
+        import ctypes
+        self.chunk = int(chunk)
+        self.P = particles_from_states(sim, mpm, xpbd)
+        self.G = grid_from_state(mpm)
+        self.prm = params_from_states(sim, mpm)
+        self.key = bytes(self.prm)
+        self.status = status_word(sim.device)
+        self.ws = workspace(mpm, sim.nPoints, sim.device)
+        self.state = torch.zeros(ctypes.sizeof(_lib.LoopState) // 8, dtype=torch.float64, device=sim.device)
+        self.lp = _lib.LoopParams(self.chunk, int(n_steps), int(min_steps), int(stall_steps),
+                                  float(residual_threshold), float(stall_threshold))
+        self.stream = torch.cuda.Stream(device=sim.device)
+        self.handle = ctypes.c_void_p()
+        _lib.check(_lib.lib().mpmw_loop_create(ctypes.byref(self.P), ctypes.byref(self.G), ctypes.byref(self.prm),
+                                               ctypes.byref(self.lp), self.state.data_ptr(), self.status.data_ptr(),
+                                               self.ws.data_ptr(), self.ws.numel(), ctypes.byref(self.handle),
+                                               stream_handle(self.stream)), "loop_create")
+
+    def _write(self, st):
+        self.state.copy_(torch.frombuffer(bytearray(bytes(st)), dtype=torch.float64))
+
+    def read(self):
+        """The loop state (an ``_lib.LoopState``) after the last launch."""
+        raw = self.state.cpu().numpy().tobytes()
+        return _lib.LoopState.from_buffer_copy(raw)
+
+    def run(self, counter, stall, residual, prev_damage, segment):
+        """Run chunks from the given monitor state for at most ``segment``
+        substeps (at least one chunk; segment is rounded down to whole
+        chunks); returns the state after the last chunk."""
+        segment = (int(segment) // self.chunk) * self.chunk
+        if segment < self.chunk:
+            raise ValueError("a device segment runs at least one chunk")
+        st = _lib.LoopState()
+        st.counter, st.stall, st.stopped_early, st.segment_left = int(counter), int(stall), 0, segment
+        st.residual, st.prev_damage = float(residual), float(prev_damage)
+        cur = torch.cuda.current_stream(self.state.device)
+        self._write(st)
+        self.stream.wait_stream(cur)
+        _lib.check(_lib.lib().mpmw_loop_launch(self.handle, stream_handle(self.stream)), "loop_launch")
+        cur.wait_stream(self.stream)
+        return self.read()
+
+    def close(self):
+        if self.handle:
+            _lib.lib().mpmw_loop_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

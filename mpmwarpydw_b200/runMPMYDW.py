@@ -45,7 +45,8 @@ import numpy as np
 import torch
 
 from . import domains as _domains
-from .engine import SubstepGraphCache, original_order, sort_particles
+from .bind import params_from_states
+from .engine import DeviceLoop, SubstepGraphCache, original_order, sort_particles
 from .scene import build_states
 from .utils import mpmRoutines
 from .utils import simulationRoutines as S
@@ -130,6 +131,22 @@ class PhaseOneMonitor:
         return True
 
 
+def device_segment(c, k, ratio, n_steps, pulse_steps=0):
+    """Substeps the device loop may run from counter c in whole chunks of k:
+    every chunk ends within n_steps and, while a gravity pulse of pulse_steps
+    substeps is on, by its end, and holds no XPBD substep (a positive multiple
+    of ratio), which the host runs with the chunk around it."""
+    n = 0
+    while True:
+        a = c + n
+        if a + k > n_steps or (pulse_steps and a < pulse_steps < a + k):
+            return n
+        first = max(ratio, ((a + ratio - 1) // ratio) * ratio)  # first positive multiple of ratio >= a
+        if first < a + k:
+            return n
+        n += k
+
+
 def _stats(sim, mpm):
     """(residual, mean damage over active, counts) from one device reduction."""
     s = S.step_stats(sim, mpm).cpu().numpy()
@@ -139,7 +156,7 @@ def _stats(sim, mpm):
     return float(residual), float(mean_damage), s
 
 
-def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=None):
+def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=None, device_loop=False):
     dev = torch.device(device)
     torch.cuda.set_device(dev)
     x, vol, props, overrides, dom = load_domain(args.domainFile, args)
@@ -155,6 +172,10 @@ def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=Non
         f"XPBD every {sim.mpmStepsPerXpbdStep} substeps")
     ratio = max(1, int(sim.mpmStepsPerXpbdStep))
     graphs = SubstepGraphCache()  # the runs of substeps between checks repeat: replay them
+    # the stop test on the device between host events (not while saving, which
+    # the host checks after every chunk)
+    use_loop = device_loop and not sim.saveFlag
+    loops = {}
     base_gravity = sim.gravity
     next_save = sim.t + args.render_interval
     start = time.time()
@@ -171,6 +192,30 @@ def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=Non
         mon.prev_damage = d0
         while mon.running():
             c = mon.counter
+            if use_loop:
+                seg = device_segment(c, check_interval, ratio, sim.nSteps, pulse_steps if pulsing else 0)
+                if seg >= check_interval:
+                    key = bytes(params_from_states(sim, mpm))
+                    loop = loops.get(key)
+                    if loop is None:
+                        loop = loops[key] = DeviceLoop(sim, mpm, xpbd, check_interval, sim.nSteps,
+                                                       sim.residualThreshold, sim.damage_stall_threshold,
+                                                       int(sim.damage_stall_duration / sim.dt), mon.min_steps)
+                    st = loop.run(c, mon.stall, mon.residual, mon.prev_damage, seg)
+                    sim.t += (st.counter - c) * sim.dt
+                    mon.counter, mon.stall, mon.residual, mon.prev_damage = st.counter, st.stall, st.residual, st.prev_damage
+                    if pulsing and mon.counter == pulse_steps:
+                        sim.gravity = base_gravity
+                    if st.stopped_early:
+                        mon.stopped_early = True
+                        log(f"    early termination: damage stalled for {sim.damage_stall_duration}s")
+                        break
+                    if mon.counter // 100 > c // 100:
+                        s7 = st.stats
+                        log(f"  big step {big + 1}, substep {mon.counter}, t {sim.t:.4f}s, residual {st.residual:.4e}, "
+                            f"mean damage {st.prev_damage:.6f}, MPM {int(s7[3])}+{int(s7[5])}, "
+                            f"XPBD {int(s7[4])}+{int(s7[6])}, wall {time.time() - start:.2f}s")
+                    continue
             # substeps up to the next check: stop at the pulse end and never skip past nSteps
             k = min(check_interval, sim.nSteps - c)
             if pulsing and c < pulse_steps:
@@ -221,6 +266,8 @@ def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=Non
                                                               2.0 * float(maxB[2] - minB[2]))
         if sim.saveFlag:
             saved.append(save_state(sim, mpm, xpbd, sim.outputFolder, big, mon.counter, checkpoint=True))
+    for loop in loops.values():
+        loop.close()
     torch.cuda.synchronize(dev)
     log(f"simulation complete in {time.time() - start:.2f}s")
     return sim, mpm, xpbd, saved
@@ -230,10 +277,12 @@ def main(argv=None):
     argv = sys.argv[1:] if argv is None else list(argv)
     extra = argparse.ArgumentParser(add_help=False)
     extra.add_argument("--check_interval", type=int, default=1)
+    extra.add_argument("--device_loop", action="store_true",
+                       help="run the checks between XPBD steps on the device (one host sync per segment)")
     extra.add_argument("--device", type=str, default="cuda:0")
     ex, rest = extra.parse_known_args(argv)
     args = get_args(rest)
-    run(args, check_interval=max(1, ex.check_interval), device=ex.device)
+    run(args, check_interval=max(1, ex.check_interval), device=ex.device, device_loop=ex.device_loop)
 
 
 if __name__ == "__main__":

@@ -188,3 +188,26 @@ def test_scene_groups_are_contiguous_balanced_and_never_empty():
         assert all(a < b for a, b in r) and all(r[i][1] == r[i + 1][0] for i in range(len(r) - 1))
     # equal scenes split evenly
     assert scene_groups([10] * 8, 4) == [(0, 2), (2, 4), (4, 6), (6, 8)]
+
+
+def test_device_segments_stop_before_host_events():
+    """The device loop runs whole chunks only: each ends within nSteps and by
+    the end of a gravity pulse, and none holds an XPBD substep (a positive
+    multiple of the XPBD ratio), which the host runs with its chunk."""
+    import random
+
+    from mpmwarpydw_b200.runMPMYDW import device_segment
+    rng = random.Random(3)
+    for _ in range(500):
+        c, k, ratio = rng.randint(0, 300), rng.randint(1, 12), rng.randint(1, 60)
+        n_steps, pulse = rng.randint(c, 400), rng.choice([0, rng.randint(1, 300)])
+        seg = device_segment(c, k, ratio, n_steps, pulse)
+        assert seg % k == 0 and c + seg <= n_steps
+        for a in range(c, c + seg, k):
+            assert not any(m % ratio == 0 for m in range(max(a, 1), a + k))
+            assert not (pulse and a < pulse < a + k)
+        # the next chunk is one the host must run (or there is none)
+        a = c + seg
+        nxt_ok = (a + k <= n_steps and not (pulse and a < pulse < a + k)
+                  and not any(m % ratio == 0 for m in range(max(a, 1), a + k)))
+        assert not nxt_ok
