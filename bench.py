@@ -34,6 +34,7 @@ sys.path.insert(0, ROOT)
 METRIC = "MPM particle-updates/s at 4M, learned vs plain return map at ≤1e-3 stress err"
 UNIT = "particle-updates/s"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
+HBM_NOMINAL_GBS = 7700.0  # B200 HBM3e, HGX nominal: fractions are also reported against it
 
 
 def load_peaks():
@@ -281,7 +282,8 @@ def run_ours(a):
                      "dram_GBps": (traffic / (dom_ms * 1e-3) / 1e9) if traffic else None,
                      "dram_frac": (traffic / (dom_ms * 1e-3) / 1e9 / hbm) if traffic else None,
                      "step_achieved_GBps": step_bytes / (ms / K * 1e-3) / 1e9,
-                     "step_frac": step_bytes / (ms / K * 1e-3) / 1e9 / hbm},
+                     "step_frac": step_bytes / (ms / K * 1e-3) / 1e9 / hbm,
+                     "nominal_GBps": HBM_NOMINAL_GBS, "frac_nominal": achieved / HBM_NOMINAL_GBS},
         "kernel_ms_per_step": {k: v / kb for k, v in per.items()},
         "e2e": e2e,
         "gpu_launches": launches[0],
