@@ -675,14 +675,17 @@ struct BatchRef {  // kernel argument: pointers into the prepared workspace
     const int *ncta_first;  // scene -> its first grid-node CTA
     int pcta_base;          // this launch covers particle CTAs pcta_base + blockIdx.x (a range of scenes)
     int ncta_base;          // ... and grid-node CTAs ncta_base + blockIdx.x
+    int nscenes;            // scene indices read from the table are checked against it
     int use_tma;
 };
 
 // Every thread of the CTA calls it: scene index of this particle CTA, and the
-// scene's record copied into `rec` (published by the barrier).
+// scene's record copied into `rec` (published by the barrier); -1 (for the
+// whole CTA, before any barrier) if the table holds no valid scene index.
 __device__ __forceinline__ int stage_scene(const BatchRef &R, BatchScene &rec)
 {
     const int s = R.pcta_scene[R.pcta_base + blockIdx.x];
+    if (s < 0 || s >= R.nscenes) return -1;  // uniform: every thread read the same entry
     constexpr int kWords = (int)(sizeof(BatchScene) / 4);
     if (threadIdx.x < kWords)
         reinterpret_cast<uint32_t *>(&rec)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&R.scene[s])[threadIdx.x];
@@ -700,6 +703,7 @@ __global__ void __launch_bounds__(kBlock) k_zero_grid_batch(const BatchRef R)
 {
     const int b = R.ncta_base + blockIdx.x;
     const int s = R.ncta_scene[b];
+    if (s < 0 || s >= R.nscenes) return;
     const mpmw_grid_t G = R.scene[s].grid;
     const int64_t total = (int64_t)G.dims[0] * G.dims[1] * G.dims[2];
     const int64_t g0 = (int64_t)(b - R.ncta_first[s]) * kBatchNodesPerCta + threadIdx.x;
@@ -714,6 +718,7 @@ __global__ void __launch_bounds__(kBlock) k_grid_update_batch(const BatchRef R, 
 {
     const int b = R.ncta_base + blockIdx.x;
     const int s = R.ncta_scene[b];
+    if (s < 0 || s >= R.nscenes) return;
     const BatchScene B = R.scene[s];
     const int64_t g0 = (int64_t)(b - R.ncta_first[s]) * kBatchNodesPerCta + threadIdx.x;
     const int64_t total = (int64_t)B.grid.dims[0] * B.grid.dims[1] * B.grid.dims[2];
@@ -737,7 +742,7 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_stress_p2g
     mpmw_particles_t P, const BatchRef R, uint32_t *status, int *svd_list, int *svd_count)
 {
     __shared__ BatchScene B;
-    stage_scene(R, B);
+    if (stage_scene(R, B) < 0) return;
     stress_p2g_body(P, B.grid, B.prm, status, svd_list, svd_count,
                     (int64_t)(R.pcta_base + blockIdx.x) * kScatterChunk);
 }
@@ -749,6 +754,7 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g_batc
 {
     __shared__ BatchScene B;
     const int s = stage_scene(R, B);
+    if (s < 0) return;
     g2p2g_body<StoreStress>(P, B.grid, B.prm, status, svd_list, svd_count, &M.tmap[s], R.use_tma, use_ahead,
                             (int64_t)(R.pcta_base + blockIdx.x) * kScatterChunk);
 }
@@ -760,6 +766,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_g2p_batch(mpmw_particles_t P, con
     static_assert(kBlock == kScatterChunk, "particle CTAs of the batched G2P and P2G kernels coincide");
     __shared__ BatchScene B;
     const int s = stage_scene(R, B);
+    if (s < 0) return;
     g2p_body<false>(P, B.grid, B.prm, status, nullptr, nullptr, &M.tmap[s], R.use_tma, use_ahead,
                     (int64_t)(R.pcta_base + blockIdx.x) * kBlock);
 }
@@ -772,7 +779,10 @@ __global__ void __launch_bounds__(kBlock) k_stress_p2g_list_batch(mpmw_particles
     uint32_t bad = 0;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += gridDim.x * blockDim.x) {
         const int64_t p = list[q];
-        const BatchScene &B = R.scene[R.pcta_scene[p / kScatterChunk]];
+        if (p < 0 || p >= P.n) continue;
+        const int s = R.pcta_scene[p / kScatterChunk];
+        if (s < 0 || s >= R.nscenes) continue;
+        const BatchScene &B = R.scene[s];
         stress_p2g_one(P, B.grid, B.prm, p, bad);
     }
     if (bad) raise_status(status, bad);
@@ -934,6 +944,7 @@ int launch_batch_substeps(const mpmw_particles_t &p, int first, int last, int ns
     R.ncta_first = reinterpret_cast<const int *>(base + bp.L.nfirst);
     R.pcta_base = bp.pfirst[first];
     R.ncta_base = bp.nfirst[first];
+    R.nscenes = bp.nscenes;
     R.use_tma = bp.use_tma;
     int *count = reinterpret_cast<int *>(base + bp.L.counts) + first;
     int *list = reinterpret_cast<int *>(base + bp.L.list) + (int64_t)bp.pfirst[first] * kScatterChunk;
