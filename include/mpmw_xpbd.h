@@ -81,8 +81,10 @@ int mpmw_hash_build(const float *x, int64_t n, const mpmw_hash_t *h, void *works
  * 13 MiB static device array inside the library, so n is limited to
  * MPMW_HASH_NOALLOC_MAX_POINTS; larger n returns MPMW_E_ARG.  The first call on
  * a device (that device current) resolves the array's address; make it before
- * any stream capture.  All calls on a device share the array: calls whose GPU
- * work overlaps race on it, so order them on one stream. */
+ * any stream capture.  The address is cached for the life of the process, so
+ * do not call this on a device after cudaDeviceReset.  All calls on a device
+ * share the array: calls whose GPU work overlaps race on it, so order them on
+ * one stream. */
 #define MPMW_HASH_NOALLOC_MAX_POINTS 1048576
 int mpmw_hash_build_noalloc(const float *x, int64_t n, const mpmw_hash_t *h, mpmw_stream_t stream);
 /* One XPBD kernel (MPMW_XK_*). */

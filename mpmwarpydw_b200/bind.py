@@ -44,6 +44,33 @@ def read_status(device, clear=True) -> int:
     return v
 
 
+STATUS_BITS = {1: "OOB", 2: "NAN", 4: "TIMEOUT"}  # MPMW_ST_* of mpmw.h
+
+
+def status_names(word: int):
+    """Names of the MPMW_ST_* bits set in a status word."""
+    return [name for bit, name in STATUS_BITS.items() if word & bit]
+
+
+class DeviceFault(RuntimeError):
+    """A kernel reported a non-finite particle position (MPMW_ST_NAN)."""
+
+
+def check_status(device, where: str, log=print) -> int:
+    """Read and clear the device status word after a stretch of GPU work.
+
+    A non-finite position (MPMW_ST_NAN) ends the run with DeviceFault; stencil
+    nodes outside the grid (MPMW_ST_OOB, the access was skipped) and bounded
+    waits that gave up (MPMW_ST_TIMEOUT, the kernel took its fallback) are
+    logged.  Returns the word."""
+    w = read_status(device)
+    if w & 2:
+        raise DeviceFault(f"{where}: a particle position became non-finite (status {status_names(w)})")
+    if w:
+        log(f"    warning: {where}: device status {status_names(w)}")
+    return w
+
+
 def ptr(t) -> int:
     return 0 if t is None else int(t.data_ptr())
 

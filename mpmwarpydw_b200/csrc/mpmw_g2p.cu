@@ -17,6 +17,7 @@
 //   the first half of a substep whenever a workspace is given; SVD-path
 //   particles go to the same worklist and k_stress_p2g_list.
 // The worklists live in the caller's workspace (mpmw_workspace_bytes).
+#include <atomic>
 #include <memory>
 #include <mutex>
 #include <unordered_map>
@@ -679,13 +680,24 @@ struct BatchRef {  // kernel argument: pointers into the prepared workspace
     int use_tma;
 };
 
+// A scene index read from the table that is not one of the prepared scenes
+// (a corrupted table): the CTA skips its work and reports it as MPMW_ST_OOB,
+// so its particles do not silently stay where they are.
+__device__ __forceinline__ bool bad_scene(int s, const BatchRef &R, uint32_t *status)
+{
+    if (s >= 0 && s < R.nscenes) return false;
+    if (threadIdx.x == 0) raise_status(status, MPMW_ST_OOB);
+    return true;
+}
+
 // Every thread of the CTA calls it: scene index of this particle CTA, and the
 // scene's record copied into `rec` (published by the barrier); -1 (for the
-// whole CTA, before any barrier) if the table holds no valid scene index.
-__device__ __forceinline__ int stage_scene(const BatchRef &R, BatchScene &rec)
+// whole CTA, before any barrier, reported in *status) if the table holds no
+// valid scene index.
+__device__ __forceinline__ int stage_scene(const BatchRef &R, BatchScene &rec, uint32_t *status)
 {
     const int s = R.pcta_scene[R.pcta_base + blockIdx.x];
-    if (s < 0 || s >= R.nscenes) return -1;  // uniform: every thread read the same entry
+    if (bad_scene(s, R, status)) return -1;  // uniform: every thread read the same entry
     constexpr int kWords = (int)(sizeof(BatchScene) / 4);
     if (threadIdx.x < kWords)
         reinterpret_cast<uint32_t *>(&rec)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&R.scene[s])[threadIdx.x];
@@ -699,11 +711,11 @@ __device__ __forceinline__ int stage_scene(const BatchRef &R, BatchScene &rec)
 constexpr int kBatchNodesPerThread = 8;
 constexpr int kBatchNodesPerCta = kBlock * kBatchNodesPerThread;
 
-__global__ void __launch_bounds__(kBlock) k_zero_grid_batch(const BatchRef R)
+__global__ void __launch_bounds__(kBlock) k_zero_grid_batch(const BatchRef R, uint32_t *status)
 {
     const int b = R.ncta_base + blockIdx.x;
     const int s = R.ncta_scene[b];
-    if (s < 0 || s >= R.nscenes) return;
+    if (bad_scene(s, R, status)) return;
     const mpmw_grid_t G = R.scene[s].grid;
     const int64_t total = (int64_t)G.dims[0] * G.dims[1] * G.dims[2];
     const int64_t g0 = (int64_t)(b - R.ncta_first[s]) * kBatchNodesPerCta + threadIdx.x;
@@ -714,11 +726,11 @@ __global__ void __launch_bounds__(kBlock) k_zero_grid_batch(const BatchRef R)
     }
 }
 
-__global__ void __launch_bounds__(kBlock) k_grid_update_batch(const BatchRef R, int zero_mv)
+__global__ void __launch_bounds__(kBlock) k_grid_update_batch(const BatchRef R, int zero_mv, uint32_t *status)
 {
     const int b = R.ncta_base + blockIdx.x;
     const int s = R.ncta_scene[b];
-    if (s < 0 || s >= R.nscenes) return;
+    if (bad_scene(s, R, status)) return;
     const BatchScene B = R.scene[s];
     const int64_t g0 = (int64_t)(b - R.ncta_first[s]) * kBatchNodesPerCta + threadIdx.x;
     const int64_t total = (int64_t)B.grid.dims[0] * B.grid.dims[1] * B.grid.dims[2];
@@ -742,7 +754,7 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_stress_p2g
     mpmw_particles_t P, const BatchRef R, uint32_t *status, int *svd_list, int *svd_count)
 {
     __shared__ BatchScene B;
-    if (stage_scene(R, B) < 0) return;
+    if (stage_scene(R, B, status) < 0) return;
     stress_p2g_body(P, B.grid, B.prm, status, svd_list, svd_count,
                     (int64_t)(R.pcta_base + blockIdx.x) * kScatterChunk);
 }
@@ -753,7 +765,7 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g_batc
     int *svd_count, int use_ahead)
 {
     __shared__ BatchScene B;
-    const int s = stage_scene(R, B);
+    const int s = stage_scene(R, B, status);
     if (s < 0) return;
     g2p2g_body<StoreStress>(P, B.grid, B.prm, status, svd_list, svd_count, &M.tmap[s], R.use_tma, use_ahead,
                             (int64_t)(R.pcta_base + blockIdx.x) * kScatterChunk);
@@ -765,7 +777,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_g2p_batch(mpmw_particles_t P, con
 {
     static_assert(kBlock == kScatterChunk, "particle CTAs of the batched G2P and P2G kernels coincide");
     __shared__ BatchScene B;
-    const int s = stage_scene(R, B);
+    const int s = stage_scene(R, B, status);
     if (s < 0) return;
     g2p_body<false>(P, B.grid, B.prm, status, nullptr, nullptr, &M.tmap[s], R.use_tma, use_ahead,
                     (int64_t)(R.pcta_base + blockIdx.x) * kBlock);
@@ -781,7 +793,7 @@ __global__ void __launch_bounds__(kBlock) k_stress_p2g_list_batch(mpmw_particles
         const int64_t p = list[q];
         if (p < 0 || p >= P.n) continue;
         const int s = R.pcta_scene[p / kScatterChunk];
-        if (s < 0 || s >= R.nscenes) continue;
+        if (s < 0 || s >= R.nscenes) { bad |= MPMW_ST_OOB; continue; }
         const BatchScene &B = R.scene[s];
         stress_p2g_one(P, B.grid, B.prm, p, bad);
     }
@@ -897,7 +909,9 @@ int prepare_batch(const mpmw_particles_t &p, const mpmw_grid_t *grids, const mpm
     return MPMW_OK;
 }
 
-static bool g_batch_attr[64];
+// per device: the batched kernels' shared-memory attribute is set (several host
+// threads may launch batches at once; setting it twice is harmless)
+static std::atomic<bool> g_batch_attr[64];
 
 // The fused schedule of mpmw_run_substeps over the scenes [first, last) of a
 // batch that prepare_batch wrote into this workspace (last < 0: to the end).
@@ -926,7 +940,7 @@ int launch_batch_substeps(const mpmw_particles_t &p, int first, int last, int ns
     const size_t smem = sizeof(G2P2GShared) + 128;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) { set_error("batch: no current device"); return MPMW_E_DEVICE; }
-    if (dev >= 0 && dev < 64 && !g_batch_attr[dev]) {
+    if (dev >= 0 && dev < 64 && !g_batch_attr[dev].load(std::memory_order_acquire)) {
         if (cudaFuncSetAttribute(k_g2p2g_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
             cudaFuncSetAttribute(k_g2p2g_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
             cudaFuncSetAttribute(k_stress_p2g_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -934,7 +948,7 @@ int launch_batch_substeps(const mpmw_particles_t &p, int first, int last, int ns
             set_error("batch: cannot reserve %zu bytes of shared memory", smem);
             return MPMW_E_DEVICE;
         }
-        g_batch_attr[dev] = true;
+        g_batch_attr[dev].store(true, std::memory_order_release);
     }
     unsigned char *base = static_cast<unsigned char *>(ws);
     BatchRef R;
@@ -955,7 +969,7 @@ int launch_batch_substeps(const mpmw_particles_t &p, int first, int last, int ns
         return MPMW_OK;
     };
     // prologue: every grid cleared, substep 1's return map and P2G
-    k_zero_grid_batch<<<nctas, kBlock, 0, s>>>(R);
+    k_zero_grid_batch<<<nctas, kBlock, 0, s>>>(R, st);
     MPMW_TRY_LAUNCH("k_zero_grid_batch");
     if (reset_count() != MPMW_OK) return MPMW_E_DEVICE;
     k_stress_p2g_batch<<<pctas, kScatterChunk, sizeof(ScatterShared), s>>>(p, R, st, list, count);
@@ -964,7 +978,7 @@ int launch_batch_substeps(const mpmw_particles_t &p, int first, int last, int ns
     MPMW_TRY_LAUNCH("k_stress_p2g_list_batch");
     for (int step = 0; step < nsteps; ++step) {
         if (step < nsteps - 1) {
-            k_grid_update_batch<<<nctas, kBlock, 0, s>>>(R, 1);
+            k_grid_update_batch<<<nctas, kBlock, 0, s>>>(R, 1, st);
             MPMW_TRY_LAUNCH("k_grid_update_batch");
             if (reset_count() != MPMW_OK) return MPMW_E_DEVICE;
             if (step + 1 == nsteps - 1)
@@ -975,7 +989,7 @@ int launch_batch_substeps(const mpmw_particles_t &p, int first, int last, int ns
             k_stress_p2g_list_batch<<<148 * 4, kBlock, 0, s>>>(p, R, st, list, count);
             MPMW_TRY_LAUNCH("k_stress_p2g_list_batch");
         } else {
-            k_grid_update_batch<<<nctas, kBlock, 0, s>>>(R, 0);
+            k_grid_update_batch<<<nctas, kBlock, 0, s>>>(R, 0, st);
             MPMW_TRY_LAUNCH("k_grid_update_batch");
             k_g2p_batch<<<pctas, kBlock, 0, s>>>(p, R, *bp.maps, st, bp.use_ahead_g2p);
             MPMW_TRY_LAUNCH("k_g2p_batch");

@@ -11,7 +11,10 @@
 //
 // Set-up: the first call on a device (with that device current) looks up the
 // array's device address with cudaGetSymbolAddress and caches it for that
-// device.  Make that first call before any stream capture begins.
+// device.  Make that first call before any stream capture begins.  The cache
+// lives as long as the process and does not notice cudaDeviceReset: a reset
+// unloads the module, and a later call would pass the stale address.  A caller
+// that resets a device must not use this entry point on it afterwards.
 //
 // Sharing: every call on a device uses the same array.  The array keeps the
 // previous call's contents; hash_build overwrites every scratch word it reads

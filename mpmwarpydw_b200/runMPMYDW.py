@@ -45,7 +45,7 @@ import numpy as np
 import torch
 
 from . import domains as _domains
-from .bind import params_from_states
+from .bind import check_status, params_from_states
 from .engine import DeviceLoop, SubstepGraphCache, original_order, sort_particles
 from .scene import build_states
 from .utils import mpmRoutines
@@ -202,6 +202,7 @@ def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=Non
                                                        sim.residualThreshold, sim.damage_stall_threshold,
                                                        int(sim.damage_stall_duration / sim.dt), mon.min_steps)
                     st = loop.run(c, mon.stall, mon.residual, mon.prev_damage, seg)
+                    check_status(dev, f"substeps {c}-{st.counter}", log)
                     sim.t += (st.counter - c) * sim.dt
                     mon.counter, mon.stall, mon.residual, mon.prev_damage = st.counter, st.stall, st.residual, st.prev_damage
                     if pulsing and mon.counter == pulse_steps:
@@ -234,6 +235,7 @@ def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=Non
                 done += m
             sim.t += k * sim.dt
             residual, mean_damage, counts = _stats(sim, mpm)
+            check_status(dev, f"substeps {c}-{c + k}", log)
             if pulsing and mon.counter + k == pulse_steps:
                 sim.gravity = base_gravity
             if not mon.update(k, residual, mean_damage):
@@ -249,6 +251,7 @@ def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=Non
         if pulsing:
             sim.gravity = base_gravity
         log(f"  phase 1 done after {mon.counter} substeps ({mon.counter * sim.dt:.3f}s simulated)")
+        check_status(dev, "phase 1", log)
         # phase 2: XPBD only
         for j in range(1, sim.xpbdOnlySteps + 1):
             S.xpbdSimulationStep(sim, mpm, xpbd, dev, xpbd_only=True)
@@ -261,6 +264,7 @@ def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=Non
         # end of big step: deactivate XPBD particles below the datum
         minB, maxB = np.asarray(sim.minBounds, np.float64), np.asarray(sim.maxBounds, np.float64)
         z_datum = args.xpbd_deactivation_z_datum if args.xpbd_deactivation_z_datum is not None else float(minB[2])
+        check_status(dev, "phase 2", log)
         mpmRoutines.deactivate_and_teleport_xpbd_below_datum(sim.particle_x, sim.particle_v, sim.activeLabel,
                                                               sim.materialLabel, float(z_datum),
                                                               2.0 * float(maxB[2] - minB[2]))

@@ -101,6 +101,13 @@ class SceneBatch:
     def replay(self):
         self.graph.replay()
 
+    def check(self, where: str = "batch", log=print) -> int:
+        """Read and clear the device status word after the batch ran (raises on
+        a non-finite position; logs out-of-grid stencils, bad scene-table
+        entries and bounded-wait timeouts)."""
+        from .bind import check_status
+        return check_status(self.device, where, log)
+
     def results(self):
         out = []
         for i, (sim, mpm, xpbd) in enumerate(self.states):
@@ -306,6 +313,13 @@ class ConcatBatch:
                     src = self.scene_field(i, name)
                     dst.copy_(src.reshape(dst.shape) if self._aos[name] else src)
 
+    def check(self, where: str = "batch", log=print) -> int:
+        """Read and clear the device status word after the batch ran (raises on
+        a non-finite position; logs out-of-grid stencils, bad scene-table
+        entries and bounded-wait timeouts)."""
+        from .bind import check_status
+        return check_status(self.device, where, log)
+
     def results(self):
         out = []
         for i, c in enumerate(self.counts):
@@ -367,4 +381,5 @@ def _run_batch(scenes, steps, chunk, device, tune_k: int = 5):
     if steps > done:
         b.step(steps - done)
     torch.cuda.synchronize(dev)
+    b.check(f"sweep of {len(scenes)} scenes")
     return b.results()

@@ -4,9 +4,9 @@ kernel and orchestration source (MPMWarpYDW utils/simulationRoutines.py,
 utils/mpmRoutines.py, utils/xpbdRoutines.py, utils/simStates.py) in float64 on
 the CPU, through the Warp stand-in in fakewarp.py.
 
-    python tests/golden/gen_golden.py [--reference PATH]
+    python tests/golden/gen_golden.py --reference PATH     (or MPMW_REFERENCE=PATH)
 
-Needs a checkout of the reference (default: /root/reference); the fixtures it
+Needs a checkout of the reference project (no default location); the fixtures it
 writes are committed, so the tests never read the reference.  Each fixture is
 one seeded scene: every input array (``in/<state>.<attribute>``), then the
 arrays that one ``mpmSimulationStep`` or ``xpbdSimulationStep`` changed
@@ -159,8 +159,11 @@ def snapshot(wp, objs, prefix):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("MPMW_REFERENCE"),
+                    help="checkout of the reference project (or set MPMW_REFERENCE)")
     a = ap.parse_args()
+    if not a.reference:
+        ap.error("give the reference checkout with --reference PATH or MPMW_REFERENCE")
     wp, SS, RS, RM = load_reference(a.reference)
     scenes = [
         ("mpm_friction", 101, dict(dt=1e-4), "mpm", {}),
