@@ -230,9 +230,12 @@ int mpmw_creep(const mpmw_particles_t *p, const float *ys_base, float dt, float 
                float damage_exponent, mpmw_stream_t stream);
 
 /* ---- per-step statistics (utils/simulationRoutines.py:538-675) ----------- */
-/* out (device, 7 doubles, overwritten): sum |v|/radius over active (velocityConvergence),
- * active count (countActiveParticles), sum damage over active (compute_mean_gpu numerator),
- * active MPM, active XPBD, inactive MPM, inactive XPBD (countParticlesByType). */
+/* out (device, 7 doubles, 8-byte aligned, overwritten): sum |v|/radius over active
+ * (velocityConvergence), active count (countActiveParticles), sum damage over active
+ * (compute_mean_gpu numerator), active MPM, active XPBD, inactive MPM, inactive XPBD
+ * (countParticlesByType).  The sums are accumulated in FP32 (compensated per thread,
+ * pairwise per block, one FP32 atomic per block), the counts in integers; only the
+ * final conversion writes doubles.  Two launches. */
 int mpmw_stats(const mpmw_particles_t *p, double *out, mpmw_stream_t stream);
 
 /* ---- phase-1 loop on the device (runMPMYDW.py:656-727) ------------------ */

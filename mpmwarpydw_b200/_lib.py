@@ -57,6 +57,8 @@ class Params(ctypes.Structure):
 STRESS_AUTO, STRESS_SVD = 0, 1
 
 MLP_IN, MLP_HID, MLP_OUT, MLP_NPARAM, MLP_PACKED_BYTES = 8, 64, 4, 9156, 20480
+SURR_NSTATS = 8          # MPMW_SURR_NSTATS
+SURR_D_MAX = 0.999       # MPMW_SURR_D_MAX
 
 
 class XPBD(ctypes.Structure):

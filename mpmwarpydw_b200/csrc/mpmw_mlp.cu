@@ -8,7 +8,9 @@
 //   yield = (1 - D)(ys - alpha p); plastic if sigma_eq > yield,
 //   edn = |dev e| + 1e-6, dgamma = edn - yield / (2 mu), d_acc = sqrt(2/3) dgamma,
 //   e_ret = e - (dgamma / edn) dev e + beta dgamma.
-// Features and targets are defined in include/mpmw_mlp.h.
+// Features and targets are defined in include/mpmw_mlp.h: the targets are the
+// return's ratios (ln rho, ln(1 - rho), beta, sqrt(2/3)), so an output error is
+// a relative error of the returned deviator and plastic multiplier.
 #include <cuda_bf16.h>
 
 #include "mpmw_common.cuh"
@@ -68,11 +70,16 @@ __device__ int dp_return(const double *e, double mu, double lam, double ys, doub
     return 1;
 }
 
+// smallest ln(1 - rho) kept in a target (trials this close to the yield
+// surface are left to the gate's exact fallback)
+constexpr double kLn1mRhoMin = -12.0;
+
 __global__ void k_dp_samples(int64_t n, uint64_t seed, float *__restrict__ x, float *__restrict__ y)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double e[3] = {0, 0, 0}, er[3] = {0, 0, 0}, dacc = 0.0, mag = 1e-6, yv = 1.0, alpha = 0, beta = 0, D = 0, nu = 0.25;
+    double rho = 0.5;
     for (int attempt = 0; attempt < 64; ++attempt) {
         uint64_t s = seed ^ (0xD1B54A32D192ED03ull * (uint64_t)(i + 1)) ^ ((uint64_t)attempt << 56);
         mag = pow(10.0, -6.0 + 5.0 * u01(s));
@@ -97,18 +104,27 @@ __global__ void k_dp_samples(int64_t n, uint64_t seed, float *__restrict__ x, fl
         const double ys = 1e5 * pow(50.0, u01(s));
         const double E = 1e9 * pow(50.0, u01(s));
         nu = 0.15 + 0.2 * u01(s);
-        D = u01(s);
+        D = (double)MPMW_SURR_D_MAX * u01(s);
         const double mu = E / (2.0 * (1.0 + nu)), lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
         yv = ys / (2.0 * mu);
-        if (dp_return(e, mu, lam, ys, alpha, beta, D, er, dacc) == 1) break;
-        er[0] = e[0]; er[1] = e[1]; er[2] = e[2]; dacc = 0.0;  // elastic fallback after 64 attempts
+        if (dp_return(e, mu, lam, ys, alpha, beta, D, er, dacc) == 1) {
+            // rho = yield / (2 mu |dev e|), from the same quantities as the return
+            const double tr = e[0] + e[1] + e[2], p = (2.0 * mu / 3.0 + lam) * tr;
+            const double m3 = tr / 3.0;
+            const double nd = sqrt((e[0] - m3) * (e[0] - m3) + (e[1] - m3) * (e[1] - m3) + (e[2] - m3) * (e[2] - m3));
+            rho = (1.0 - D) * (ys - alpha * p) / (2.0 * mu * nd);
+            if (rho > 0.0 && rho < 1.0) break;
+        }
+        rho = 0.5;  // (only after 64 elastic attempts)
     }
     float *xo = x + 8 * i, *yo = y + 4 * i;
     xo[0] = (float)(e[0] / mag); xo[1] = (float)(e[1] / mag); xo[2] = (float)(e[2] / mag);
     xo[3] = (float)log10(mag / yv);
-    xo[4] = (float)alpha; xo[5] = (float)beta; xo[6] = (float)D; xo[7] = (float)nu;
-    for (int k = 0; k < 3; ++k) yo[k] = (float)((er[k] - e[k]) / mag);
-    yo[3] = (float)(dacc / mag);
+    xo[4] = (float)alpha; xo[5] = (float)beta; xo[6] = (float)log1p(-D); xo[7] = (float)nu;
+    yo[0] = (float)log(rho);
+    yo[1] = (float)fmax(log1p(-rho), kLn1mRhoMin);
+    yo[2] = (float)beta;
+    yo[3] = (float)sqrt(2.0 / 3.0);
 }
 
 // ---------------------------------------------------------------------------
@@ -147,7 +163,8 @@ __device__ void load_weights(TrainShared &S, const float *__restrict__ P)
         S.w2t[k][j] = bf16r(P[oW2 + q]);
         S.w3t[k][j] = bf16r(P[oW3 + q]);
     }
-    for (int q = threadIdx.x; q < OUT * H; q += blockDim.x) { int o = q / H, k = q % H; S.w4t[k][o] = bf16r(P[oW4 + q]); }
+    // the last layer stays FP32 (it runs on the CUDA cores at inference)
+    for (int q = threadIdx.x; q < OUT * H; q += blockDim.x) { int o = q / H, k = q % H; S.w4t[k][o] = P[oW4 + q]; }
     for (int q = threadIdx.x; q < H; q += blockDim.x) { S.b1[q] = P[oB1 + q]; S.b2[q] = P[oB2 + q]; S.b3[q] = P[oB3 + q]; }
     if (threadIdx.x < OUT) S.b4[threadIdx.x] = P[oB4 + threadIdx.x];
 }
@@ -350,9 +367,9 @@ __global__ void k_mlp_pack(const float *__restrict__ P, __nv_bfloat16 *__restric
     auto put = [&](int off, int r, int k, int K, float v) {
         *reinterpret_cast<__nv_bfloat16 *>(base + off + core_offset(r, k, K)) = __float2bfloat16_rn(v);
     };
-    if (q < H * 16) {  // W1: 64 x 16 (inputs 8..15 zero)
+    if (q < H * 16) {  // W1: 64 x 16, [W1 | W1]: inputs 0..7 take the features' hi terms, 8..15 their lo terms
         const int r = q / 16, k = q % 16;
-        put(kPackW1, r, k, 16, k < IN ? P[oW1 + r * IN + k] : 0.f);
+        put(kPackW1, r, k, 16, P[oW1 + r * IN + (k & (IN - 1))]);
     }
     if (q < H * H) {
         const int r = q / H, k = q % H;
@@ -367,7 +384,9 @@ __global__ void k_mlp_pack(const float *__restrict__ P, __nv_bfloat16 *__restric
 
 struct TcShared {
     unsigned char w[MPMW_MLP_PACKED_BYTES];   // B operands
-    unsigned char a[kTcRows * H * 2];         // A operand (activations)
+    unsigned char a[kTcRows * H * 2];         // A operand: activations, BF16 hi terms
+    unsigned char alo[kTcRows * H * 2];       // A operand: activations, BF16 lo terms (a - hi)
+    float w4[OUT][H];                         // last layer, FP32
     float bias[3 * H + OUT];
     uint64_t bar;
     uint32_t tmem;
@@ -420,15 +439,25 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float *v)
 
 __device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// write this thread's row of 64 BF16 activations into the K = 64 A tile
-__device__ __forceinline__ void put_row64(unsigned char *a, int r, const float *h)
+// a = hi + lo with hi = bf16(a), lo = bf16(a - hi): the pair carries about
+// 16 mantissa bits, and both terms go through the MMA with the same weights
+__device__ __forceinline__ void split_bf16(float a0, float a1, __nv_bfloat162 &hi, __nv_bfloat162 &lo)
+{
+    hi = __floats2bfloat162_rn(a0, a1);
+    const float2 h = __bfloat1622float2(hi);
+    lo = __floats2bfloat162_rn(a0 - h.x, a1 - h.y);
+}
+
+// write this thread's row of 64 activations into the K = 64 A tiles (hi, lo)
+__device__ __forceinline__ void put_row64(unsigned char *a, unsigned char *alo, int r, const float *h)
 {
 #pragma unroll
     for (int kb = 0; kb < 8; ++kb) {
-        __nv_bfloat162 v[4];
+        __nv_bfloat162 v[4], w[4];
 #pragma unroll
-        for (int c = 0; c < 4; ++c) v[c] = __floats2bfloat162_rn(h[8 * kb + 2 * c], h[8 * kb + 2 * c + 1]);
+        for (int c = 0; c < 4; ++c) split_bf16(h[8 * kb + 2 * c], h[8 * kb + 2 * c + 1], v[c], w[c]);
         *reinterpret_cast<uint4 *>(a + core_offset(r, 8 * kb, H)) = *reinterpret_cast<uint4 *>(v);
+        *reinterpret_cast<uint4 *>(alo + core_offset(r, 8 * kb, H)) = *reinterpret_cast<uint4 *>(w);
     }
 }
 
@@ -456,23 +485,19 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const unsigned char *_
             S.bias[2 * H + q] = P[oB3 + q];
         }
         if (t < OUT) S.bias[3 * H + t] = P[oB4 + t];
+        for (int q = t; q < OUT * H; q += kTcRows) S.w4[q / H][q % H] = P[oW4 + q];
     }
-    // layer-1 operand: this row's 8 features, K padded to 16
+    // layer-1 operand: this row's 8 features as hi terms (k 0..7) and lo terms
+    // (k 8..15), against [W1 | W1]
     {
-        float f[16];
+        float f[IN];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) f[k] = 0.f;
-        if (row < n) {
+        for (int k = 0; k < IN; ++k) f[k] = row < n ? X[row * IN + k] : 0.f;
+        __nv_bfloat162 v[4], w[4];
 #pragma unroll
-            for (int k = 0; k < IN; ++k) f[k] = X[row * IN + k];
-        }
-#pragma unroll
-        for (int kb = 0; kb < 2; ++kb) {
-            __nv_bfloat162 v[4];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) v[c] = __floats2bfloat162_rn(f[8 * kb + 2 * c], f[8 * kb + 2 * c + 1]);
-            *reinterpret_cast<uint4 *>(S.a + core_offset(t, 8 * kb, 16)) = *reinterpret_cast<uint4 *>(v);
-        }
+        for (int c = 0; c < 4; ++c) split_bf16(f[2 * c], f[2 * c + 1], v[c], w[c]);
+        *reinterpret_cast<uint4 *>(S.a + core_offset(t, 0, 16)) = *reinterpret_cast<uint4 *>(v);
+        *reinterpret_cast<uint4 *>(S.a + core_offset(t, 8, 16)) = *reinterpret_cast<uint4 *>(w);
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&S.tmem)),
@@ -489,17 +514,23 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const unsigned char *_
     const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
     unsigned phase = 0;
     float h[H];
-    for (int layer = 0; layer < 4; ++layer) {
+    // layers 1-3 on the tensor cores (hi and lo operand terms into one
+    // accumulator), the last layer in FP32 from the registers
+    for (int layer = 0; layer < 3; ++layer) {
         const int K = layer == 0 ? 16 : H;
-        const int N = layer == 3 ? 16 : H;
+        const int N = H;
         if (t == 0 && !S.timeout) {
             tc_fence_after();
-            const unsigned char *w = S.w + (layer == 0 ? kPackW1 : layer == 1 ? kPackW2 : layer == 2 ? kPackW3 : kPackW4);
+            const unsigned char *w = S.w + (layer == 0 ? kPackW1 : layer == 1 ? kPackW2 : kPackW3);
             const uint32_t id = idesc_bf16(N);
-            for (int kk = 0; kk < K / 16; ++kk) {
-                const uint64_t ad = smem_desc(S.a + kk * 256, 128, (K / 8) * 128);
-                const uint64_t bd = smem_desc(w + kk * 256, 128, (K / 8) * 128);
-                tc_mma(tmem, ad, bd, id, kk > 0);
+            const int terms = layer == 0 ? 1 : 2;  // layer 1 holds both terms in its K = 16
+            for (int term = 0; term < terms; ++term) {
+                const unsigned char *a = term == 0 ? S.a : S.alo;
+                for (int kk = 0; kk < K / 16; ++kk) {
+                    const uint64_t ad = smem_desc(a + kk * 256, 128, (K / 8) * 128);
+                    const uint64_t bd = smem_desc(w + kk * 256, 128, (K / 8) * 128);
+                    tc_mma(tmem, ad, bd, id, (term | kk) > 0);
+                }
             }
             tc_commit(&S.bar);
         }
@@ -512,20 +543,27 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const unsigned char *_
         // accumulators of this thread's row
         for (int c = 0; c < N; c += 16) tc_ld16(lane_addr + (uint32_t)c, h + c);
         tc_wait_ld();
-        if (layer < 3) {
+        {
             const float *b = S.bias + layer * H;
 #pragma unroll
             for (int j = 0; j < H; ++j) {
                 const float z = h[j] + b[j];
                 h[j] = z / (1.f + expf(-z));
             }
-            put_row64(S.a, t, h);
+        }
+        if (layer < 2) {
+            put_row64(S.a, S.alo, t, h);
             proxy_fence();
             tc_fence_before();
             __syncthreads();
         } else if (row < n) {
 #pragma unroll
-            for (int o = 0; o < OUT; ++o) Y[row * OUT + o] = h[o] + S.bias[3 * H + o];
+            for (int o = 0; o < OUT; ++o) {
+                float z = S.bias[3 * H + o];
+#pragma unroll
+                for (int k = 0; k < H; ++k) z = fmaf(h[k], S.w4[o][k], z);
+                Y[row * OUT + o] = z;
+            }
         }
     }
     tc_fence_before();

@@ -202,11 +202,32 @@ __global__ void k_creep(mpmw_particles_t P, const float *ys_base, float dt, floa
     P.ys[p] = rmax(0.f, P.ys[p] - decay);
 }
 
-// per-step statistics: block reduce in double, one atomic per block per field
-__global__ void __launch_bounds__(kBlock) k_stats(mpmw_particles_t P, double *out)
+// Per-step statistics in FP32 and integers (no FP64 arithmetic on the GPU).
+// The two sums (|v|/r and damage over active particles) are Kahan-compensated
+// per thread, reduced pairwise across the block with the compensation folded
+// in, and added across blocks with one FP32 atomic per block (at most 1184
+// terms, so the cross-block rounding stays near 1e-7 relative); the five
+// counts are exact integer atomics.  While the kernel runs, `out` (7 doubles)
+// holds that accumulator (StatsAcc); k_stats_finish converts it in place.
+struct StatsAcc {
+    float res, dmg;           // sum |v|/r, sum damage over active particles
+    unsigned int count[5];    // active, active MPM, active XPBD, inactive MPM, inactive XPBD
+};
+static_assert(sizeof(StatsAcc) <= 7 * sizeof(double), "the accumulator fits the output");
+
+__device__ __forceinline__ void kahan_add(float &sum, float &c, float x)
+{
+    const float y = x - c;
+    const float t = sum + y;
+    c = (t - sum) - y;
+    sum = t;
+}
+
+__global__ void __launch_bounds__(kBlock) k_stats(mpmw_particles_t P, StatsAcc *acc_out)
 {
     const int64_t n = P.n;
-    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    float res = 0.f, res_c = 0.f, dmg = 0.f, dmg_c = 0.f;
+    unsigned int cnt[5] = {0u, 0u, 0u, 0u, 0u};
     // every field is loaded whatever the labels, so the loads of several
     // iterations are in flight together
 #pragma unroll 4
@@ -214,29 +235,61 @@ __global__ void __launch_bounds__(kBlock) k_stats(mpmw_particles_t P, double *ou
         const int a = P.active[p], mt = P.material[p];
         float v3[3];
         load3(P.v, n, p, v3);
-        const float r = P.radius[p], dmg = P.damage[p];
+        const float r = P.radius[p], d = P.damage[p];
         const bool act = a == 1, xp = mt == 2;
         if (act) {
-            acc[0] += (double)(len3(v3) / r);
-            acc[1] += 1.0;
-            acc[2] += (double)dmg;
+            kahan_add(res, res_c, len3(v3) / r);
+            kahan_add(dmg, dmg_c, d);
+            ++cnt[0];
         }
-        if (xp) { if (act) acc[4] += 1.0; else acc[6] += 1.0; }
-        else { if (act) acc[3] += 1.0; else acc[5] += 1.0; }
+        if (xp) { if (act) ++cnt[2]; else ++cnt[4]; }
+        else { if (act) ++cnt[1]; else ++cnt[3]; }
     }
-    __shared__ double red[7][kBlock / 32];
+    res -= res_c;
+    dmg -= dmg_c;
+    // pairwise across the warp, then across the warps of the block
+    for (int o = 16; o > 0; o >>= 1) {
+        res += __shfl_down_sync(0xffffffffu, res, o);
+        dmg += __shfl_down_sync(0xffffffffu, dmg, o);
 #pragma unroll
-    for (int k = 0; k < 7; ++k) {
-        double v = acc[k];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = v;
+        for (int k = 0; k < 5; ++k) cnt[k] += __shfl_down_sync(0xffffffffu, cnt[k], o);
+    }
+    __shared__ float fr[kBlock / 32], fd[kBlock / 32];
+    __shared__ unsigned int fc[5][kBlock / 32];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        fr[w] = res; fd[w] = dmg;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) fc[k][w] = cnt[k];
     }
     __syncthreads();
-    if (threadIdx.x < 7) {
-        double s = 0;
-        for (int w = 0; w < kBlock / 32; ++w) s += red[threadIdx.x][w];
-        atomicAdd(&out[threadIdx.x], s);
+    if (threadIdx.x == 0) {
+        float a = 0.f, b = 0.f;
+        unsigned int c[5] = {0u, 0u, 0u, 0u, 0u};
+        for (int q = 0; q < kBlock / 32; ++q) {
+            a += fr[q]; b += fd[q];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) c[k] += fc[k][q];
+        }
+        atomicAdd(&acc_out->res, a);
+        atomicAdd(&acc_out->dmg, b);
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+            if (c[k]) atomicAdd(&acc_out->count[k], c[k]);
     }
+}
+
+// the accumulator -> the 7 doubles of mpmw_stats, in place (one thread)
+__global__ void k_stats_finish(double *out)
+{
+    const StatsAcc a = *reinterpret_cast<const StatsAcc *>(out);
+    out[0] = (double)a.res;
+    out[1] = (double)a.count[0];
+    out[2] = (double)a.dmg;
+    out[3] = (double)a.count[1];
+    out[4] = (double)a.count[2];
+    out[5] = (double)a.count[3];
+    out[6] = (double)a.count[4];
 }
 
 // ---------------------------------------------------------------------------
@@ -593,13 +646,16 @@ int mpmw_stats(const mpmw_particles_t *p, double *out, mpmw_stream_t stream)
         set_error("stats: active, material, v, radius and damage are required");
         return MPMW_E_ARG;
     }
+    if ((reinterpret_cast<uintptr_t>(out) & 7u) != 0) { set_error("stats: out must be 8-byte aligned"); return MPMW_E_ARG; }
     cudaStream_t s = as_stream(stream);
     if (cudaMemsetAsync(out, 0, 7 * sizeof(double), s) != cudaSuccess) { set_error("stats: memset failed"); return MPMW_E_DEVICE; }
     if (p->n == 0) return MPMW_OK;
     int64_t blocks = (p->n + kBlock - 1) / kBlock;
     if (blocks > 148 * 8) blocks = 148 * 8;
-    k_stats<<<(unsigned)blocks, kBlock, 0, s>>>(*p, out);
-    return check_launch("k_stats");
+    k_stats<<<(unsigned)blocks, kBlock, 0, s>>>(*p, reinterpret_cast<StatsAcc *>(out));
+    MPMW_TRY_LAUNCH("k_stats");
+    k_stats_finish<<<1, 1, 0, s>>>(out);
+    return check_launch("k_stats_finish");
 }
 
 }  // extern "C"

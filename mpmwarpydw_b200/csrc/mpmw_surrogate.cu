@@ -10,7 +10,10 @@
 //                    with their principal log strains e, eigenvectors Q and
 //                    surrogate features.
 //   k_mlp_infer_tc   the network on the listed features (tensor cores).
-//   k_surr_finish    returned strains e_ret = e + |e| y[0..2], d_acc = |e| y[3];
+//   k_surr_finish    the return from the network's ratios (include/mpmw_mlp.h):
+//                    rho = exp(y[0]), dgamma = n exp(y[1]) + 1e-6 with
+//                    n = |dev e|, e_ret = e + (rho n/(n + 1e-6) - 1) dev e +
+//                    y[2] dgamma, d_acc = y[3] dgamma;
 //                    a gate on the return's defining identities (yield
 //                    residual, flow-rule magnitude, volumetric part), each
 //                    within `gate_tol`, else the exact closed-form return;
@@ -127,7 +130,7 @@ __global__ void __launch_bounds__(kBlock) k_surr_classify(mpmw_particles_t P, fl
         make_trial(P, p, eps, T);
         const bool d_one = T.ys < 0.f || T.yield_eff < 0.f;
         const bool plastic = (2.f * T.mu) * T.dev_norm > T.yield_eff;
-        if (plastic && !d_one && T.dev_norm > 0.f) {
+        if (plastic && !d_one && T.dev_norm > 0.f && T.D <= MPMW_SURR_D_MAX) {
             float A[9], lam[3], Q[9];
             sym_to_full(eps, A);
             sym_eigen3(A, lam, Q);
@@ -138,7 +141,7 @@ __global__ void __launch_bounds__(kBlock) k_surr_classify(mpmw_particles_t P, fl
             float *f = W.feat + 8 * (int64_t)slot;
             f[0] = lam[0] / mag; f[1] = lam[1] / mag; f[2] = lam[2] / mag;
             f[3] = log10f(mag / y);
-            f[4] = T.alpha; f[5] = 0.3f * T.alpha; f[6] = T.D;
+            f[4] = T.alpha; f[5] = 0.3f * T.alpha; f[6] = log1pf(-T.D);
             f[7] = T.lam / (2.f * (T.lam + T.mu));
             float *q = W.eq + 12 * (int64_t)slot;
             q[0] = lam[0]; q[1] = lam[1]; q[2] = lam[2];
@@ -159,7 +162,8 @@ __global__ void __launch_bounds__(kBlock) k_surr_classify(mpmw_particles_t P, fl
 // stats: [0] listed (surrogate candidates), [1] gate fallbacks, [2] audited,
 // [3] largest audited relative stress error (float bits, atomicMax on the bits
 // of a non-negative float), [4] sum of audited relative errors (float),
-// [5] audited with relative error <= 1e-3
+// [5] audited with relative error <= 1e-3, [6] audited and accepted by the
+// gate, [7] largest audited relative stress error among those accepted
 __global__ void __launch_bounds__(kBlock) k_surr_finish(mpmw_particles_t P, float eff, SurrWork W, float gate_tol,
                                                         int audit_per_mille, uint64_t audit_seed, uint32_t *stats)
 {
@@ -178,28 +182,35 @@ __global__ void __launch_bounds__(kBlock) k_surr_finish(mpmw_particles_t P, floa
         float Q[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) Q[k] = eq[3 + k];
-        const float mag = sqrtf(fma_(e[0], e[0], fma_(e[1], e[1], e[2] * e[2])));
         const float *y = W.out + 4 * (int64_t)q;
-        float er[3] = {fma_(mag, y[0], e[0]), fma_(mag, y[1], e[1]), fma_(mag, y[2], e[2])};
-        float dacc = mag * y[3];
-        // exact return quantities of the trial (closed form)
-        const float twomu = 2.f * T.mu;
-        const float edn = T.dev_norm + 1e-6f;
-        const float dg_ex = edn - T.yield_eff / twomu;
         const float em = (e[0] + e[1] + e[2]) / 3.f;
         const float ed[3] = {e[0] - em, e[1] - em, e[2] - em};
+        const float nd = sqrtf(fma_(ed[0], ed[0], fma_(ed[1], ed[1], ed[2] * ed[2])));
+        const float edn = nd + 1e-6f;
+        // the network's return: deviator scaled by rho n / (n + 1e-6), plastic
+        // multiplier n (1 - rho) + 1e-6 (both ratios predicted in log form)
+        const float rho = expf(y[0]);
+        const float dg = fma_(nd, expf(y[1]), 1e-6f);
+        const float sdev = rho * (nd / edn) - 1.f;
+        float er[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) er[k] = fma_(sdev, ed[k], e[k]) + y[2] * dg;
+        float dacc = y[3] * dg;
+        // exact return quantities of the trial (closed form)
+        const float twomu = 2.f * T.mu;
+        const float dg_ex = edn - T.yield_eff / twomu;
         const float beta = 0.3f * T.alpha;
         // gate: the identities that define the radial return
-        const float dg = dacc / sqrtf(2.f / 3.f);
         const float rm = (er[0] + er[1] + er[2]) / 3.f;
         const float edr[3] = {er[0] - rm, er[1] - rm, er[2] - rm};
         const float ndr = sqrtf(edr[0] * edr[0] + edr[1] * edr[1] + edr[2] * edr[2]);
         const float ysc = fmaxf(T.yield_eff / twomu, 1e-12f);
-        const float r_yield = fabsf(ndr - (T.yield_eff / twomu) * (T.dev_norm / edn)) / ysc;
-        const float r_flow = fabsf(dg - dg_ex) / fmaxf(dg_ex, 1e-12f);
-        const float r_vol = fabsf((rm - em) * 3.f - 3.f * beta * dg) / fmaxf(3.f * beta * dg_ex, ysc);
+        const float r_yield = fabsf(ndr - (T.yield_eff / twomu) * (nd / edn)) / ysc;
+        const float r_flow = fmaxf(fabsf(dg - dg_ex), fabsf(dacc - sqrtf(2.f / 3.f) * dg_ex) / sqrtf(2.f / 3.f)) /
+                             fmaxf(dg_ex, 1e-12f);
+        const float r_vol = fabsf((rm - em) * 3.f - 3.f * beta * dg_ex) / fmaxf(3.f * beta * dg_ex, ysc);
         const bool ok = dg > 0.f && r_yield <= gate_tol && r_flow <= gate_tol && r_vol <= gate_tol &&
-                        isfinite(er[0]) && isfinite(er[1]) && isfinite(er[2]);
+                        isfinite(er[0]) && isfinite(er[1]) && isfinite(er[2]) && isfinite(dacc);
         float ex[3];
         const float f_ex = dg_ex / edn, vc_ex = beta * dg_ex;
 #pragma unroll
@@ -221,6 +232,10 @@ __global__ void __launch_bounds__(kBlock) k_surr_finish(mpmw_particles_t P, floa
             atomicMax(&stats[3], __float_as_uint(rel));
             atomicAdd(reinterpret_cast<float *>(&stats[4]), rel);
             if (rel <= 1e-3f) atomicAdd(&stats[5], 1u);
+            if (ok) {
+                atomicAdd(&stats[6], 1u);
+                atomicMax(&stats[7], __float_as_uint(rel));
+            }
         }
         if (!ok) {
             atomicAdd(&stats[1], 1u);

@@ -154,3 +154,36 @@ def build(domain: Domain, device="cuda:0", **extra):
     args = domain.args(**extra)
     return build_states(args, domain.x, domain.vol, domain.props, device=device, dx=domain.dx,
                         minBounds=domain.minBounds, gridDims=domain.gridDims, adjust_dt=False)
+
+
+def seed_plastic_trials(sim, mpm, seed=3, emin=1e-6, emax=1e-1):
+    """Overwrite a built scene's trial state with the learned-return-map
+    benchmark's distributions (in place, on the device): per particle a trial
+    log strain of magnitude log-uniform in [emin, emax] along a uniformly
+    random direction of principal values, in a uniformly random principal
+    frame (F_trial = Q diag(exp(e)) Q^T), a friction angle U(20, 45) deg ->
+    alpha, a cohesion log-uniform in [0.1, 5] MPa -> ys and a damage U(0, 1).
+    mu, lam and the rest of the scene stay.  Returns the number of particles."""
+    import torch
+    dev = mpm.particle_F_trial.device
+    n = sim.nPoints
+    g = torch.Generator(device=dev).manual_seed(int(seed))
+    u = lambda *shape: torch.rand(*shape, generator=g, device=dev, dtype=torch.float64)  # noqa: E731
+    mag = torch.exp(math.log(emin) + (math.log(emax) - math.log(emin)) * u(n))
+    d = torch.randn(n, 3, generator=g, device=dev, dtype=torch.float64)
+    e = mag[:, None] * d / d.norm(dim=1, keepdim=True).clamp_min(1e-300)
+    q = torch.randn(n, 4, generator=g, device=dev, dtype=torch.float64)
+    q = q / q.norm(dim=1, keepdim=True)
+    w, x, y, z = q.unbind(1)
+    Q = torch.stack([1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y),
+                     2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x),
+                     2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)], 1).view(n, 3, 3)
+    F = Q @ torch.diag_embed(torch.exp(e)) @ Q.transpose(1, 2)
+    mpm.particle_F_trial = F.to(torch.float32)
+    phi = 20.0 + 25.0 * u(n)
+    s = torch.sin(torch.deg2rad(phi))
+    # in place: the library holds pointers to these arrays
+    mpm.alpha.copy_(2.0 * s / (math.sqrt(3.0) * (3.0 - s)))
+    mpm.ys.copy_(torch.exp(math.log(0.1e6) + (math.log(5e6) - math.log(0.1e6)) * u(n)))
+    mpm.particle_damage.copy_(u(n))
+    return n

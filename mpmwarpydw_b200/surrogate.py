@@ -7,7 +7,8 @@ It is trained on the GPU by the library's own kernels: labelled samples from
 the plain return map (``mpmw_dp_samples``), forward/backward in FP32 with the
 weights rounded to BF16 (``mpmw_mlp_grad``), Adam (``mpmw_mlp_adam``).
 Inference runs on the tensor cores (``mpmw_mlp_infer_tc``: tcgen05.mma with
-BF16 operands and FP32 accumulation in tensor memory).
+BF16 weights, each hidden-layer input split into hi + lo BF16 terms, FP32
+accumulation in tensor memory; the last layer in FP32).
 """
 from __future__ import annotations
 
@@ -92,7 +93,7 @@ class ReturnMapSurrogate:
         return self.packed
 
     def infer(self, x, out=None):
-        """Tensor-core inference (tcgen05, BF16 operands, FP32 accumulation)."""
+        """Tensor-core inference (tcgen05, BF16 weights, split BF16 activations, FP32 accumulation)."""
         packed = self.pack()
         y = out if out is not None else torch.empty(x.shape[0], _lib.MLP_OUT, dtype=torch.float32, device=x.device)
         st = status_word(x.device)
@@ -113,11 +114,11 @@ def compute_stress(sim, mpm, xpbd, net: ReturnMapSurrogate, gate_tol: float = 1e
                    audit_seed: int = 0, stats=None):
     """The stress phase (compute_stress_from_F_trial) with the surrogate for
     plastic returns: gate, audit and exact fallback as mpmw_stress_surrogate.
-    Returns the (6,) int32 device stats (see :func:`stats_summary`),
+    Returns the (8,) int32 device stats (see :func:`stats_summary`),
     accumulated into ``stats``."""
     dev = sim.device
     if stats is None:
-        stats = torch.zeros(6, dtype=torch.int32, device=dev)
+        stats = torch.zeros(_lib.SURR_NSTATS, dtype=torch.int32, device=dev)
     n = sim.nPoints
     need = int(_lib.lib().mpmw_surrogate_workspace_bytes(n))
     ws = getattr(mpm, "_mpmw_surr_ws", None)
@@ -137,11 +138,12 @@ def compute_stress(sim, mpm, xpbd, net: ReturnMapSurrogate, gate_tol: float = 1e
 
 def stats_summary(stats) -> dict:
     """[candidates, fallbacks, audited, largest audited relative stress error,
-    sum of audited relative errors, audited within 1e-3] as a dict."""
+    sum of audited relative errors, audited within 1e-3, audited and accepted,
+    largest audited relative stress error among the accepted] as a dict."""
     import struct
     s = [v & 0xFFFFFFFF for v in stats.detach().cpu().to(torch.int64).tolist()]
     f = lambda u: struct.unpack("<f", struct.pack("<I", u))[0]  # noqa: E731
     aud = s[2]
     return {"candidates": s[0], "fallbacks": s[1], "accepted": s[0] - s[1], "audited": aud,
             "audit_max_rel_err": f(s[3]), "audit_mean_rel_err": f(s[4]) / aud if aud else 0.0,
-            "audit_within_1e-3": s[5]}
+            "audit_within_1e-3": s[5], "audited_accepted": s[6], "accepted_audit_max_rel_err": f(s[7])}

@@ -4,9 +4,11 @@ MLP kernels; the product never imports it).
 
 Same definitions as include/mpmw_mlp.h: 8 -> 64 -> 64 -> 64 -> 4, SiLU after the
 hidden layers, parameters packed W1 b1 W2 b2 W3 b3 W4 b4 (W[out][in]); the
-weights are rounded to BF16 (round to nearest even) before use, the biases are
-not.  ``bf16_activations=True`` also rounds every layer input to BF16, which
-is what the tensor-core inference kernel feeds its MMAs.
+hidden layers' weights W1..W3 are rounded to BF16 (round to nearest even)
+before use, W4 and the biases are not.  ``split_activations=True`` rounds the
+inputs of the three hidden layers to the sum of two BF16 terms (hi = bf16(a),
+lo = bf16(a - hi)), which is what the tensor-core inference kernel feeds its
+MMAs.  :func:`targets` restates the sample labels (the radial return's ratios).
 """
 from __future__ import annotations
 
@@ -37,22 +39,31 @@ def _silu(z):
     return z * s, s * (1.0 + z * (1.0 - s))
 
 
-def forward(p, x, bf16_activations=False):
+def split_round(a):
+    """a as the sum of its two BF16 terms hi = bf16(a), lo = bf16(a - hi)."""
+    a32 = np.asarray(a, np.float32)
+    hi = bf16_round(a32)
+    lo = bf16_round((a32.astype(np.float64) - hi).astype(np.float32))
+    return hi + lo
+
+
+def forward(p, x, split_activations=False):
     """Outputs and the cache for backward."""
     P = unpack(p)
-    W = {k: bf16_round(P[k].astype(np.float32)) for k in ("W1", "W2", "W3", "W4")}
-    r = bf16_round if bf16_activations else (lambda a: np.asarray(a, np.float64))
+    W = {k: bf16_round(P[k].astype(np.float32)) for k in ("W1", "W2", "W3")}
+    W["W4"] = P["W4"].astype(np.float32).astype(np.float64)
+    r = split_round if split_activations else (lambda a: np.asarray(a, np.float64))
     a0 = r(np.asarray(x, np.float32))
     z1 = a0 @ W["W1"].T + P["b1"]; a1, d1 = _silu(z1)
     z2 = r(a1) @ W["W2"].T + P["b2"]; a2, d2 = _silu(z2)
     z3 = r(a2) @ W["W3"].T + P["b3"]; a3, d3 = _silu(z3)
-    out = r(a3) @ W["W4"].T + P["b4"]
+    out = a3 @ W["W4"].T + P["b4"]
     return out, (a0, a1, a2, a3, d1, d2, d3, W)
 
 
 def loss_and_grad(p, x, y):
     """mean((out - y)^2) over all entries and its gradient (straight-through
-    through the BF16 rounding of the weights), packed like p."""
+    through the BF16 rounding of the hidden layers' weights), packed like p."""
     out, (a0, a1, a2, a3, d1, d2, d3, W) = forward(p, x)
     r = out - np.asarray(y, np.float64)
     n = r.size
@@ -86,3 +97,20 @@ def dp_return_principal(e, mu, lam, ys, alpha, beta, D):
     edn = np.sqrt(np.sum(ed * ed)) + 1e-6
     dg = edn - ye / (2.0 * mu)
     return e - (dg / edn) * ed + beta * dg, np.sqrt(2.0 / 3.0) * dg
+
+
+def targets(e, mu, lam, ys, alpha, beta, D):
+    """The sample labels of one plastic trial (include/mpmw_mlp.h): (ln rho,
+    ln(1 - rho), beta, sqrt(2/3)) with rho = yield / (2 mu |dev e|), and the
+    return they encode, e_ret = e + (rho n / (n + 1e-6) - 1) dev e + beta dgamma,
+    dgamma = n (1 - rho) + 1e-6, which equals dp_return_principal's."""
+    e = np.asarray(e, np.float64)
+    tr = e.sum()
+    ed = e - tr / 3.0
+    n = np.sqrt(np.sum(ed * ed))
+    p = (2.0 * mu / 3.0 + lam) * tr
+    rho = (1.0 - D) * (ys - alpha * p) / (2.0 * mu * n)
+    y = np.array([np.log(rho), max(np.log1p(-rho), -12.0), beta, np.sqrt(2.0 / 3.0)])
+    dg = n * (1.0 - rho) + 1e-6
+    e_ret = e + (rho * n / (n + 1e-6) - 1.0) * ed + beta * dg
+    return y, e_ret, np.sqrt(2.0 / 3.0) * dg

@@ -49,7 +49,7 @@ _I = ctypes.c_int
 
 
 class Oracle:
-    """One precision of the oracle: 'f32', 'f64' or 'f32_omp' (OpenMP)."""
+    """One precision of the oracle: 'f32', 'f64', 'f32_omp' or 'f64_omp' (OpenMP)."""
 
     def __init__(self, prec: str = "f64"):
         path = os.path.join(_BUILD, f"libmpm_oracle_{prec}.so")
@@ -57,8 +57,8 @@ class Oracle:
             build()
         self.lib = ctypes.CDLL(path)
         self.prec = prec
-        self.dtype = np.float64 if prec == "f64" else np.float32
-        self.R = ctypes.c_double if prec == "f64" else ctypes.c_float
+        self.dtype = np.float64 if prec.startswith("f64") else np.float32
+        self.R = ctypes.c_double if prec.startswith("f64") else ctypes.c_float
         assert self.lib.orc_real_bytes() == np.dtype(self.dtype).itemsize
 
     # -- argument helpers ---------------------------------------------------

@@ -1,0 +1,160 @@
+"""Parity at the benchmark configurations' full sizes.
+
+* The Drucker-Prager block collapse (64,000 particles, 40^3 lattice at 0.25 m,
+  grid 40^3 at dx 0.5, dt 1e-4) for 1,000 fused substeps against the FP64 and
+  FP32 oracles run the same 1,000 reference-order steps: total mass, momentum
+  and the damaged-volume fraction.
+* The tunnel (3,873,600 particles, grid 120 x 70 x 120, geostatic pre-stress)
+  after one substep of the drop-in mpmSimulationStep, per particle against the
+  oracles with the one-step rules of the small-scene tests, and after two
+  fused substeps (G2P, return map and P2G in one kernel at full size).
+
+The oracles are the OpenMP builds (oracle/Makefile); the steps follow
+utils/simulationRoutines.py:6-293.
+"""
+import time
+
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from tests.harness import close_to_either, gpu_fields, oracle, rel_err, stress_parity_violation, to_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _momentum(m, v):
+    return (np.asarray(m, np.float64)[:, None] * np.asarray(v, np.float64)).sum(0)
+
+
+def _damaged_fraction(vol, D, act):
+    vol = np.asarray(vol, np.float64)
+    return float(vol[act & (np.asarray(D) >= 1.0)].sum() / vol[act].sum())
+
+
+def test_block_collapse_64k_1000_steps():
+    """1,000 fused substeps of the 64,000-particle block collapse.
+
+    Total mass is exact (no particle changes mass or leaves the grid; the grid
+    mass after the last P2G agrees to FP32 summation order).  Momentum and the
+    damaged-volume fraction are compared with the FP64 oracle beside the FP32
+    oracle's own distance from FP64 on the same 1,000 steps: FP32 rounding,
+    amplified by the block's ringing on the frictional floor, sets that floor,
+    so the GPU is held to max(1e-3, 2 x the FP32 oracle's distance)."""
+    import torch
+
+    from mpmwarpydw_b200 import domains
+    from mpmwarpydw_b200.bind import read_status
+    from mpmwarpydw_b200.engine import sort_particles
+    from mpmwarpydw_b200.utils import simulationRoutines as S
+    nsteps = 1000
+    d = domains.block_collapse()
+    sim, mpm, xpbd = domains.build(d, device="cuda:0")
+    sort_particles(sim, mpm, xpbd)
+    assert sim.nPoints == 64000
+    s32 = to_oracle(sim, mpm, xpbd)
+    s64 = to_oracle(sim, mpm, xpbd, np.float64)
+    read_status(sim.device)
+    S.run_mpm_substeps(sim, mpm, xpbd, nsteps)
+    torch.cuda.synchronize()
+    assert read_status(sim.device) == 0
+    t = time.time()
+    for s, prec in ((s32, "f32_omp"), (s64, "f64_omp")):
+        o = oracle(prec)
+        for _ in range(nsteps):
+            orc.mpm_step(o, s)
+    g = gpu_fields(sim, mpm, xpbd)
+    m = s64.particle_mass
+    act = (s64.activeLabel == 1) & (s64.materialLabel <= 1)
+    act_g = (g["activeLabel"] == 1) & (g["materialLabel"] <= 1)
+    mg, m32, m64 = _momentum(m, g["particle_v"]), _momentum(m, s32.particle_v), _momentum(m, s64.particle_v)
+    scale = float(np.linalg.norm(m64))
+    e_gpu, e_32 = float(np.linalg.norm(mg - m64)) / scale, float(np.linalg.norm(m32 - m64)) / scale
+    fg = _damaged_fraction(s64.particle_vol, g["particle_damage"], act_g)
+    f32 = _damaged_fraction(s64.particle_vol, s32.particle_damage, (s32.activeLabel == 1) & (s32.materialLabel <= 1))
+    f64 = _damaged_fraction(s64.particle_vol, s64.particle_damage, act)
+    yielded = [int((a > 0).sum()) for a in (g["particle_accumulated_strain"], s32.particle_accumulated_strain,
+                                            s64.particle_accumulated_strain)]
+    print(f"block collapse 64k, {nsteps} steps (oracles {time.time() - t:.0f} s): momentum rel. to FP64 "
+          f"GPU {e_gpu:.2e}, FP32 oracle {e_32:.2e}; |p| {scale:.4e}; damaged-volume fraction GPU {fg:.4e} "
+          f"FP32 {f32:.4e} FP64 {f64:.4e}; yielded particles GPU/FP32/FP64 {yielded}; "
+          f"x rel. to FP64 GPU {rel_err(g['particle_x'], s64.particle_x):.2e} "
+          f"FP32 {rel_err(s32.particle_x, s64.particle_x):.2e}")
+    # total mass: exact per particle, and the grid's after the last P2G to summation order
+    assert np.array_equal(act_g, act)
+    assert float(np.asarray(sim.particle_mass.cpu().numpy(), np.float64)[act].sum()) == float(m[act].sum())
+    assert abs(g["grid_m"].sum() - s64.grid_m.sum()) <= 1e-5 * s64.grid_m.sum()
+    assert e_gpu <= max(1e-3, 2.0 * e_32)
+    assert abs(fg - f64) <= max(1e-3, 2.0 * abs(f32 - f64))
+    ex_gpu, ex_32 = rel_err(g["particle_x"], s64.particle_x), rel_err(s32.particle_x, s64.particle_x)
+    assert ex_gpu <= max(1e-5, 2.0 * ex_32), (ex_gpu, ex_32)
+
+
+def _tunnel():
+    from mpmwarpydw_b200 import domains
+    from mpmwarpydw_b200.engine import sort_particles
+    d = domains.tunnel()
+    sim, mpm, xpbd = domains.build(d, device="cuda:0")
+    sort_particles(sim, mpm, xpbd)
+    assert sim.nPoints == 3_873_600
+    return sim, mpm, xpbd
+
+
+def test_tunnel_full_size_one_substep():
+    """One drop-in mpmSimulationStep of the 3,873,600-particle tunnel against
+    the FP32 and FP64 oracles: stress per particle by the stress parity rule,
+    labels and F per particle, grid and G2P outputs within 1e-5 (array-relative,
+    of either oracle)."""
+    import torch
+
+    from mpmwarpydw_b200.bind import read_status
+    from mpmwarpydw_b200.utils import simulationRoutines as S
+    sim, mpm, xpbd = _tunnel()
+    s32 = to_oracle(sim, mpm, xpbd)
+    s64 = to_oracle(sim, mpm, xpbd, np.float64)
+    mu0 = s32.mu.astype(np.float64)
+    read_status(sim.device)
+    S.mpmSimulationStep(sim, mpm, xpbd, "cuda:0")
+    torch.cuda.synchronize()
+    assert read_status(sim.device) == 0
+    orc.mpm_step(oracle("f32_omp"), s32)
+    orc.mpm_step(oracle("f64_omp"), s64)
+    g = gpu_fields(sim, mpm, xpbd)
+    lab_ok = (g["materialLabel"] == s32.materialLabel) | (g["materialLabel"] == s64.materialLabel)
+    assert lab_ok.all()
+    v = stress_parity_violation(g["particle_stress"], s32.particle_stress, s64.particle_stress, 2.0 * mu0)
+    assert v <= 1.0, v
+    ok, bad = close_to_either(g["particle_F"], s32.particle_F, s64.particle_F, rtol=0, atol=2e-6)
+    assert ok, ("F", bad)
+    errs = {}
+    for k in ("grid_m", "grid_v_in", "grid_v_out", "particle_x", "particle_v", "particle_C", "particle_F_trial"):
+        errs[k] = min(rel_err(g[k], getattr(s32, k)), rel_err(g[k], getattr(s64, k)))
+    print("tunnel one substep, array-relative error vs the nearer oracle:", {k: f"{e:.1e}" for k, e in errs.items()})
+    for k, e in errs.items():
+        assert e <= 1e-5, (k, e)
+
+
+def test_tunnel_full_size_two_fused_substeps():
+    """Two substeps of the tunnel through mpmw_run_substeps (the second one's
+    G2P, return map and P2G in the fused kernel at full size) against two FP64
+    oracle steps, with the fused-run tolerances: x 1e-5, v and C 1e-4, stress
+    1e-3 (array-relative)."""
+    import torch
+
+    from mpmwarpydw_b200.bind import read_status
+    from mpmwarpydw_b200.utils import simulationRoutines as S
+    sim, mpm, xpbd = _tunnel()
+    s64 = to_oracle(sim, mpm, xpbd, np.float64)
+    read_status(sim.device)
+    S.run_mpm_substeps(sim, mpm, xpbd, 2)
+    torch.cuda.synchronize()
+    assert read_status(sim.device) == 0
+    o = oracle("f64_omp")
+    for _ in range(2):
+        orc.mpm_step(o, s64)
+    g = gpu_fields(sim, mpm, xpbd)
+    assert np.array_equal(g["materialLabel"], s64.materialLabel)
+    errs = {k: rel_err(g[k], getattr(s64, k)) for k in ("particle_x", "particle_v", "particle_C", "particle_stress")}
+    print("tunnel two fused substeps, array-relative error vs FP64:", {k: f"{e:.1e}" for k, e in errs.items()})
+    for k, tol in (("particle_x", 1e-5), ("particle_v", 1e-4), ("particle_C", 1e-4), ("particle_stress", 1e-3)):
+        assert errs[k] <= tol, (k, errs[k])

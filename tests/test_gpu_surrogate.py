@@ -45,10 +45,10 @@ def test_gradient_matches_cpu():
         assert _rel(g[off:off + n], g_ref[off:off + n]) <= 1e-4, name
 
 
-def test_tensor_core_inference_matches_bf16_emulation():
-    """tcgen05 MMA path (BF16 operands, FP32 accumulate) against the same
-    network with every layer input rounded to BF16 on the CPU; and within the
-    BF16 envelope of the FP32 forward."""
+def test_tensor_core_inference_matches_split_emulation():
+    """tcgen05 MMA path (BF16 weights, every hidden-layer input fed as hi + lo
+    BF16 terms, FP32 accumulate, FP32 last layer) against the same network
+    with that rounding emulated on the CPU, and against the FP32 forward."""
     import torch
     net = _net(3)
     x, _ = net.samples(1000, 13)          # 7 full 128-row tiles and a partial one
@@ -57,50 +57,117 @@ def test_tensor_core_inference_matches_bf16_emulation():
     torch.cuda.synchronize()
     from mpmwarpydw_b200.bind import read_status
     assert read_status(x.device) == 0
-    emu, _ = M.forward(net.params.cpu().numpy(), x.cpu().numpy(), bf16_activations=True)
+    emu, _ = M.forward(net.params.cpu().numpy(), x.cpu().numpy(), split_activations=True)
     a = y_tc.cpu().numpy()
     assert np.all(np.isfinite(a))
-    assert _rel(a, emu) <= 1e-2
-    assert float(np.mean(np.abs(a - emu))) <= 1e-3 * float(np.mean(np.abs(emu)))
-    assert _rel(a, y32.cpu().numpy()) <= 5e-2
+    assert _rel(a, emu) <= 1e-4
+    assert _rel(a, y32.cpu().numpy()) <= 1e-4
 
 
 def test_samples_satisfy_radial_return_identities():
-    """Targets of a radial return: the deviatoric part of e_ret - e is
-    anti-parallel to dev e, and its trace is 3 beta dgamma with
-    dgamma = d_acc / sqrt(2/3)."""
+    """Targets of a radial return: y[2] is the dilation beta (feature 5), y[3]
+    is sqrt(2/3), rho + (1 - rho) = 1, and ln rho is the ratio the features
+    define: (1 - D)(10^-f3 - alpha (1/3 + nu/(1 - 2 nu)) tr(e/|e|)) / |dev e/|e||."""
     import torch
     net = _net(4)
     x, y = net.samples(20000, 14)
     torch.cuda.synchronize()
     x, y = x.cpu().numpy().astype(np.float64), y.cpu().numpy().astype(np.float64)
+    assert np.all(np.isfinite(y))
+    assert np.max(np.abs(y[:, 2] - x[:, 5])) <= 1e-7
+    assert np.max(np.abs(y[:, 3] - np.sqrt(2.0 / 3.0))) <= 1e-7
+    rho = np.exp(y[:, 0])
+    assert np.all((rho > 0) & (rho < 1))
+    far = y[:, 1] > -12.0 + 1e-6          # targets not clamped at the floor
+    assert np.max(np.abs(rho + np.exp(y[:, 1]) - 1.0)[far]) <= 1e-5
     d = x[:, :3]
     dd = d - d.mean(1, keepdims=True)
-    de = y[:, :3]
-    dde = de - de.mean(1, keepdims=True)
-    plastic = y[:, 3] > 0
-    assert plastic.mean() > 0.99
-    cos = np.sum(dd * dde, 1) / (np.linalg.norm(dd, axis=1) * np.linalg.norm(dde, axis=1) + 1e-30)
-    assert np.all(cos[plastic] < -0.999)
-    beta = x[:, 5]
-    tr = de.sum(1)
-    expect = 3.0 * beta * y[:, 3] / np.sqrt(2.0 / 3.0)
-    assert np.max(np.abs(tr - expect)[plastic]) <= 1e-5 * (np.max(np.abs(expect)) + 1e-6)
+    nu = x[:, 7]
+    c = 1.0 / 3.0 + nu / (1.0 - 2.0 * nu)
+    rho_f = np.exp(x[:, 6]) * (10.0 ** (-x[:, 3]) - x[:, 4] * c * d.sum(1)) / np.linalg.norm(dd, axis=1)
+    assert np.median(np.abs(np.log(rho_f) - y[:, 0])) <= 1e-5
+    assert np.quantile(np.abs(np.log(rho_f) - y[:, 0]), 0.99) <= 1e-3
 
 
-def test_training_gain():
-    """What training gains: validation error of the trained network against
-    the same network untrained, on fresh samples (printed)."""
+def _stress_phase_compare(net, n_side=60, seed=31):
+    """The plain stress phase (mpmw_stress) and the surrogate's on the same
+    seeded plastic trial state (config 3's distributions): (plain stress,
+    surrogate stress, plastic mask, stats summary, ms plain, ms surrogate,
+    particles whose material label differs between the two)."""
+    import torch
+
+    from mpmwarpydw_b200 import _lib, domains
+    from mpmwarpydw_b200.bind import params_from_states, particles_from_states, status_word, stream_handle
+    from mpmwarpydw_b200.surrogate import compute_stress, stats_summary
+    d = domains.block_collapse(n_side=n_side, spacing=0.25, seed=seed)
+    sim, mpm, xpbd = domains.build(d, device="cuda:0")
+    domains.seed_plastic_trials(sim, mpm, seed=seed, emax=1e-2)
+    fields = [mpm._s_particle_F, mpm._s_particle_stress, mpm._s_particle_accumulated_strain,
+              mpm._s_particle_damage, mpm._s_ys, mpm._s_mu, mpm._s_lam, mpm._s_alpha,
+              sim._s_materialLabel, sim._s_particle_v]
+    snap = [t.clone() for t in fields]
+    acc0 = mpm._s_particle_accumulated_strain.clone()
+
+    def restore():
+        for t, s0 in zip(fields, snap):
+            t.copy_(s0)
+
+    L = _lib.lib()
+    P, prm = particles_from_states(sim, mpm, xpbd), params_from_states(sim, mpm)
+    st = status_word("cuda:0")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record()
+    _lib.check(L.mpmw_stress(P, prm, st.data_ptr(), stream_handle()), "stress")
+    ev[1].record()
+    torch.cuda.synchronize()
+    plain = mpm._s_particle_stress.clone()
+    lab_plain = sim._s_materialLabel.clone()
+    plastic = (mpm._s_particle_accumulated_strain > acc0) & (sim._s_materialLabel <= 1)
+    restore()
+    stats = torch.zeros(_lib.SURR_NSTATS, dtype=torch.int32, device="cuda:0")
+    ev[2].record()
+    compute_stress(sim, mpm, xpbd, net, gate_tol=1e-3, audit=1.0, audit_seed=5, stats=stats)
+    ev[3].record()
+    torch.cuda.synchronize()
+    surr = mpm._s_particle_stress.clone()
+    flipped = sim._s_materialLabel != lab_plain
+    return (plain, surr, plastic & ~flipped, stats_summary(stats), ev[0].elapsed_time(ev[1]),
+            ev[2].elapsed_time(ev[3]), int(flipped.sum()))
+
+
+def test_surrogate_against_plain_return_map():
+    """What the trained network gains over the method without it.  On 216,000
+    seeded plastic trial states (config 3's distributions, |e| up to 1e-2, the
+    tensor form's range), the stress phase runs with the plain return map and
+    with the surrogate (gate 1e-3, every return audited):
+      - untrained, the gate rejects every surrogate return (all fall back);
+      - trained, the gate accepts returns, every accepted and audited return
+        is within 1e-3 (relative stress error against the exact return), and
+        the stress over the plastic particles is within 1e-3 norm-wise of the
+        plain path's (particles whose phase-transition label differs, a damage
+        threshold reached with the predicted increment, are counted apart:
+        at most 0.1 % of the candidates);
+    the times of both phases are printed (the plain map is a closed form of a
+    few dozen FLOPs; the network costs 17,920 per candidate)."""
     import torch
     net = _net(5)
-    x, y = net.samples(1_000_000, 15)
-    xv, yv = net.samples(50_000, 16)
-    l0 = float(((net.infer(xv) - yv) ** 2).mean().item())
-    losses = net.train(x, y, steps=1500, batch=8192)
-    torch.cuda.synchronize()
-    l1 = float(((net.infer(xv) - yv) ** 2).mean().item())
-    print(f"surrogate validation MSE: untrained {l0:.3e}, trained {l1:.3e} (train loss {losses[0]:.2e} -> {losses[-1]:.2e})")
-    assert l1 <= 1e-2 * l0
+    st0 = _stress_phase_compare(net)[3]
+    x, y = net.samples(4_000_000, 15)
+    losses = net.train(x, y, steps=20000, batch=16384)
+    del x, y
+    plain, surr, plastic, st1, ms_p, ms_s, flipped = _stress_phase_compare(net)
+    d = (surr - plain)[:, plastic].double()
+    err = float(torch.linalg.norm(d) / torch.linalg.norm(plain[:, plastic].double()))
+    print(f"untrained: {st0}\ntrained (loss {losses[0]:.2e} -> {losses[-1]:.2e}): {st1}\n"
+          f"plastic particles {int(plastic.sum())}, label differences {flipped}, stress error vs plain {err:.2e}, "
+          f"stress phase plain {ms_p:.3f} ms, surrogate {ms_s:.3f} ms")
+    assert st0["candidates"] > 10000 and st0["accepted"] == 0
+    assert st1["candidates"] == st0["candidates"]
+    assert st1["accepted"] > 0
+    assert st1["audited_accepted"] == st1["accepted"]
+    assert st1["accepted_audit_max_rel_err"] <= 1e-3
+    assert flipped <= max(1, st1["candidates"] // 1000)
+    assert err <= 1e-3
 
 
 def test_surrogate_stress_phase_vs_fp64_oracle():
@@ -115,8 +182,8 @@ def test_surrogate_stress_phase_vs_fp64_oracle():
     from mpmwarpydw_b200.surrogate import ReturnMapSurrogate, compute_stress, stats_summary
     from tests.harness import gpu_fields, oracle, small_scene, to_oracle
     net = ReturnMapSurrogate("cuda:0", seed=6)
-    x, y = net.samples(2_000_000, 17)
-    net.train(x, y, steps=6000, batch=16384)
+    x, y = net.samples(4_000_000, 17)
+    net.train(x, y, steps=20000, batch=16384)
     sim, mpm, xpbd = small_scene(seed=21)
     s64 = to_oracle(sim, mpm, xpbd, np.float64)
     stats = compute_stress(sim, mpm, xpbd, net, gate_tol=1e-3, audit=1.0, audit_seed=3)
@@ -138,5 +205,7 @@ def test_surrogate_stress_phase_vs_fp64_oracle():
     print(f"surrogate stress phase: {st}, plastic particles {int(mpm_now.sum())}, "
           f"norm-wise stress error vs FP64 {err:.2e}, label mismatches {mism}")
     assert st["candidates"] > 50
+    assert st["accepted"] > 0
+    assert st["accepted_audit_max_rel_err"] <= 1e-3
     assert err <= 1e-3
     assert mism <= max(1, st["candidates"] // 100)

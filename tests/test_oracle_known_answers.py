@@ -167,3 +167,34 @@ def test_hash_grid_restatement():
     for c in np.unique(h):
         ids = hg.point_ids[hg.cell_starts[c]:hg.cell_ends[c]]
         assert np.all(h[ids] == c) and np.all(np.diff(ids) > 0)
+
+
+def test_surrogate_targets_encode_the_radial_return():
+    """The network's targets (ln rho, ln(1 - rho), beta, sqrt(2/3)) decoded as
+    the stress phase decodes them give the reference's principal-space return
+    (utils/mpmRoutines.py:339-453) to FP64 rounding, over seeded plastic trials."""
+    from oracle import mlp_oracle as M
+    rng = np.random.default_rng(7)
+    checked = 0
+    for _ in range(2000):
+        mag = 10.0 ** rng.uniform(-6, -1)
+        g = rng.standard_normal(3)
+        e = np.sort(mag * g / np.linalg.norm(g))[::-1]
+        E, nu = 1e9 * 50.0 ** rng.uniform(), rng.uniform(0.15, 0.35)
+        mu, lam = E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu))
+        ys, D = 1e5 * 50.0 ** rng.uniform(), rng.uniform(0, 0.999)
+        s = np.sin(np.radians(rng.uniform(20, 45)))
+        alpha = 2 * s / (np.sqrt(3) * (3 - s))
+        beta = 0.3 * alpha
+        ref = M.dp_return_principal(e, mu, lam, ys, alpha, beta, D)
+        tr = e.sum()
+        if ref is None or (1 - D) * (ys - alpha * (2 * mu / 3 + lam) * tr) <= 0:
+            continue
+        y, e_ret, dacc = M.targets(e, mu, lam, ys, alpha, beta, D)
+        if y[1] <= -12.0:
+            continue
+        assert np.allclose(e_ret, ref[0], rtol=0, atol=1e-12 * max(1.0, np.abs(e).max() / 1e-6) * 1e-6 + 1e-15)
+        assert abs(dacc - ref[1]) <= 1e-9 * abs(ref[1]) + 1e-18
+        assert y[2] == beta and abs(y[3] - np.sqrt(2 / 3)) == 0.0
+        checked += 1
+    assert checked > 500
