@@ -223,6 +223,23 @@ int mpmw_batch_run_substeps(const mpmw_particles_t *p, int nsteps, uint32_t *sta
 int mpmw_batch_run_range(const mpmw_particles_t *p, int first_scene, int last_scene, int nsteps, uint32_t *status,
                          void *workspace, size_t ws_bytes, mpmw_stream_t stream);
 
+/* ---- particle order ------------------------------------------------------ */
+/* No counterpart in the reference (its kernels do not depend on particle
+ * order, utils/mpmRoutines.py:485-569).  perm[n] receives the stable order of
+ * the particles by block key: each particle's stencil base cell
+ * int((x - min_bounds) inv_dx - 0.5) per axis (utils/mpmRoutines.py:514-517),
+ * clamped to the grid `dims`, grouped in blocks of block^3 cells -- key =
+ * (block index, C order) * block^3 + (cell within the block, C order) -- by
+ * the library's stable LSD radix sort.  Position i of the sorted order holds
+ * particle perm[i].  x is [3][n] SoA; prm supplies min_bounds and inv_dx.
+ * Gathering every particle field through perm keeps the particles a CTA of
+ * the scatter and gather kernels holds within a few cells.  Needs
+ * mpmw_block_sort_workspace_bytes(n) of workspace; the number of keys must
+ * stay below 2^31. */
+size_t mpmw_block_sort_workspace_bytes(int64_t n);
+int mpmw_block_sort(const float *x, int64_t n, const mpmw_params_t *prm, const int32_t *dims, int block,
+                    int32_t *perm, void *workspace, size_t ws_bytes, mpmw_stream_t stream);
+
 /* utils/mpmRoutines.py:1446-1475 deactivate_and_teleport_xpbd_below_datum */
 int mpmw_teleport(const mpmw_particles_t *p, float z_datum, float teleport_distance, mpmw_stream_t stream);
 /* utils/mpmRoutines.py:3-21 creep_by_damage_with_baseline */

@@ -140,6 +140,9 @@ _SIGS = {
     "mpmw_surrogate_workspace_bytes": (ctypes.c_size_t, [_I64]),
     "mpmw_stress_surrogate": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Params), _P, _P, _F, _I,
                                    ctypes.c_uint64, _P, _P, _P, ctypes.c_size_t, _P]),
+    "mpmw_block_sort_workspace_bytes": (ctypes.c_size_t, [_I64]),
+    "mpmw_block_sort": (_I, [_P, _I64, ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_int32), _I, _P, _P,
+                             ctypes.c_size_t, _P]),
     "mpmw_hash_workspace_bytes": (ctypes.c_size_t, [_I64]),
     "mpmw_xpbd_step_workspace_bytes": (ctypes.c_size_t, [_I64, ctypes.POINTER(ctypes.c_int32)]),
     "mpmw_hash_build": (_I, [_P, _I64, ctypes.POINTER(Hash), _P, ctypes.c_size_t, _P]),

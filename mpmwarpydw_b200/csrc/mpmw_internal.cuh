@@ -18,6 +18,9 @@ size_t g2p_workspace_bytes(int64_t n);
 int launch_stress_p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st,
                       void *ws, size_t ws_bytes, cudaStream_t s);
 size_t hash_workspace_bytes(int64_t n);
+size_t block_sort_workspace_bytes(int64_t n);
+int block_sort(const float *x, int64_t n, const mpmw_params_t &prm, const int32_t *dims, int block, int32_t *perm,
+               void *ws, size_t ws_bytes, cudaStream_t s);
 int reserve_fused_smem();
 size_t batch_workspace_bytes(const mpmw_grid_t *grids, int nscenes, int64_t n);
 int prepare_batch(const mpmw_particles_t &p, const mpmw_grid_t *grids, const mpmw_params_t *prms,

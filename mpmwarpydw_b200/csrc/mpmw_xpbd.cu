@@ -153,6 +153,101 @@ size_t hash_workspace_bytes(int64_t n)
     return (size_t)(al(4 * n) * 3 + al(4 * hist) * 2 + al(4 * scan_scratch));
 }
 
+// Stable LSD radix sort of the (key, id) pairs in keys_a / ids_a over the low
+// `bits` bits of the keys, with the workspace carved as hash_workspace_bytes
+// lays it out after those two arrays; returns the arrays that hold the sorted
+// pairs (either the a or the b buffers) in *keys_out / *ids_out.
+static int radix_sort_pairs(int *keys_a, int *ids_a, int64_t n, int bits, char *w, int **keys_out, int **ids_out,
+                            cudaStream_t s)
+{
+    auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
+    const int64_t nt = sort_tiles(n), hist_n = (int64_t)kRadix * nt;
+    int *keys_b = reinterpret_cast<int *>(w); w += al(4 * n);
+    int *ids_b = reinterpret_cast<int *>(w); w += al(4 * n);
+    int *hist = reinterpret_cast<int *>(w); w += al(4 * hist_n);
+    int *offs = reinterpret_cast<int *>(w); w += al(4 * hist_n);
+    int *scr = reinterpret_cast<int *>(w);
+    int *ki = keys_a, *vi = ids_a, *ko = keys_b, *vo = ids_b;
+    for (int shift = 0; shift < bits; shift += kRadixBits) {
+        k_radix_hist<<<(unsigned)nt, kSortThreads, 0, s>>>(ki, n, shift, (int)nt, hist);
+        MPMW_TRY_LAUNCH("k_radix_hist");
+        if (!exclusive_scan(hist, offs, hist_n, scr, s)) { set_error("radix sort: too many items"); return MPMW_E_ARG; }
+        MPMW_TRY_LAUNCH("scan");
+        k_radix_scatter<<<(unsigned)nt, kSortThreads, 0, s>>>(ki, vi, n, shift, (int)nt, offs, ko, vo);
+        MPMW_TRY_LAUNCH("k_radix_scatter");
+        int *t = ki; ki = ko; ko = t;
+        t = vi; vi = vo; vo = t;
+    }
+    *keys_out = ki;
+    *ids_out = vi;
+    return MPMW_OK;
+}
+
+// Key of the 4x4x4-cell block order (block = edge in cells): the particle's
+// stencil base cell int((x - min_bounds) inv_dx - 0.5) per axis (truncation,
+// utils/mpmRoutines.py:514-517), clamped to the grid, as
+// (block index, C order) * block^3 + (cell within the block, C order).
+__global__ void k_block_keys(const float *__restrict__ x, int64_t n, float mb0, float mb1, float mb2, float inv_dx,
+                             int d0, int d1, int d2, int block, int *__restrict__ keys, int *__restrict__ ids)
+{
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const float mb[3] = {mb0, mb1, mb2};
+    const int d[3] = {d0, d1, d2};
+    int c[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float gp = (x[(int64_t)a * n + p] - mb[a]) * inv_dx;
+        const float f = gp - 0.5f;
+        // truncation toward zero of a finite value; non-finite or huge positions clamp
+        int v = isfinite(f) ? (f >= 2.0e9f ? INT32_MAX : (f <= -2.0e9f ? INT32_MIN : (int)f)) : 0;
+        v = v < 0 ? 0 : v;
+        c[a] = v > d[a] - 1 ? d[a] - 1 : v;
+    }
+    const int nb1 = (d1 + block - 1) / block, nb2 = (d2 + block - 1) / block;
+    const int bidx = ((c[0] / block) * nb1 + c[1] / block) * nb2 + c[2] / block;
+    const int ridx = ((c[0] % block) * block + c[1] % block) * block + c[2] % block;
+    keys[p] = bidx * (block * block * block) + ridx;
+    ids[p] = (int)p;
+}
+
+// the block keys, then the radix sort's buffers: the hash build's layout
+size_t block_sort_workspace_bytes(int64_t n) { return hash_workspace_bytes(n); }
+
+int block_sort(const float *x, int64_t n, const mpmw_params_t &prm, const int32_t *dims, int block, int32_t *perm,
+               void *ws, size_t ws_bytes, cudaStream_t s)
+{
+    if (ws_bytes < block_sort_workspace_bytes(n)) {
+        set_error("block_sort: workspace of %zu bytes is smaller than the %zu required", ws_bytes,
+                  block_sort_workspace_bytes(n));
+        return MPMW_E_WORKSPACE;
+    }
+    if (n == 0) return MPMW_OK;
+    const int64_t nb = (int64_t)((dims[0] + block - 1) / block) * ((dims[1] + block - 1) / block) *
+                       ((dims[2] + block - 1) / block);
+    const int64_t nkeys = nb * block * block * block;
+    if (nkeys > (int64_t)INT32_MAX) {
+        set_error("block_sort: %lld block keys exceed the 31-bit key range", (long long)nkeys);
+        return MPMW_E_ARG;
+    }
+    auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
+    char *w = static_cast<char *>(ws);
+    int *keys_a = reinterpret_cast<int *>(w); w += al(4 * n);
+    k_block_keys<<<grid_for(n), kBlock, 0, s>>>(x, n, prm.min_bounds[0], prm.min_bounds[1], prm.min_bounds[2],
+                                                prm.inv_dx, dims[0], dims[1], dims[2], block, keys_a, perm);
+    MPMW_TRY_LAUNCH("k_block_keys");
+    int bits = 0;
+    for (int64_t c = nkeys - 1; c > 0; c >>= 1) ++bits;
+    int *ko = nullptr, *vo = nullptr;
+    int rc = radix_sort_pairs(keys_a, perm, n, bits, w, &ko, &vo, s);
+    if (rc != MPMW_OK) return rc;
+    if (vo != perm && cudaMemcpyAsync(perm, vo, n * sizeof(int), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+        set_error("block_sort: copy failed");
+        return MPMW_E_DEVICE;
+    }
+    return MPMW_OK;
+}
+
 int hash_build(const float *x, int64_t n, const mpmw_hash_t &h, void *ws, size_t ws_bytes, cudaStream_t s)
 {
     if (ws_bytes < hash_workspace_bytes(n)) {
@@ -168,14 +263,8 @@ int hash_build(const float *x, int64_t n, const mpmw_hash_t &h, void *ws, size_t
     }
     if (n == 0) return MPMW_OK;
     auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
-    const int64_t nt = sort_tiles(n), hist_n = (int64_t)kRadix * nt;
     char *w = static_cast<char *>(ws);
     int *keys_a = reinterpret_cast<int *>(w); w += al(4 * n);
-    int *keys_b = reinterpret_cast<int *>(w); w += al(4 * n);
-    int *ids_b = reinterpret_cast<int *>(w); w += al(4 * n);
-    int *hist = reinterpret_cast<int *>(w); w += al(4 * hist_n);
-    int *offs = reinterpret_cast<int *>(w); w += al(4 * hist_n);
-    int *scr = reinterpret_cast<int *>(w);
     int *ids_a = h.point_ids;  // the sorted ids end up here (3 passes: a->b->a->b, then copy)
     HashDims hd{{h.dims[0], h.dims[1], h.dims[2]}};
     float inv = 1.0f / h.cell_width;
@@ -183,16 +272,10 @@ int hash_build(const float *x, int64_t n, const mpmw_hash_t &h, void *ws, size_t
     MPMW_TRY_LAUNCH("k_hash_cells");
     int bits = 0;
     for (int64_t c = ncell - 1; c > 0; c >>= 1) ++bits;
-    int *ki = keys_a, *vi = ids_a, *ko = keys_b, *vo = ids_b;
-    for (int shift = 0; shift < bits; shift += kRadixBits) {
-        k_radix_hist<<<(unsigned)nt, kSortThreads, 0, s>>>(ki, n, shift, (int)nt, hist);
-        MPMW_TRY_LAUNCH("k_radix_hist");
-        if (!exclusive_scan(hist, offs, hist_n, scr, s)) { set_error("hash_build: too many points"); return MPMW_E_ARG; }
-        MPMW_TRY_LAUNCH("scan");
-        k_radix_scatter<<<(unsigned)nt, kSortThreads, 0, s>>>(ki, vi, n, shift, (int)nt, offs, ko, vo);
-        MPMW_TRY_LAUNCH("k_radix_scatter");
-        int *t = ki; ki = ko; ko = t;
-        t = vi; vi = vo; vo = t;
+    int *ki = nullptr, *vi = nullptr;
+    {
+        int rc = radix_sort_pairs(keys_a, ids_a, n, bits, w, &ki, &vi, s);
+        if (rc != MPMW_OK) return rc;
     }
     if (vi != h.point_ids) {
         if (cudaMemcpyAsync(h.point_ids, vi, n * sizeof(int), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
@@ -594,6 +677,20 @@ static int check_hash(const mpmw_hash_t *h, int64_t n)
 extern "C" {
 
 size_t mpmw_hash_workspace_bytes(int64_t n) { return mpmw::hash_workspace_bytes(n < 0 ? 0 : n); }
+
+size_t mpmw_block_sort_workspace_bytes(int64_t n) { return mpmw::block_sort_workspace_bytes(n < 0 ? 0 : n); }
+
+int mpmw_block_sort(const float *x, int64_t n, const mpmw_params_t *prm, const int32_t *dims, int block,
+                    int32_t *perm, void *workspace, size_t ws_bytes, mpmw_stream_t stream)
+{
+    if (count_too_large(n, "block_sort")) return MPMW_E_ARG;
+    if (n < 0 || !prm || !dims || block < 1 || block > 16 || (n > 0 && (!x || !perm || !workspace))) {
+        set_error("block_sort: bad arguments");
+        return MPMW_E_ARG;
+    }
+    if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1) { set_error("block_sort: grid dims must be positive"); return MPMW_E_ARG; }
+    return mpmw::block_sort(x, n, *prm, dims, block, perm, workspace, ws_bytes, as_stream(stream));
+}
 
 // After the hash build the step reuses its scratch: [0, 256) the count of
 // XPBD-labelled particles, then one bit per hash cell, then two float4 contact

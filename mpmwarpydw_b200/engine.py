@@ -61,11 +61,38 @@ def _permute_state(obj, perm: torch.Tensor, n: int):
                 s.copy_(s[:, perm])
 
 
-def sort_particles(sim, mpm, xpbd=None, block: int = 4):
-    """Reorder all per-particle state into block order (returns the permutation)."""
+def block_order(sim, mpm, block: int = 4) -> torch.Tensor:
+    """The stable order of the particles by :func:`block_sort_key`, computed on
+    the device by the library (``mpmw_block_sort``: key kernel + stable LSD
+    radix sort); an int64 permutation (position i holds particle perm[i])."""
+    import ctypes
     n = sim.nPoints
-    key = block_sort_key(sim.particle_x, sim.minBounds, sim.invdx, mpm.gridDims, block)
-    perm = torch.argsort(key, stable=True)
+    dev = sim.device
+    perm = torch.empty(n, dtype=torch.int32, device=dev)
+    if n == 0:
+        return perm.long()
+    L = _lib.lib()
+    need = int(L.mpmw_block_sort_workspace_bytes(n))
+    ws = getattr(mpm, "_mpmw_sort_ws", None)
+    if ws is None or ws.numel() < need:
+        ws = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
+        mpm._mpmw_sort_ws = ws
+    prm = params_from_states(sim, mpm)
+    dims = (ctypes.c_int32 * 3)(*[int(d) for d in mpm.gridDims])
+    _lib.check(L.mpmw_block_sort(sim._s_particle_x.data_ptr(), n, ctypes.byref(prm), dims, int(block),
+                                 perm.data_ptr(), ws.data_ptr(), ws.numel(), stream_handle()), "block_sort")
+    return perm.long()
+
+
+def sort_particles(sim, mpm, xpbd=None, block: int = 4):
+    """Reorder all per-particle state into block order (returns the permutation).
+
+    The order comes from the library's device sort (:func:`block_order`); the
+    fields are gathered through it in place.  Used at set-up and, by the
+    driver, every ``resort_interval`` substeps, as particles drift out of the
+    cells their CTA covers."""
+    n = sim.nPoints
+    perm = block_order(sim, mpm, block)
     for obj in (sim, mpm, xpbd):
         if obj is not None:
             _permute_state(obj, perm, n)

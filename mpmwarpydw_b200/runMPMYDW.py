@@ -156,7 +156,14 @@ def _stats(sim, mpm):
     return float(residual), float(mean_damage), s
 
 
-def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=None, device_loop=False):
+def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=None, device_loop=False,
+        resort_interval=0):
+    """The big-step loop.  ``resort_interval`` > 0 re-sorts the particles into
+    block order on the device (engine.sort_particles) at the first check at or
+    after every ``resort_interval`` substeps of phase 1, so the particles of a
+    CTA stay within a few cells as the material flows (results do not depend
+    on the order; the captured graphs stay valid, as the fields keep their
+    storage)."""
     dev = torch.device(device)
     torch.cuda.set_device(dev)
     x, vol, props, overrides, dom = load_domain(args.domainFile, args)
@@ -190,7 +197,11 @@ def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=Non
         mon = PhaseOneMonitor(sim.nSteps, sim.residualThreshold, sim.damage_stall_threshold,
                               int(sim.damage_stall_duration / sim.dt))
         mon.prev_damage = d0
+        next_resort = resort_interval if resort_interval > 0 else None
         while mon.running():
+            if next_resort is not None and mon.counter >= next_resort:
+                sort_particles(sim, mpm, xpbd)
+                next_resort = (mon.counter // resort_interval + 1) * resort_interval
             c = mon.counter
             if use_loop:
                 seg = device_segment(c, check_interval, ratio, sim.nSteps, pulse_steps if pulsing else 0)
@@ -284,9 +295,12 @@ def main(argv=None):
     extra.add_argument("--device_loop", action="store_true",
                        help="run the checks between XPBD steps on the device (one host sync per segment)")
     extra.add_argument("--device", type=str, default="cuda:0")
+    extra.add_argument("--resort_interval", type=int, default=0,
+                       help="re-sort the particles into block order every N substeps (0: only at set-up)")
     ex, rest = extra.parse_known_args(argv)
     args = get_args(rest)
-    run(args, check_interval=max(1, ex.check_interval), device=ex.device, device_loop=ex.device_loop)
+    run(args, check_interval=max(1, ex.check_interval), device=ex.device, device_loop=ex.device_loop,
+        resort_interval=max(0, ex.resort_interval))
 
 
 if __name__ == "__main__":
