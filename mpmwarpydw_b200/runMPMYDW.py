@@ -25,14 +25,18 @@ K substeps instead, and the MPM substeps in between run as one fused library
 call (their XPBD steps still fall on the same counters).  Termination is then
 decided at those points.
 
-Domain input (``--domainFile``): an HDF5 file in the reference's schema when
-h5py is importable, an .npz with the same keys (``x`` [3, N] or [N, 3],
-``particle_volume`` [N], optional per-particle ``density``, ``E``, ``nu``,
-``ys``, ``alpha``, ``hardening``, ``softening``, ``eta_shear``, ``eta_bulk``,
-``strainCriteria``, ``damage``), or ``synthetic:<name>`` for a seeded generator
-of ``domains`` (``block_collapse``, ``caving_block``, ``tunnel``).
-Output (``saveFlag``): one .npz of particle state per render interval in
-``outputFolder``.
+Domain input (``--domainFile``): an HDF5 file in the reference's schema (read
+by the package's own reader, no h5py needed), an .npz with the same keys
+(``x`` [3, N] or [N, 3], ``particle_volume`` [N], optional per-particle
+``density``, ``E``, ``nu``, ``ys``, ``alpha``, ``hardening``, ``softening``,
+``eta_shear``, ``eta_bulk``, ``strainCriteria``, ``damage``), or
+``synthetic:<name>`` for a seeded generator of ``domains`` (``block_collapse``,
+``caving_block``, ``tunnel``).
+Output (``saveFlag``): the reference's files, <prefix>_grid.vti and
+<prefix>_particles.vtp per render interval in ``outputFolder``, the end of each
+big step a checkpoint with the restart arrays (runMPMYDW.py:606-627).
+``--restart <checkpoint.vtp>`` continues from such a checkpoint at the next big
+step (runMPMYDW.py:498-576).
 """
 from __future__ import annotations
 
@@ -50,6 +54,7 @@ from .engine import DeviceLoop, SubstepGraphCache, original_order, sort_particle
 from .scene import build_states
 from .utils import mpmRoutines
 from .utils import simulationRoutines as S
+from .utils import fs5PlotUtils
 from .utils.getArgs import get_args
 from .utils.simStates import vec3
 
@@ -69,11 +74,8 @@ def load_domain(path: str, args):
         get = lambda k: np.asarray(z[k])  # noqa: E731
         keys = set(z.files)
     else:
-        try:
-            import h5py
-        except ImportError as e:  # pragma: no cover - depends on the install
-            raise RuntimeError(f"{path}: reading HDF5 needs h5py; convert it to .npz or install h5py") from e
-        f = h5py.File(path, "r")
+        from .hdf5io import HDF5File
+        f = HDF5File(path)
         get = lambda k: np.asarray(f[k])  # noqa: E731
         keys = set(f.keys())
     x = get("x")
@@ -85,18 +87,56 @@ def load_domain(path: str, args):
 
 
 def save_state(sim, mpm, xpbd, folder, big_step, counter, checkpoint=False):
-    """Particle state in input order as an .npz (positions, velocities, labels,
-    damage, accumulated strain, stress, F, radius); the end-of-big-step
-    checkpoint gets its own name."""
+    """One save as the reference writes it (utils/fs5PlotUtils.py:785-881):
+    <prefix>_grid.vti and <prefix>_particles.vtp in ``folder``, particles in
+    input order; a checkpoint (the end of a big step) adds the restart
+    arrays.  Returns the .vtp path."""
     os.makedirs(folder, exist_ok=True)
-    o = lambda t: original_order(sim, t).detach().cpu().numpy()  # noqa: E731
-    tag = "checkpoint" if checkpoint else "sim_step"
-    path = os.path.join(folder, f"{tag}_{big_step:04d}_{counter:08d}.npz")
-    np.savez_compressed(path, x=o(sim.particle_x), v=o(sim.particle_v), materialLabel=o(sim.materialLabel),
-                        activeLabel=o(sim.activeLabel), damage=o(mpm.particle_damage),
-                        accumulated_strain=o(mpm.particle_accumulated_strain), stress=o(mpm.particle_stress),
-                        F=o(mpm.particle_F), radius=o(sim.particle_radius), t=sim.t)
-    return path
+    out = sim.outputFolder
+    sim.outputFolder = folder
+    try:
+        return fs5PlotUtils.save_mpm(sim, mpm, big_step, counter, include_restart_data=checkpoint,
+                                     xpbd=xpbd if checkpoint else None, order=lambda t: original_order(sim, t))
+    finally:
+        sim.outputFolder = out
+
+
+def apply_restart(sim, mpm, xpbd, path):
+    """Restore the state of a checkpoint (runMPMYDW.py:498-576) into state
+    objects that hold the particles in input order; returns the first big step
+    to run (the one after the checkpoint's)."""
+    import torch
+    r = fs5PlotUtils.load_restart_from_vtp(path)
+    if len(r["particle_x"]) != sim.nPoints:
+        raise ValueError(f"Restart file has {len(r['particle_x'])} particles, but domain has {sim.nPoints}. "
+                         "Cannot restart with different particle count.")
+    dev = sim.device
+    t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)  # noqa: E731
+    sim.t = float(r["sim_time"])
+    sim.particle_x, sim.particle_v = t(r["particle_x"]), t(r["particle_v"])
+    if r["materialLabel"] is not None:
+        sim.materialLabel = t(r["materialLabel"], torch.int32)
+    if r["activeLabel"] is not None:
+        sim.activeLabel = t(r["activeLabel"], torch.int32)
+    mpm.particle_F = t(r["particle_F"])
+    mpm.particle_F_trial = t(r["particle_F"])
+    mpm.particle_C = t(r["particle_C"])
+    for key, attr in (("particle_accumulated_strain", "particle_accumulated_strain"),
+                      ("particle_damage", "particle_damage"), ("particle_stress", "particle_stress"),
+                      ("ys", "ys"), ("ys_base", "ys_base")):
+        if r.get(key) is not None:
+            setattr(mpm, attr, t(r[key]))
+    for p in fs5PlotUtils.MATERIAL_PROPERTIES:
+        if r.get(p) is not None:
+            setattr(mpm, p, t(r[p]))
+    for key in ("particle_vol", "particle_mass", "particle_density", "particle_radius"):
+        if r.get(key) is not None:
+            setattr(sim, key, t(r[key]))
+    if r.get("particle_x_initial_xpbd") is not None:
+        xpbd.particle_x_initial_xpbd = t(r["particle_x_initial_xpbd"])
+    if r.get("particle_cumDist_xpbd") is not None:
+        xpbd.particle_cumDist_xpbd = t(r["particle_cumDist_xpbd"])
+    return int(r["bigStep"]) + 1
 
 
 class PhaseOneMonitor:
@@ -173,6 +213,9 @@ def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=Non
     if dom is not None:
         kw = dict(dx=dom.dx, minBounds=dom.minBounds, gridDims=dom.gridDims)
     sim, mpm, xpbd = build_states(args, x, vol, props, device=dev, adjust_dt=True, **kw)
+    first_big = 0
+    if getattr(args, "restart", None):
+        first_big = apply_restart(sim, mpm, xpbd, args.restart)
     sort_particles(sim, mpm, xpbd)
     log = print if verbose else (lambda *a, **k: None)
     log(f"particles {sim.nPoints}, grid {mpm.gridDims}, dx {sim.dx:.4f}, dt {sim.dt:.3e}, "
@@ -188,7 +231,7 @@ def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=Non
     start = time.time()
     saved = []
     big_steps = sim.bigSteps if max_big_steps is None else min(sim.bigSteps, max_big_steps)
-    for big in range(big_steps):
+    for big in range(first_big, big_steps):
         pulse_steps = int(args.gravity_pulse_duration / sim.dt) if args.gravity_pulse_duration > 0 else 0
         pulsing = args.gravity_pulse_factor != 1.0 and pulse_steps > 0
         if pulsing:

@@ -232,10 +232,11 @@ def write_vtp(path, points, point_data=None, field_data=None):
 def write_vti(path, dims, origin, spacing, point_data):
     """A grid as a .vti file; each point_data array is (nx, ny, nz[, c]) in C order."""
     nx, ny, nz = (int(d) for d in dims)
-    sp = np.broadcast_to(np.asarray(spacing, np.float64), (3,))
+    sp = [float(v) for v in np.broadcast_to(np.asarray(spacing, np.float64), (3,))]
+    org = [float(v) for v in np.asarray(origin, np.float64).reshape(3)]
     parts = [_header("ImageData"),
              f'<ImageData WholeExtent="0 {nx - 1} 0 {ny - 1} 0 {nz - 1}" '
-             f'Origin="{origin[0]!r} {origin[1]!r} {origin[2]!r}" Spacing="{sp[0]!r} {sp[1]!r} {sp[2]!r}">\n',
+             f'Origin="{org[0]!r} {org[1]!r} {org[2]!r}" Spacing="{sp[0]!r} {sp[1]!r} {sp[2]!r}">\n',
              f'<Piece Extent="0 {nx - 1} 0 {ny - 1} 0 {nz - 1}">\n<PointData>\n']
     for k, v in point_data.items():
         v = np.asarray(v)
