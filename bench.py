@@ -557,6 +557,134 @@ def run_reference(a):
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+def run_sweep(a):
+    """The batched parameter sweep (64 Drucker-Prager block collapses of
+    20,000-500,000 particles, seeded friction angle and cohesion; domains.
+    sweep_scenes) as the sweep runner steps it: the scenes are sharded over the
+    ranks by particle count (sweep.partition, no exchange while stepping), each
+    rank concatenates its share into one batch (one launch per kernel over its
+    scenes), tunes the launch configuration, and runs K substeps of every
+    scene in one fused call.  value = all ranks' particle-updates / the
+    max-over-ranks device time."""
+    import torch
+    import torch.distributed as dist
+
+    from mpmwarpydw_b200 import domains
+    from mpmwarpydw_b200.bind import read_status
+    from mpmwarpydw_b200.sweep import ConcatBatch, partition
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    scenes = domains.sweep_scenes()
+    counts = [d.n for d in scenes]
+    mine = partition(counts, world)[rank]
+    b = ConcatBatch([scenes[i] for i in mine], device=dev)
+    N = b.particles
+    G = sum(int(np.prod(st[1].gridDims)) for st in b.states)
+    b.tune(5, reuse=False)
+    stream = torch.cuda.current_stream(dev)
+    clocks = ClockSampler(local)
+    clocks.start()
+    b.step(a.warmup)
+    torch.cuda.synchronize(dev)
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    b.step(a.steps)
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks.stop()
+    ms = t0.elapsed_time(t1)
+    status = b.check("bench sweep", log=lambda *x: None)
+    totals = torch.tensor([ms, float(N)], device=dev, dtype=torch.float64)
+    if world > 1:
+        mx = totals[:1].clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        n_all = totals[1:].clone()
+        dist.all_reduce(n_all, op=dist.ReduceOp.SUM)
+        ms, n_total = float(mx.item()), int(n_all.item())
+    else:
+        n_total = N
+    K = a.steps
+    # end to end: the rank's concatenated particle state uploaded from pinned
+    # host memory, K substeps, the per-scene results read back
+    fields = [t for t in b.fields.values() if t is not None]
+    host = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in fields]
+    for h, t in zip(host, fields):
+        h.copy_(t)
+    h2d = sum(t.numel() * t.element_size() for t in fields)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for h, t in zip(host, fields):
+        t.copy_(h, non_blocking=True)
+    b.step(K)
+    res = b.results()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_e2e = e0.elapsed_time(e1)
+    if world > 1:
+        tt = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_e2e = float(tt.item())
+    peaks = load_peaks()
+    hbm = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
+    step_bytes = SUBSTEP_BYTES_P * N + SUBSTEP_BYTES_NODE * G
+    gbs = step_bytes / (ms / K * 1e-3) / 1e9
+    out = {
+        "metric": METRIC, "value": n_total * K / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": a.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded sweep scenes)",
+        "config": {"workload": "batched sweep: 64 Drucker-Prager block collapses (10 m cubes, 20,000-500,000 "
+                               "particles, friction angle U(20,45) deg, cohesion log-uniform [0.1,5] MPa, seed 4), "
+                               "scenes sharded over ranks by particle count, one launch per kernel over a rank's "
+                               "scenes, K substeps of every scene per timed call",
+                   "particles_total": int(sum(counts)), "particles_rank0": N, "scenes_rank0": len(mine),
+                   "grid_nodes_rank0": G, "tuned": {"groups": b.groups, "gather_tile": b.options[0],
+                                                    "read_ahead": b.options[1]},
+                   "l2": "working set > 126 MB L2, no flush", "parallelism": f"scene shards x{world}"},
+        "roofline": {"bound": "hbm", "kernel": "whole batched substep (fused G2P/return map/P2G + grid pass)",
+                     "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "traffic": None,
+                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks.get("source") == "measured"
+                     else "fallback 6650 GB/s", "bytes_per_particle": SUBSTEP_BYTES_P,
+                     "bytes_per_node": SUBSTEP_BYTES_NODE},
+        "e2e": {"value": n_total * K / (ms_e2e * 1e-3), "unit": UNIT, "steps": K,
+                "copies": "each rank's concatenated particle state uploaded from pinned host memory, K substeps, "
+                          "the per-scene results read back",
+                "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": 64 * len(res) / K},
+        "gpu_launches": 2 + 4 * K,
+        "status_word": status,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        d0 = scenes[0]
+        from oracle.oracle import Oracle, build_state
+        o = Oracle("f32_omp")
+        st = build_state(o, d0.x, d0.vol, d0.args(), d0.dx, d0.minBounds, d0.gridDims, limit=a.cpu_sample)
+        k, el = _time_oracle(o, st, seconds=a.cpu_seconds)
+        m = st.particle_x.shape[0]
+        cores = os.cpu_count() or 1
+        out["cpu_baseline"] = {"value": m * k / el, "unit": UNIT, "cores": cores, "kind": "port",
+                               "sample": f"{k} substep(s) of sweep scene 0 ({m} particles), FP32 oracle "
+                                         f"(reference algorithm restated in C), OpenMP {cores} threads",
+                               "seconds": el}
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_profile_small(k):
     """K substeps of a 788,160-particle tunnel (120x60x120 lattice cells, same
     per-particle work as the bench workload) through mpmw_run_substeps, for
@@ -593,6 +721,9 @@ def main():
     ap.add_argument("--variant-steps", type=int, default=50,
                     help="substeps of the getArgs-default (VLC + covariance) variant")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["tunnel", "sweep"], default="tunnel",
+                    help="tunnel: the 3,873,600-particle tunnel (replicas over ranks); sweep: the batched "
+                         "64-scene parameter sweep (scenes sharded over ranks)")
     ap.add_argument("--cpu-sample", type=int, default=250_000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -604,6 +735,8 @@ def main():
         run_profile_small(a.profile_small)
     elif a.impl == "reference":
         run_reference(a)
+    elif a.workload == "sweep":
+        run_sweep(a)
     else:
         run_ours(a)
 

@@ -240,6 +240,14 @@ size_t mpmw_block_sort_workspace_bytes(int64_t n);
 int mpmw_block_sort(const float *x, int64_t n, const mpmw_params_t *prm, const int32_t *dims, int block,
                     int32_t *perm, void *workspace, size_t ws_bytes, mpmw_stream_t stream);
 
+/* Launch options of the batch prepared in this workspace (no counterpart in
+ * the reference; what sweep.ConcatBatch.tune searches): gather_tile != 0 lets
+ * a CTA load its grid tile by TMA (else the gather reads the grid through L1),
+ * read_ahead != 0 lets it read its particle fields ahead by bulk copies (else
+ * plain loads).  Either is used only where mpmw_batch_prepare found it usable;
+ * the results are the same either way.  Host-side only: no device work. */
+int mpmw_batch_set_options(const void *workspace, int gather_tile, int read_ahead);
+
 /* utils/mpmRoutines.py:1446-1475 deactivate_and_teleport_xpbd_below_datum */
 int mpmw_teleport(const mpmw_particles_t *p, float z_datum, float teleport_distance, mpmw_stream_t stream);
 /* utils/mpmRoutines.py:3-21 creep_by_damage_with_baseline */

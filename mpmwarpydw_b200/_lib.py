@@ -123,6 +123,7 @@ _SIGS = {
                                 ctypes.POINTER(_I64), _I, _P, ctypes.c_size_t, _P]),
     "mpmw_batch_run_substeps": (_I, [ctypes.POINTER(Particles), _I, _P, _P, ctypes.c_size_t, _P]),
     "mpmw_batch_run_range": (_I, [ctypes.POINTER(Particles), _I, _I, _I, _P, _P, ctypes.c_size_t, _P]),
+    "mpmw_batch_set_options": (_I, [_P, _I, _I]),
     "mpmw_loop_create": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params),
                               ctypes.POINTER(LoopParams), _P, _P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p),
                               _P]),

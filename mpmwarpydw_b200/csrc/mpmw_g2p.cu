@@ -835,6 +835,7 @@ int64_t batch_node_ctas(const mpmw_grid_t *grids, int nscenes)
 struct BatchPrepared {
     int64_t n;
     int nscenes, pctas, nctas, use_tma, use_ahead, use_ahead_g2p;
+    int tma_avail = -1, ahead_avail = 0, ahead_g2p_avail = 0;  // what prepare found usable (set_batch_options)
     BatchLayout L;
     std::shared_ptr<BatchMaps> maps;
     std::vector<int> pfirst, nfirst;  // first particle / grid-node CTA of each scene (+ the totals)
@@ -907,6 +908,24 @@ int prepare_batch(const mpmw_particles_t &p, const mpmw_grid_t *grids, const mpm
     if (g_batches.size() > 256) g_batches.clear();
     g_batches[ws] = bp;
     return MPMW_OK;
+}
+
+// The launch options of a prepared batch (what ConcatBatch.tune searches):
+// the G2P grid tile by TMA (else the gather reads the grid through L1) and the
+// bulk read-ahead of the particle fields (else plain loads).  Either can only
+// be turned off where prepare_batch found it usable.  Returns false if the
+// workspace was not prepared.
+bool set_batch_options(const void *ws, int gather_tile, int read_ahead)
+{
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    auto it = g_batches.find(ws);
+    if (it == g_batches.end()) return false;
+    BatchPrepared &bp = it->second;
+    if (bp.tma_avail < 0) { bp.tma_avail = bp.use_tma; bp.ahead_avail = bp.use_ahead; bp.ahead_g2p_avail = bp.use_ahead_g2p; }
+    bp.use_tma = gather_tile ? bp.tma_avail : 0;
+    bp.use_ahead = read_ahead ? bp.ahead_avail : 0;
+    bp.use_ahead_g2p = read_ahead ? bp.ahead_g2p_avail : 0;
+    return true;
 }
 
 // per device: the batched kernels' shared-memory attribute is set (several host

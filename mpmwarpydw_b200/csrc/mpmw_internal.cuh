@@ -25,6 +25,7 @@ int reserve_fused_smem();
 size_t batch_workspace_bytes(const mpmw_grid_t *grids, int nscenes, int64_t n);
 int prepare_batch(const mpmw_particles_t &p, const mpmw_grid_t *grids, const mpmw_params_t *prms,
                   const int64_t *offsets, int nscenes, void *ws, size_t ws_bytes, cudaStream_t s);
+bool set_batch_options(const void *ws, int gather_tile, int read_ahead);
 int launch_batch_substeps(const mpmw_particles_t &p, int first, int last, int nsteps, uint32_t *st, void *ws,
                           size_t ws_bytes, cudaStream_t s);
 

@@ -617,6 +617,16 @@ int mpmw_batch_run_range(const mpmw_particles_t *p, int first_scene, int last_sc
                                  as_stream(stream));
 }
 
+int mpmw_batch_set_options(const void *workspace, int gather_tile, int read_ahead)
+{
+    if (!workspace) { set_error("batch: workspace is NULL"); return MPMW_E_ARG; }
+    if (!set_batch_options(workspace, gather_tile, read_ahead)) {
+        set_error("batch: the workspace was not prepared (mpmw_batch_prepare)");
+        return MPMW_E_ARG;
+    }
+    return MPMW_OK;
+}
+
 int mpmw_teleport(const mpmw_particles_t *p, float z_datum, float teleport_distance, mpmw_stream_t stream)
 {
     MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV));

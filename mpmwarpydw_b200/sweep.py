@@ -122,7 +122,7 @@ class SceneBatch:
 
 
 _CHUNK = 256  # particles per CTA: scene offsets are multiples of this
-_TUNED = {}   # (scenes, log2 particles) -> group count chosen by ConcatBatch.tune
+_TUNED = {}   # (scenes, log2 particles) -> (group count, kernel options) chosen by ConcatBatch.tune
 
 
 def scene_groups(counts, groups: int):
@@ -208,6 +208,7 @@ class ConcatBatch:
         self.graph = None
         self.graph_steps = 0
         self.groups = 1
+        self.options = (True, True)
         self.tuning = {}
         self._streams = []
         self.prepare()
@@ -255,29 +256,53 @@ class ConcatBatch:
         for st in self._streams[:len(ranges)]:
             cur.wait_stream(st)
 
+    def set_options(self, gather_tile: bool = True, read_ahead: bool = True):
+        """Launch options of the batch's kernels (mpmw_batch_set_options): the
+        G2P grid tile by TMA or gathers through L1, particle fields read ahead
+        by bulk copies or loaded plainly.  Same results either way."""
+        from . import _lib
+        _lib.check(_lib.lib().mpmw_batch_set_options(self.ws.data_ptr(), int(bool(gather_tile)),
+                                                     int(bool(read_ahead))), "batch_set_options")
+        self.options = (bool(gather_tile), bool(read_ahead))
+
+    def _rate(self, k, groups):
+        self.step(k, groups)
+        torch.cuda.synchronize(self.device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        self.step(k, groups)
+        e1.record()
+        torch.cuda.synchronize(self.device)
+        return self.particles * k / (e0.elapsed_time(e1) * 1e-3)
+
     def tune(self, k: int = 5, candidates=None, reuse: bool = True):
-        """Pick the number of scene groups (streams) that steps this batch
-        fastest: each candidate runs k substeps to warm up and k timed (so the
-        tuning advances every scene by 2 k substeps per candidate).  The choice
-        is kept in ``self.groups`` and, per batch shape, for later batches."""
+        """Pick the launch configuration that steps this batch fastest: first
+        the kernels' options (grid tile by TMA or L1 gathers, bulk read-ahead
+        or plain loads) with one group, then the number of scene groups
+        (streams) with the best options.  Each candidate runs k substeps to
+        warm up and k timed, so the tuning advances every scene by 2 k
+        substeps per candidate.  The choice is kept in ``self.groups`` /
+        ``self.options`` and, per batch shape, for later batches."""
         import math
         key = (len(self.counts), int(round(math.log2(max(1, self.particles)))))
         if reuse and key in _TUNED:
-            self.groups = _TUNED[key]
+            g, opts = _TUNED[key]
+            self.set_options(*opts)
+            self.groups = g
             return self.groups
         n = len(self.counts)
-        cands = sorted({c for c in (candidates or (1, 2, 4, 8, 16, 32, n)) if 1 <= c <= n})
+        self.tuning = {}
+        for opts in ((True, True), (True, False), (False, True), (False, False)):
+            self.set_options(*opts)
+            self.tuning[(1, opts)] = self._rate(k, 1)
+        best_opts = max(((o, r) for (g, o), r in self.tuning.items()), key=lambda t: t[1])[0]
+        self.set_options(*best_opts)
+        cands = sorted({c for c in (candidates or (1, 2, 4, 8, 16, 32, n)) if 1 < c <= n})
         for g in cands:
-            self.step(k, g)
-            torch.cuda.synchronize(self.device)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            self.step(k, g)
-            e1.record()
-            torch.cuda.synchronize(self.device)
-            self.tuning[g] = self.particles * k / (e0.elapsed_time(e1) * 1e-3)
-        self.groups = max(self.tuning, key=self.tuning.get)
-        _TUNED[key] = self.groups
+            self.tuning[(g, best_opts)] = self._rate(k, g)
+        (self.groups, opts) = max(self.tuning, key=self.tuning.get)
+        self.set_options(*opts)
+        _TUNED[key] = (self.groups, opts)
         return self.groups
 
     def capture(self, k: int):
@@ -368,7 +393,7 @@ def _run_batch(scenes, steps, chunk, device, tune_k: int = 5):
     dev = device or torch.device("cuda", torch.cuda.current_device())
     b = ConcatBatch(scenes, device=dev)
     done = 0
-    n_cands = len({c for c in (1, 2, 4, 8, 16, 32, len(scenes)) if 1 <= c <= len(scenes)})
+    n_cands = 4 + len({c for c in (2, 4, 8, 16, 32, len(scenes)) if 1 < c <= len(scenes)})
     if steps >= 2 * tune_k * n_cands + 2 * chunk:
         b.tune(tune_k, reuse=False)
         done = 2 * tune_k * len(b.tuning)

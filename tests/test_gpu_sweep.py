@@ -76,3 +76,32 @@ def test_concatenated_batch_equals_scenes_one_by_one():
         assert int(pad.abs().sum().item()) == 0
     res = b.results()
     assert [r.particles for r in res] == [d.n for d in scenes]
+
+
+def test_batch_options_and_tuner():
+    """Every launch option the tuner searches (grid tile by TMA or L1 gathers,
+    read-ahead by bulk copies or plain loads) gives the same scenes (to the
+    scatter's atomic-order noise); the tuner keeps the configuration it timed
+    fastest and the batch then still steps correctly."""
+    import torch
+
+    from mpmwarpydw_b200.sweep import ConcatBatch
+    scenes = _scenes()
+    ref = None
+    for opts in ((True, True), (False, True), (True, False), (False, False)):
+        b = ConcatBatch(scenes)
+        b.set_options(*opts)
+        b.step(6)
+        torch.cuda.synchronize()
+        x = b.fields["x"].cpu().numpy()
+        if ref is None:
+            ref = x
+        else:
+            assert rel_err(x, ref) <= 1e-5, opts
+    b = ConcatBatch(scenes)
+    g = b.tune(2, reuse=False)
+    assert len(b.tuning) >= 5 and b.tuning[(g, b.options)] == max(b.tuning.values())
+    b.step(3)
+    torch.cuda.synchronize()
+    from mpmwarpydw_b200.bind import read_status
+    assert read_status("cuda:0") == 0
