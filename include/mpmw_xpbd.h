@@ -101,6 +101,41 @@ size_t mpmw_xpbd_step_workspace_bytes(int64_t n, const int32_t *dims);
 int mpmw_xpbd_step(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_hash_t *h,
                    const mpmw_xpbd_params_t *q, void *workspace, size_t ws_bytes, mpmw_stream_t stream);
 
+/* ---- the big step on the device (runMPMYDW.py:633-844) ------------------ */
+/* Phase 1 with its XPBD steps and gravity pulse inside one CUDA graph: a while
+ * node whose body runs `loop.chunk` fused substeps with the pulse parameters
+ * (prm_pulse, q_pulse) while the substep index is below pulse_steps and the
+ * plain ones after (the chunk the pulse ends in is split at that substep), an
+ * XPBD step after every substep whose index is a positive multiple of
+ * xpbd_ratio (runMPMYDW.py:677-682), then the statistics and the driver's
+ * check of mpmw_loop_* (residual, damage stall, n_steps, segment budget).  IF
+ * nodes pick the branches per chunk, so the launch leaves the graph only when
+ * the phase ends or the segment budget runs out.
+ * Chunks start at counters = phase (mod chunk); with XPBD steps chunk must
+ * divide xpbd_ratio and phase must be 1 mod chunk, so every XPBD substep ends a
+ * chunk.  The caller runs the substeps before the first aligned counter.
+ * Everything passed is baked into the graph: keep it alive and unchanged. */
+typedef struct mpmw_phase_params {
+    mpmw_loop_params_t loop;
+    int32_t xpbd_ratio;          /* mpmStepsPerXpbdStep; 0: no XPBD steps */
+    int32_t pulse_steps;         /* substeps of the gravity pulse from counter 0; 0: none */
+    int32_t phase;               /* chunks start at counters = phase (mod loop.chunk) */
+} mpmw_phase_params_t;
+int mpmw_phase_loop_create(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpmw_params_t *prm,
+                           const mpmw_params_t *prm_pulse, const mpmw_xpbd_t *x, const mpmw_hash_t *h,
+                           const mpmw_xpbd_params_t *q, const mpmw_xpbd_params_t *q_pulse,
+                           const mpmw_phase_params_t *pp, mpmw_loop_state_t *state, uint32_t *status,
+                           void *workspace, size_t ws_bytes, void *xpbd_workspace, size_t xpbd_ws_bytes,
+                           mpmw_loop_t **out, mpmw_stream_t stream);
+/* Phase 2 (runMPMYDW.py:780-844): XPBD-only steps (q->xpbd_only set) until
+ * max_steps steps ran (state->counter counts them), the segment budget
+ * (state->segment_left) runs out, or the sleeping fraction of XPBD particles
+ * (x->counts) reaches sleep_ratio (< 1; state->stopped_early = 1).  Launch with
+ * mpmw_loop_launch, destroy with mpmw_loop_destroy. */
+int mpmw_xpbd_loop_create(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_hash_t *h,
+                          const mpmw_xpbd_params_t *q, int max_steps, double sleep_ratio, mpmw_loop_state_t *state,
+                          void *xpbd_workspace, size_t xpbd_ws_bytes, mpmw_loop_t **out, mpmw_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -96,6 +96,12 @@ class LoopParams(ctypes.Structure):
                 ("stall_threshold", ctypes.c_double)]
 
 
+class PhaseParams(ctypes.Structure):
+    """mpmw_phase_params_t"""
+    _fields_ = [("loop", LoopParams), ("xpbd_ratio", ctypes.c_int32), ("pulse_steps", ctypes.c_int32),
+                ("phase", ctypes.c_int32)]
+
+
 _SIGS = {
     "mpmw_last_error": (ctypes.c_char_p, []),
     "mpmw_version": (_I, []),
@@ -127,6 +133,14 @@ _SIGS = {
     "mpmw_loop_create": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params),
                               ctypes.POINTER(LoopParams), _P, _P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p),
                               _P]),
+    "mpmw_phase_loop_create": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(Grid), ctypes.POINTER(Params),
+                                    ctypes.POINTER(Params), ctypes.POINTER(XPBD), ctypes.POINTER(Hash),
+                                    ctypes.POINTER(XPBDParams), ctypes.POINTER(XPBDParams), ctypes.POINTER(PhaseParams),
+                                    _P, _P, _P, ctypes.c_size_t, _P, ctypes.c_size_t,
+                                    ctypes.POINTER(ctypes.c_void_p), _P]),
+    "mpmw_xpbd_loop_create": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(XPBD), ctypes.POINTER(Hash),
+                                   ctypes.POINTER(XPBDParams), _I, ctypes.c_double, _P, _P, ctypes.c_size_t,
+                                   ctypes.POINTER(ctypes.c_void_p), _P]),
     "mpmw_loop_launch": (_I, [_P, _P]),
     "mpmw_loop_destroy": (None, [_P]),
     "mpmw_teleport": (_I, [ctypes.POINTER(Particles), _F, _F, _P]),

@@ -240,3 +240,117 @@ class DeviceLoop:
             self.close()
         except Exception:
             pass
+
+
+class PhaseLoop(DeviceLoop):
+    """Phase 1 of a big step with its XPBD steps and gravity pulse inside one
+    CUDA graph (``mpmw_phase_loop_create``; runMPMYDW.py:646-727): each
+    iteration of the graph's while node runs ``chunk`` fused substeps with the
+    pulse gravity or the plain one (an IF node per case, the chunk the pulse
+    ends in split at that substep), the XPBD step when the chunk's last
+    substep index is a positive multiple of ``xpbd_ratio``, the statistics and
+    the driver's check.  Chunks start at counters = ``phase`` (mod chunk); with
+    XPBD steps that is 1 mod chunk and chunk must divide xpbd_ratio, so that
+    every XPBD substep ends a chunk.  The graph bakes in the structs: make a
+    new loop when dt or the base gravity changes."""
+
+    def __init__(self, sim, mpm, xpbd, chunk, n_steps, residual_threshold, stall_threshold, stall_steps, min_steps,
+                 xpbd_ratio=0, pulse_steps=0, pulse_gravity=None, gravity=None):
+        """``gravity``: the plain gravity (default sim.gravity); ``pulse_gravity``:
+        the gravity of the first ``pulse_steps`` substeps."""
+        import ctypes
+
+        from .bind import params_struct
+        from .utils.xpbdRoutines import xpbd_structs
+        self.chunk = int(chunk)
+        self.xpbd_ratio, self.pulse_steps = int(xpbd_ratio), int(pulse_steps)
+        self.phase = (1 % self.chunk) if self.xpbd_ratio > 0 else 0
+        self.P = particles_from_states(sim, mpm, xpbd)
+        self.G = grid_from_state(mpm)
+        self.prm = params_from_states(sim, mpm)
+        self.prm_pulse = params_from_states(sim, mpm)
+        base = tuple(float(g) for g in (gravity if gravity is not None else sim.gravity))
+        for i in range(3):
+            self.prm.gravity[i] = base[i]
+        pg = tuple(float(g) for g in (pulse_gravity if pulse_gravity is not None else base))
+        for i in range(3):
+            self.prm_pulse.gravity[i] = pg[i]
+        self.key = (bytes(self.prm), bytes(self.prm_pulse), self.chunk, self.xpbd_ratio, self.pulse_steps)
+        self.status = status_word(sim.device)
+        self.ws = workspace(mpm, sim.nPoints, sim.device)
+        self.state = torch.zeros(ctypes.sizeof(_lib.LoopState) // 8, dtype=torch.float64, device=sim.device)
+        self.lp = _lib.PhaseParams(_lib.LoopParams(self.chunk, int(n_steps), int(min_steps), int(stall_steps),
+                                                   float(residual_threshold), float(stall_threshold)),
+                                   self.xpbd_ratio, self.pulse_steps, self.phase)
+        self._keep = []
+        X = H = Q = QP = None
+        xws, xws_n = None, 0
+        if self.xpbd_ratio > 0:
+            _, X, Q = xpbd_structs(sim, mpm, xpbd)
+            _, _, QP = xpbd_structs(sim, mpm, xpbd)
+            for i in range(3):
+                Q.gravity[i] = base[i]
+                QP.gravity[i] = pg[i]
+            hg = xpbd.particle_grid
+            hg.cell_width = float(sim.dx)
+            hg._ensure(sim.nPoints)
+            hg.n = sim.nPoints
+            H = hg.struct()
+            xw = hg.workspace()
+            xws, xws_n = xw.data_ptr(), xw.numel()
+            self._keep += [X, Q, QP, H, xw]
+        self.stream = torch.cuda.Stream(device=sim.device)
+        self.handle = ctypes.c_void_p()
+        ref = lambda o: ctypes.byref(o) if o is not None else None  # noqa: E731
+        _lib.check(_lib.lib().mpmw_phase_loop_create(
+            ctypes.byref(self.P), ctypes.byref(self.G), ctypes.byref(self.prm), ctypes.byref(self.prm_pulse),
+            ref(X), ref(H), ref(Q), ref(QP), ctypes.byref(self.lp), self.state.data_ptr(), self.status.data_ptr(),
+            self.ws.data_ptr(), self.ws.numel(), xws, xws_n, ctypes.byref(self.handle), stream_handle(self.stream)),
+            "phase_loop_create")
+
+    def run(self, counter, stall, residual, prev_damage, segment):
+        """As DeviceLoop.run; ``counter`` must be = phase (mod chunk)."""
+        if int(counter) % self.chunk != self.phase:
+            raise ValueError(f"phase loop: chunks start at counters = {self.phase} mod {self.chunk}, not {counter}")
+        return super().run(counter, stall, residual, prev_damage, segment)
+
+
+class XPBDLoop(DeviceLoop):
+    """Phase 2 of a big step (runMPMYDW.py:780-844) in one CUDA graph
+    (``mpmw_xpbd_loop_create``): XPBD-only steps until ``max_steps`` ran or the
+    sleeping fraction of the XPBD particles reaches ``sleep_ratio``."""
+
+    def __init__(self, sim, mpm, xpbd, max_steps, sleep_ratio):
+        import ctypes
+
+        from .utils.xpbdRoutines import xpbd_structs
+        self.chunk = 1
+        P, X, Q = xpbd_structs(sim, mpm, xpbd, xpbd_only=True)
+        hg = xpbd.particle_grid
+        hg.cell_width = float(sim.dx)
+        hg._ensure(sim.nPoints)
+        hg.n = sim.nPoints
+        H = hg.struct()
+        xw = hg.workspace()
+        self._keep = [P, X, Q, H, xw]
+        self.state = torch.zeros(ctypes.sizeof(_lib.LoopState) // 8, dtype=torch.float64, device=sim.device)
+        self.stream = torch.cuda.Stream(device=sim.device)
+        self.handle = ctypes.c_void_p()
+        _lib.check(_lib.lib().mpmw_xpbd_loop_create(ctypes.byref(P), ctypes.byref(X), ctypes.byref(H),
+                                                    ctypes.byref(Q), int(max_steps), float(sleep_ratio),
+                                                    self.state.data_ptr(), xw.data_ptr(), xw.numel(),
+                                                    ctypes.byref(self.handle), stream_handle(self.stream)),
+                   "xpbd_loop_create")
+
+    def run_steps(self, done, budget):
+        """Run from ``done`` steps for at most ``budget`` more (at least one);
+        returns the loop state (counter = steps done, stopped_early = 1 on the
+        sleep-ratio stop, stats[0:2] = XPBD total / sleeping)."""
+        st = _lib.LoopState()
+        st.counter, st.stall, st.stopped_early, st.segment_left = int(done), 0, 0, int(budget)
+        cur = torch.cuda.current_stream(self.state.device)
+        self._write(st)
+        self.stream.wait_stream(cur)
+        _lib.check(_lib.lib().mpmw_loop_launch(self.handle, stream_handle(self.stream)), "loop_launch")
+        cur.wait_stream(self.stream)
+        return self.read()

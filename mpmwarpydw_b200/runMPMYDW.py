@@ -50,7 +50,7 @@ import torch
 
 from . import domains as _domains
 from .bind import check_status, params_from_states
-from .engine import DeviceLoop, SubstepGraphCache, original_order, sort_particles
+from .engine import DeviceLoop, PhaseLoop, SubstepGraphCache, XPBDLoop, original_order, sort_particles
 from .scene import build_states
 from .utils import mpmRoutines
 from .utils import simulationRoutines as S
@@ -246,7 +246,36 @@ def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=Non
                 sort_particles(sim, mpm, xpbd)
                 next_resort = (mon.counter // resort_interval + 1) * resort_interval
             c = mon.counter
-            if use_loop:
+            kc = check_interval
+            if use_loop and ratio % kc == 0 and c % kc == 1 % kc and c + kc <= sim.nSteps:
+                # the rest of phase 1 in one launch: XPBD steps and the pulse's end inside the graph
+                key = ("phase", bytes(params_from_states(sim, mpm)), tuple(base_gravity), pulse_steps if pulsing else 0)
+                loop = loops.get(key)
+                if loop is None:
+                    loop = loops[key] = PhaseLoop(
+                        sim, mpm, xpbd, kc, sim.nSteps, sim.residualThreshold, sim.damage_stall_threshold,
+                        int(sim.damage_stall_duration / sim.dt), mon.min_steps, xpbd_ratio=ratio,
+                        pulse_steps=pulse_steps if pulsing else 0,
+                        pulse_gravity=[g * args.gravity_pulse_factor for g in base_gravity], gravity=base_gravity)
+                seg = ((sim.nSteps - c) // kc) * kc
+                if next_resort is not None:
+                    seg = min(seg, max(kc, ((next_resort - c + kc - 1) // kc) * kc))
+                st = loop.run(c, mon.stall, mon.residual, mon.prev_damage, seg)
+                check_status(dev, f"substeps {c}-{st.counter}", log)
+                sim.t += (st.counter - c) * sim.dt
+                mon.counter, mon.stall, mon.residual, mon.prev_damage = st.counter, st.stall, st.residual, st.prev_damage
+                if pulsing and mon.counter >= pulse_steps:
+                    sim.gravity = base_gravity
+                if st.stopped_early:
+                    mon.stopped_early = True
+                    log(f"    early termination: damage stalled for {sim.damage_stall_duration}s")
+                    break
+                s7 = st.stats
+                log(f"  big step {big + 1}, substep {mon.counter}, t {sim.t:.4f}s, residual {st.residual:.4e}, "
+                    f"mean damage {st.prev_damage:.6f}, MPM {int(s7[3])}+{int(s7[5])}, "
+                    f"XPBD {int(s7[4])}+{int(s7[6])}, wall {time.time() - start:.2f}s")
+                continue
+            if use_loop and ratio % kc != 0:
                 seg = device_segment(c, check_interval, ratio, sim.nSteps, pulse_steps if pulsing else 0)
                 if seg >= check_interval:
                     key = bytes(params_from_states(sim, mpm))
@@ -272,7 +301,10 @@ def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=Non
                             f"XPBD {int(s7[4])}+{int(s7[6])}, wall {time.time() - start:.2f}s")
                     continue
             # substeps up to the next check: stop at the pulse end and never skip past nSteps
+            # (with the phase loop, up to the first counter = 1 mod check_interval)
             k = min(check_interval, sim.nSteps - c)
+            if use_loop and ratio % kc == 0 and kc > 1:
+                k = min(k, (1 - c) % kc or kc)
             if pulsing and c < pulse_steps:
                 k = min(k, pulse_steps - c)
             done = 0
@@ -307,7 +339,15 @@ def run(args, check_interval=1, device="cuda:0", verbose=True, max_big_steps=Non
         log(f"  phase 1 done after {mon.counter} substeps ({mon.counter * sim.dt:.3f}s simulated)")
         check_status(dev, "phase 1", log)
         # phase 2: XPBD only
-        for j in range(1, sim.xpbdOnlySteps + 1):
+        if device_loop and sim.xpbdOnlySteps > 0:
+            xl = loops.get("xpbd_only")
+            if xl is None:
+                xl = loops["xpbd_only"] = XPBDLoop(sim, mpm, xpbd, sim.xpbdOnlySteps, sim.xpbd_sleep_termination_ratio)
+            st2 = xl.run_steps(0, sim.xpbdOnlySteps)
+            sim.t += st2.counter * sim.dtxpbd
+            if st2.stopped_early:
+                log(f"    phase 2 stopped early: {int(st2.stats[1])}/{int(st2.stats[0])} XPBD particles asleep")
+        for j in range(1, sim.xpbdOnlySteps + 1) if not device_loop else ():
             S.xpbdSimulationStep(sim, mpm, xpbd, dev, xpbd_only=True)
             sim.t += sim.dtxpbd
             if sim.xpbd_sleep_termination_ratio < 1.0:

@@ -81,3 +81,37 @@ def test_driver_device_loop_matches_host_checks(tmp_path):
     assert np.array_equal(s1.materialLabel.cpu().numpy(), s2.materialLabel.cpu().numpy())
     assert rel_err(s1.particle_x.cpu().numpy(), s2.particle_x.cpu().numpy()) <= 1e-5
     assert rel_err(m1.particle_F.cpu().numpy(), m2.particle_F.cpu().numpy()) <= 1e-5
+
+
+def test_driver_phase_loop_crosses_xpbd_steps_and_pulse_end(tmp_path):
+    """The whole of phase 1 in one device-loop launch (mpmw_phase_loop_*): the
+    XPBD step every 5 substeps and the end of a 2x gravity pulse after 12
+    substeps happen inside the graph, and phase 2's XPBD-only steps run as
+    their own device loop (mpmw_xpbd_loop_*).  The final state equals the host
+    path's (the same substeps, XPBD steps and gravities by counter) to the
+    scatter's atomic-order noise."""
+    import torch
+
+    from mpmwarpydw_b200.engine import original_order
+    from mpmwarpydw_b200.runMPMYDW import run
+    from mpmwarpydw_b200.utils.getArgs import get_args
+    from mpmwarpydw_b200 import domains
+    d = domains.block_collapse(n_side=20, spacing=0.25, seed=8)
+    dom = str(tmp_path / "block.npz")
+    np.savez(dom, x=d.x.T, particle_volume=d.vol)
+    # the domain file carries geometry only, so these flags set the scene
+    argv = ["--domainFile", dom, "--bigSteps", "1", "--bigStepDuration", "0.004", "--dt", "1e-4",
+            "--xpbdOnlyDuration", "0.0015", "--saveFlag", "0", "--outputFolder", str(tmp_path),
+            "--dtxpbd", "5e-4", "--gravity_pulse_duration", "0.0012", "--gravity_pulse_factor", "2.0",
+            "--ys", "2e4", "--gravity", "-9.81"]
+    a1, a2 = get_args(argv, verbose=False), get_args(argv, verbose=False)
+    s1, m1, _, _ = run(a1, check_interval=5, verbose=False)
+    s2, m2, _, _ = run(a2, check_interval=5, verbose=False, device_loop=True)
+    torch.cuda.synchronize()
+    assert s1.mpmStepsPerXpbdStep == 5 and s1.nSteps == 40
+    assert s1.t == pytest.approx(s2.t)
+    o = lambda s, t: original_order(s, t).cpu().numpy()  # noqa: E731
+    assert np.array_equal(o(s1, s1.materialLabel), o(s2, s2.materialLabel))
+    assert rel_err(o(s2, s2.particle_x), o(s1, s1.particle_x)) <= 1e-5
+    assert rel_err(o(s2, s2.particle_v), o(s1, s1.particle_v)) <= 1e-4
+    assert rel_err(o(s2, m2.particle_F), o(s1, m1.particle_F)) <= 1e-5
