@@ -685,6 +685,78 @@ def run_sweep(a):
         dist.destroy_process_group()
 
 
+def run_resort_study(a):
+    """The fused kernel's time as the material flows, with and without
+    periodic re-sorting of the particles into block order on the device: the
+    caving block (509,696 particles, undercut, lognormal E and cohesion, XPBD
+    on: an XPBD step every 5 substeps) stepped 2,000 substeps as the driver
+    steps it, re-sorted every `resort_every` substeps or never; the mean
+    k_g2p2g launch time (CUDA events, 20 launches on a snapshot of the state)
+    at the start and at the end.  One JSON line."""
+    import torch
+
+    from mpmwarpydw_b200 import _lib, domains
+    from mpmwarpydw_b200.bind import (grid_from_state, params_from_states, particles_from_states, read_status,
+                                      status_word, workspace)
+    from mpmwarpydw_b200.engine import sort_particles
+    from mpmwarpydw_b200.utils import simulationRoutines as S
+    dev = torch.device("cuda", 0)
+    L = _lib.lib()
+    total, every = 2000, 100
+
+    def g2p2g_ms(sim, mpm, xpbd, reps=20):
+        tensors = _state_tensors(sim, mpm, xpbd) + [mpm._grid_mv.t, mpm._grid_v.t]
+        snap = [t.clone() for t in tensors]
+        P, G, prm = particles_from_states(sim, mpm, xpbd), grid_from_state(mpm), params_from_states(sim, mpm)
+        st = status_word(dev).data_ptr()
+        ws = workspace(mpm, sim.nPoints, dev)
+        stream = torch.cuda.current_stream(dev)
+        _lib.check(L.mpmw_run_substeps(P, G, prm, 2, st, ws.data_ptr(), ws.numel(), stream.cuda_stream), "warm")
+        ts = []
+        for _ in range(reps):
+            mpm._grid_mv.t.zero_()
+            _lib.check(L.mpmw_stress_p2g(P, G, prm, st, ws.data_ptr(), ws.numel(), stream.cuda_stream), "sp")
+            _lib.check(L.mpmw_grid_update(G, prm, stream.cuda_stream), "grid")
+            mpm._grid_mv.t.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _lib.check(L.mpmw_g2p2g(P, G, prm, 0, st, ws.data_ptr(), ws.numel(), stream.cuda_stream), "g2p2g")
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ts.append(e0.elapsed_time(e1))
+            for t, s0 in zip(tensors, snap):
+                t.copy_(s0)
+        return sorted(ts)[len(ts) // 2]
+
+    out = {"study": "fused kernel time over 2,000 substeps of the caving block, with and without re-sorting",
+           "workload": "caving block, 509,696 particles, XPBD step every 5 substeps", "resort_every": every,
+           "unit": "ms per k_g2p2g launch (median of 20)"}
+    for resort in (False, True):
+        sim, mpm, xpbd = domains.build(domains.caving_block(), device=dev)
+        sort_particles(sim, mpm, xpbd)
+        ratio = max(1, int(sim.mpmStepsPerXpbdStep))
+        t_start = g2p2g_ms(sim, mpm, xpbd)
+        t0 = time.perf_counter()
+        c = 0
+        while c < total:
+            nxt = ratio if c == 0 else ((c + ratio - 1) // ratio) * ratio
+            m = min(total - c, nxt - c + 1)
+            S.run_mpm_substeps(sim, mpm, xpbd, m)
+            if c + m - 1 == nxt:
+                S.xpbdSimulationStep(sim, mpm, xpbd, dev)
+            c += m
+            if resort and c % every < m:
+                sort_particles(sim, mpm, xpbd)
+        torch.cuda.synchronize(dev)
+        wall = time.perf_counter() - t0
+        t_end = g2p2g_ms(sim, mpm, xpbd)
+        xp = int((sim.materialLabel == 2).sum().item())
+        out["resort" if resort else "no_resort"] = {"g2p2g_ms_start": t_start, "g2p2g_ms_end": t_end,
+                                                    "wall_s_2000_substeps": wall, "xpbd_particles_end": xp,
+                                                    "status_word": read_status(dev)}
+    print(json.dumps(out))
+
+
 def run_profile_small(k):
     """K substeps of a 788,160-particle tunnel (120x60x120 lattice cells, same
     per-particle work as the bench workload) through mpmw_run_substeps, for
@@ -721,6 +793,9 @@ def main():
     ap.add_argument("--variant-steps", type=int, default=50,
                     help="substeps of the getArgs-default (VLC + covariance) variant")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--study", choices=["resort"], default=None,
+                    help="resort: the fused kernel's time over 2,000 caving-block substeps with and without "
+                         "re-sorting (prints its own JSON line, not a bench line)")
     ap.add_argument("--workload", choices=["tunnel", "sweep"], default="tunnel",
                     help="tunnel: the 3,873,600-particle tunnel (replicas over ranks); sweep: the batched "
                          "64-scene parameter sweep (scenes sharded over ranks)")
@@ -733,6 +808,8 @@ def main():
         a.warmup = 3
     if a.profile_small:
         run_profile_small(a.profile_small)
+    elif a.study == "resort":
+        run_resort_study(a)
     elif a.impl == "reference":
         run_reference(a)
     elif a.workload == "sweep":
