@@ -757,6 +757,56 @@ def run_resort_study(a):
     print(json.dumps(out))
 
 
+def run_profile_xpbd(k):
+    """K substeps of the caving block (509,696 particles) with an XPBD step
+    every 5 substeps, after seeding 35 % of the particles as XPBD particles
+    (damage 1, the phase transition's label), for ncu captures of the XPBD
+    kernels; prints one status line."""
+    import torch
+
+    from mpmwarpydw_b200 import domains
+    from mpmwarpydw_b200.bind import read_status
+    from mpmwarpydw_b200.engine import sort_particles
+    from mpmwarpydw_b200.utils import simulationRoutines as S
+    dev = torch.device("cuda", 0)
+    sim, mpm, xpbd = domains.build(domains.caving_block(), device=dev)
+    sort_particles(sim, mpm, xpbd)
+    g = torch.Generator(device=dev).manual_seed(5)
+    xp = torch.rand(sim.nPoints, generator=g, device=dev) < 0.35
+    sim.materialLabel.copy_(torch.where(xp, 2, sim.materialLabel))
+    ratio = max(1, int(sim.mpmStepsPerXpbdStep))
+    c = 0
+    while c < k:
+        nxt = ratio if c == 0 else ((c + ratio - 1) // ratio) * ratio
+        m = min(k - c, nxt - c + 1)
+        S.run_mpm_substeps(sim, mpm, xpbd, m)
+        if c + m - 1 == nxt:
+            S.xpbdSimulationStep(sim, mpm, xpbd, dev)
+        c += m
+    torch.cuda.synchronize(dev)
+    print(json.dumps({"profile_xpbd": {"particles": sim.nPoints, "substeps": int(k), "xpbd_ratio": ratio,
+                                       "xpbd_particles": int((sim.materialLabel == 2).sum().item()),
+                                       "status_word": read_status(dev)}}))
+
+
+def run_profile_mlp(n):
+    """Tensor-core inference of the surrogate network on n samples (after a
+    short training), for ncu captures of k_mlp_infer_tc; prints one line."""
+    import torch
+
+    from mpmwarpydw_b200.bind import read_status
+    from mpmwarpydw_b200.surrogate import ReturnMapSurrogate
+    dev = torch.device("cuda", 0)
+    net = ReturnMapSurrogate(dev, seed=0)
+    x, y = net.samples(int(n), 1)
+    net.train(x, y, steps=200, batch=16384)
+    for _ in range(3):
+        out = net.infer(x)
+    torch.cuda.synchronize(dev)
+    print(json.dumps({"profile_mlp": {"samples": int(n), "mse": float(((out - y) ** 2).mean().item()),
+                                      "status_word": read_status(dev)}}))
+
+
 def run_profile_small(k):
     """K substeps of a 788,160-particle tunnel (120x60x120 lattice cells, same
     per-particle work as the bench workload) through mpmw_run_substeps, for
@@ -785,6 +835,10 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--profile-small", type=int, default=0, metavar="K",
                     help="run K substeps of the 788,160-particle tunnel and exit (small case for ncu)")
+    ap.add_argument("--profile-xpbd", type=int, default=0, metavar="K",
+                    help="K substeps of the caving block with 35%% XPBD particles (small case for ncu)")
+    ap.add_argument("--profile-mlp", type=int, default=0, metavar="N",
+                    help="tensor-core inference of the surrogate on N samples (small case for ncu)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=10)
@@ -808,6 +862,10 @@ def main():
         a.warmup = 3
     if a.profile_small:
         run_profile_small(a.profile_small)
+    elif a.profile_xpbd:
+        run_profile_xpbd(a.profile_xpbd)
+    elif a.profile_mlp:
+        run_profile_mlp(a.profile_mlp)
     elif a.study == "resort":
         run_resort_study(a)
     elif a.impl == "reference":
