@@ -380,7 +380,7 @@ def surrogate_comparison(sim, mpm, xpbd, dev, reps=10):
     t0 = time.perf_counter()
     net = ReturnMapSurrogate(dev, seed=0)
     x, y = net.samples(4_000_000, 1)
-    losses = net.train(x, y, steps=20000, batch=16384)
+    losses = net.train(x, y, steps=60000, batch=16384)
     torch.cuda.synchronize(dev)
     train_s = time.perf_counter() - t0
     del x, y

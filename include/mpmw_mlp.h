@@ -94,12 +94,15 @@ size_t mpmw_surrogate_workspace_bytes(int64_t n);
 /* The stress phase (utils/mpmRoutines.py:229-312) with the surrogate for the
  * return of plastic trial states.  Particles outside the tensor form's range,
  * elastic trials and trials that set D = 1 are computed exactly as mpmw_stress
- * (MPMW_STRESS_AUTO).  A surrogate return is accepted only if its yield
- * residual, flow-rule magnitude and volumetric part each agree with the return
- * identities within gate_tol (relative); otherwise the exact closed form is
- * used.  audit_per_mille of the surrogate's returns (chosen by a hash of the
- * particle index and audit_seed; audited before the gate) are compared with
- * the exact return.  Trials with D > MPMW_SURR_D_MAX take the exact return.
+ * (MPMW_STRESS_AUTO).  A surrogate return is accepted only if it agrees with
+ * the state the return's identities define (the yield condition fixes the
+ * returned deviatoric norm, the flow rule the volumetric part and the
+ * accumulated-strain increment): principal stresses within gate_tol
+ * (relative, norm-wise) and the increment within gate_tol of the larger of
+ * itself and the yield strain; otherwise the exact closed form is used.
+ * audit_per_mille of the surrogate's returns (chosen by a hash of the particle
+ * index and audit_seed; audited before the gate) are compared with the exact
+ * return.  Trials with D > MPMW_SURR_D_MAX take the exact return.
  * stats (device, MPMW_SURR_NSTATS x uint32, accumulated; the caller zeroes
  * it): surrogate candidates, gate fallbacks, audited, largest audited relative
  * stress error (float bits), sum of audited relative errors (float bits),

@@ -22,10 +22,13 @@
 
 namespace mpmw {
 
+constexpr int kGatherMaxWarps = 8;  // warps of a gathering CTA (256 threads)
+
 struct GatherShared {
     float4 tile[kTileNodes];
     uint64_t bar;
     int lo[3], hi[3];
+    int wbox[kGatherMaxWarps][6];  // each warp's min and max stencil base (one barrier, no atomics)
     int tma_ok;
 };
 
@@ -36,31 +39,46 @@ struct GatherShared {
 __device__ __forceinline__ bool gather_prepare(GatherShared &S, bool act, const Weights &W, const CUtensorMap *tmap,
                                                int use_tma, uint32_t *status, bool &tile, int &ox, int &oy, int &oz)
 {
-    const int t = threadIdx.x;
-    if (t < 3) { S.lo[t] = INT32_MAX; S.hi[t] = INT32_MIN; }
+    const int t = threadIdx.x, lane = t & 31, nw = (int)(blockDim.x >> 5);
     // one read of the status word per CTA, so the tile decision below is uniform:
     // once any CTA has reported a TMA timeout the rest of the launch gathers from
     // global memory
     if (t == 0) {
         S.tma_ok = use_tma && !(status && (*reinterpret_cast<volatile uint32_t *>(status) & MPMW_ST_TIMEOUT));
-        mbar_init(&S.bar, 1);  // used only if the tile fits; the barriers below publish it
+        mbar_init(&S.bar, 1);  // used only if the tile fits; the barrier below publishes it
     }
-    __syncthreads();
     {
+        // each warp's box into its own slot (no initialisation, no atomics) ...
         int lo0 = act ? W.base[0] : INT32_MAX, lo1 = act ? W.base[1] : INT32_MAX, lo2 = act ? W.base[2] : INT32_MAX;
         int hi0 = act ? W.base[0] : INT32_MIN, hi1 = act ? W.base[1] : INT32_MIN, hi2 = act ? W.base[2] : INT32_MIN;
         lo0 = __reduce_min_sync(0xffffffffu, lo0); lo1 = __reduce_min_sync(0xffffffffu, lo1); lo2 = __reduce_min_sync(0xffffffffu, lo2);
         hi0 = __reduce_max_sync(0xffffffffu, hi0); hi1 = __reduce_max_sync(0xffffffffu, hi1); hi2 = __reduce_max_sync(0xffffffffu, hi2);
-        if ((t & 31) == 0) {
-            atomicMin(&S.lo[0], lo0); atomicMin(&S.lo[1], lo1); atomicMin(&S.lo[2], lo2);
-            atomicMax(&S.hi[0], hi0); atomicMax(&S.hi[1], hi1); atomicMax(&S.hi[2], hi2);
+        if (lane == 0) {
+            int *w = S.wbox[t >> 5];
+            w[0] = lo0; w[1] = lo1; w[2] = lo2; w[3] = hi0; w[4] = hi1; w[5] = hi2;
         }
     }
     __syncthreads();
-    if (S.lo[0] == INT32_MAX) return false;  // no active particle (uniform)
-    ox = S.lo[0]; oy = S.lo[1]; oz = S.lo[2];
-    tile = S.tma_ok && (int64_t)S.hi[0] - ox + 3 <= kTileEdge && (int64_t)S.hi[1] - oy + 3 <= kTileEdge &&
-           (int64_t)S.hi[2] - oz + 3 <= kTileEdge;
+    int b[6];
+    {
+        // ... then every warp reduces the slots: lane w reads warp w's
+#pragma unroll
+        for (int c = 0; c < 6; ++c) b[c] = lane < nw ? S.wbox[lane][c] : (c < 3 ? INT32_MAX : INT32_MIN);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            b[c] = __reduce_min_sync(0xffffffffu, b[c]);
+            b[c + 3] = __reduce_max_sync(0xffffffffu, b[c + 3]);
+        }
+    }
+    // the box for the caller (the fused kernel's scatter reads it with no
+    // barrier in between): every thread stores the same values, so each thread
+    // reads back its own store or an identical one
+#pragma unroll
+    for (int c = 0; c < 3; ++c) { S.lo[c] = b[c]; S.hi[c] = b[c + 3]; }
+    if (b[0] == INT32_MAX) return false;  // no active particle (uniform)
+    ox = b[0]; oy = b[1]; oz = b[2];
+    tile = S.tma_ok && (int64_t)b[3] - ox + 3 <= kTileEdge && (int64_t)b[4] - oy + 3 <= kTileEdge &&
+           (int64_t)b[5] - oz + 3 <= kTileEdge;
     if (tile) {
         if (t == 0) {
             mbar_arrive_expect_tx(&S.bar, kTileBytes);

@@ -14,9 +14,11 @@
 //                    rho = exp(y[0]), dgamma = n exp(y[1]) + 1e-6 with
 //                    n = |dev e|, e_ret = e + (rho n/(n + 1e-6) - 1) dev e +
 //                    y[2] dgamma, d_acc = y[3] dgamma;
-//                    a gate on the return's defining identities (yield
-//                    residual, flow-rule magnitude, volumetric part), each
-//                    within `gate_tol`, else the exact closed-form return;
+//                    a gate on the return's defining identities (the yield
+//                    condition's deviatoric norm and the flow rule's volumetric
+//                    part and strain increment): the surrogate's principal
+//                    stresses and increment against the state they define,
+//                    each within `gate_tol`, else the exact closed-form return;
 //                    an audit of a hashed fraction of the surrogate's returns
 //                    (before the gate) against the exact return (relative
 //                    error of the principal stresses: largest, sum, count
@@ -200,21 +202,33 @@ __global__ void __launch_bounds__(kBlock) k_surr_finish(mpmw_particles_t P, floa
         const float twomu = 2.f * T.mu;
         const float dg_ex = edn - T.yield_eff / twomu;
         const float beta = 0.3f * T.alpha;
-        // gate: the identities that define the radial return
-        const float rm = (er[0] + er[1] + er[2]) / 3.f;
-        const float edr[3] = {er[0] - rm, er[1] - rm, er[2] - rm};
-        const float ndr = sqrtf(edr[0] * edr[0] + edr[1] * edr[1] + edr[2] * edr[2]);
-        const float ysc = fmaxf(T.yield_eff / twomu, 1e-12f);
-        const float r_yield = fabsf(ndr - (T.yield_eff / twomu) * (nd / edn)) / ysc;
-        const float r_flow = fmaxf(fabsf(dg - dg_ex), fabsf(dacc - sqrtf(2.f / 3.f) * dg_ex) / sqrtf(2.f / 3.f)) /
-                             fmaxf(dg_ex, 1e-12f);
-        const float r_vol = fabsf((rm - em) * 3.f - 3.f * beta * dg_ex) / fmaxf(3.f * beta * dg_ex, ysc);
-        const bool ok = dg > 0.f && r_yield <= gate_tol && r_flow <= gate_tol && r_vol <= gate_tol &&
-                        isfinite(er[0]) && isfinite(er[1]) && isfinite(er[2]) && isfinite(dacc);
+        // the state the return's identities define: the yield condition fixes the
+        // returned deviatoric norm (yield / 2 mu, scaled by n / (n + 1e-6) as the
+        // reference's radial return does), the non-associated flow rule the
+        // volumetric part (beta dgamma) and the accumulated-strain increment
+        // (sqrt(2/3) dgamma)
         float ex[3];
         const float f_ex = dg_ex / edn, vc_ex = beta * dg_ex;
 #pragma unroll
         for (int k = 0; k < 3; ++k) ex[k] = fma_(-f_ex, ed[k], e[k]) + vc_ex;
+        // gate: the surrogate's principal stresses against that state (relative,
+        // norm-wise) and its accumulated-strain increment (relative to the
+        // larger of the increment and the yield strain), each within gate_tol
+        float num = 0.f, den = 0.f;
+        {
+            const float ts = T.lam * (er[0] + er[1] + er[2]), tx = T.lam * (ex[0] + ex[1] + ex[2]);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float a = fma_(twomu, er[k], ts), b = fma_(twomu, ex[k], tx);
+                num += (a - b) * (a - b);
+                den += b * b;
+            }
+        }
+        const float ysc = fmaxf(T.yield_eff / twomu, 1e-12f);
+        const float r_stress = sqrtf(num) / fmaxf(sqrtf(den), 1e-30f);
+        const float r_acc = fabsf(dacc - sqrtf(2.f / 3.f) * dg_ex) / (sqrtf(2.f / 3.f) * fmaxf(dg_ex, ysc));
+        const bool ok = dg > 0.f && r_stress <= gate_tol && r_acc <= gate_tol && isfinite(er[0]) &&
+                        isfinite(er[1]) && isfinite(er[2]) && isfinite(dacc);
         if (audit_per_mille > 0 && (int)(audit_hash(audit_seed ^ (uint64_t)p) % 1000u) < audit_per_mille) {
             // audit the surrogate's own return (before the gate) against the exact one:
             // relative error of the principal stresses

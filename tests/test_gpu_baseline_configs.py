@@ -137,24 +137,31 @@ def test_tunnel_full_size_one_substep():
 def test_tunnel_full_size_two_fused_substeps():
     """Two substeps of the tunnel through mpmw_run_substeps (the second one's
     G2P, return map and P2G in the fused kernel at full size) against two FP64
-    oracle steps, with the fused-run tolerances: x 1e-5, v and C 1e-4, stress
-    1e-3 (array-relative)."""
+    oracle steps, with the fused-run tolerances (x 1e-5, v and C 1e-4, stress
+    1e-3, array-relative) or, where the FP32 restatement of the reference is
+    itself farther from FP64 (the pre-stressed tunnel barely moves, so v and C
+    are rounding-sized), twice the FP32 oracle's distance."""
     import torch
 
     from mpmwarpydw_b200.bind import read_status
     from mpmwarpydw_b200.utils import simulationRoutines as S
     sim, mpm, xpbd = _tunnel()
     s64 = to_oracle(sim, mpm, xpbd, np.float64)
+    s32 = to_oracle(sim, mpm, xpbd)
     read_status(sim.device)
     S.run_mpm_substeps(sim, mpm, xpbd, 2)
     torch.cuda.synchronize()
     assert read_status(sim.device) == 0
-    o = oracle("f64_omp")
-    for _ in range(2):
-        orc.mpm_step(o, s64)
+    for s, prec in ((s64, "f64_omp"), (s32, "f32_omp")):
+        o = oracle(prec)
+        for _ in range(2):
+            orc.mpm_step(o, s)
     g = gpu_fields(sim, mpm, xpbd)
     assert np.array_equal(g["materialLabel"], s64.materialLabel)
-    errs = {k: rel_err(g[k], getattr(s64, k)) for k in ("particle_x", "particle_v", "particle_C", "particle_stress")}
-    print("tunnel two fused substeps, array-relative error vs FP64:", {k: f"{e:.1e}" for k, e in errs.items()})
+    keys = ("particle_x", "particle_v", "particle_C", "particle_stress")
+    errs = {k: rel_err(g[k], getattr(s64, k)) for k in keys}
+    e32 = {k: rel_err(getattr(s32, k), getattr(s64, k)) for k in keys}
+    print("tunnel two fused substeps, array-relative error vs FP64:", {k: f"{e:.1e}" for k, e in errs.items()},
+          "FP32 oracle vs FP64:", {k: f"{e:.1e}" for k, e in e32.items()})
     for k, tol in (("particle_x", 1e-5), ("particle_v", 1e-4), ("particle_C", 1e-4), ("particle_stress", 1e-3)):
-        assert errs[k] <= tol, (k, errs[k])
+        assert errs[k] <= max(tol, 2.0 * e32[k]), (k, errs[k], e32[k])

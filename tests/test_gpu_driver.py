@@ -34,8 +34,10 @@ def test_driver_check_interval_matches_per_substep_checks(tmp_path):
     s2, m2, x2, saved2 = run(a2, check_interval=10, verbose=False)
     torch.cuda.synchronize()
     assert s1.nPoints == 64000
-    assert len(saved1) >= 2 and len(glob.glob(str(tmp_path / "a" / "*_particles.vtp"))) == len(saved1)
-    assert len(glob.glob(str(tmp_path / "a" / "*_grid.vti"))) == len(saved1)
+    # the big step's checkpoint and its last regular save can share a time and so a file name
+    # (as in the reference, whose names hold the big step, counter and time)
+    assert len(saved1) >= 2 and len(glob.glob(str(tmp_path / "a" / "*_particles.vtp"))) == len(set(saved1))
+    assert len(glob.glob(str(tmp_path / "a" / "*_grid.vti"))) == len(set(saved1))
     assert np.array_equal(s1.materialLabel.cpu().numpy(), s2.materialLabel.cpu().numpy())
     assert rel_err(s1.particle_x.cpu().numpy(), s2.particle_x.cpu().numpy()) <= 1e-5
     assert rel_err(m1.particle_F.cpu().numpy(), m2.particle_F.cpu().numpy()) <= 1e-5

@@ -56,7 +56,7 @@ def test_device_block_order_equals_stable_argsort(n):
 
 
 def test_resorted_run_equals_unsorted_run():
-    """A block collapse stepped 300 substeps with a device re-sort every 50
+    """A block sliding over the floor, stepped 300 substeps with a device re-sort every 50
     (every particle field gathered through the new order) equals the same run
     without re-sorting, once both are put back in input order: to the
     atomic-order noise of the scatter (x 1e-5, v and C 1e-4)."""
@@ -69,6 +69,7 @@ def test_resorted_run_equals_unsorted_run():
     runs = []
     for resort in (False, True):
         sim, mpm, xpbd = domains.build(d, device="cuda:0")
+        sim.particle_v = torch.tensor([[4.0, 2.0, 0.0]], device="cuda:0").expand(sim.nPoints, 3)  # slides across cells
         sort_particles(sim, mpm, xpbd)
         for k in range(6):
             S.run_mpm_substeps(sim, mpm, xpbd, 50)
@@ -81,7 +82,7 @@ def test_resorted_run_equals_unsorted_run():
             assert not np.array_equal(sim.particle_order.cpu().numpy(), np.sort(sim.particle_order.cpu().numpy()))
     a, b = runs
     moved = float(np.abs(a["particle_x"] - d.x).max())
-    assert moved > 0.01                          # the block did move
+    assert moved > 0.05                          # the block did move across cells
     assert np.array_equal(a["materialLabel"], b["materialLabel"])
     for k, tol in (("particle_x", 1e-5), ("particle_v", 1e-4), ("particle_C", 1e-4)):
         assert rel_err(a[k], b[k]) <= tol, (k, rel_err(a[k], b[k]))
