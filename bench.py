@@ -501,14 +501,19 @@ def run_e2e(a, sim, mpm, xpbd, dev, S, world):
 
 
 def _oracle_sample(m):
-    """FP32 oracle state of the first m tunnel particles (input order = bottom
-    slab of the lattice), built on the CPU."""
+    """FP32 oracle state of the tunnel, built on the CPU: all 3,873,600
+    particles when m is 0 (the GPU line's workload), else the first m (input
+    order = the bottom slab of the lattice)."""
     from mpmwarpydw_b200 import domains
     from oracle.oracle import Oracle, build_state
     d = domains.tunnel()
     o = Oracle("f32_omp")
-    s = build_state(o, d.x, d.vol, d.args(), d.dx, d.minBounds, d.gridDims, limit=m)
+    s = build_state(o, d.x, d.vol, d.args(), d.dx, d.minBounds, d.gridDims, limit=(m or None))
     return o, s, d.n
+
+
+def _sample_text(m, n):
+    return f"all {n} tunnel particles" if m == n else f"the first {m} of {n} tunnel particles (bottom slab)"
 
 
 def _time_oracle(o, s, steps=None, seconds=None):
@@ -529,8 +534,9 @@ def cpu_baseline(a):
     k, el = _time_oracle(o, s, seconds=a.cpu_seconds)
     cores = os.cpu_count() or 1
     return {"value": m * k / el, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{k} substep(s) of the first {m} of {n} tunnel particles (bottom slab), FP32 oracle "
-                      f"(reference algorithm restated in C), OpenMP {cores} threads", "seconds": el}
+            "sample": f"{k} substep(s) of {_sample_text(m, n)}, FP32 oracle (reference algorithm restated in C; "
+                      f"the reference's Warp CPU path is not installable here or on the GPU box), "
+                      f"OpenMP {cores} threads", "seconds": el, "same_config": m == n}
 
 
 def run_reference(a):
@@ -542,8 +548,10 @@ def run_reference(a):
         return
     o, s, n = _oracle_sample(a.cpu_sample)
     m = s.particle_x.shape[0]
+    t1 = time.perf_counter()
     _time_oracle(o, s, steps=1)
-    k, el = _time_oracle(o, s, steps=a.steps if a.steps * 2.0 < 240 else max(1, int(240 / 2.0)))
+    per = max(time.perf_counter() - t1, 1e-3)
+    k, el = _time_oracle(o, s, steps=max(1, min(a.steps, int(180.0 / per))))
     cores = os.cpu_count() or 1
     v = m * k / el
     print(json.dumps({
@@ -551,9 +559,11 @@ def run_reference(a):
         "n_gpus": int(os.environ.get("WORLD_SIZE", 1)), "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": el / k * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded tunnel domain)",
-        "config": {"workload": f"tunnel: first {m} of {n} particles per substep, oracle substeps timed: {k}"},
+        "config": {"workload": f"tunnel: {_sample_text(m, n)} per substep, oracle substeps timed: {k}",
+                   "same_config": m == n},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"first {m} of {n} tunnel particles per substep, OpenMP {cores} threads"},
+                         "sample": f"{_sample_text(m, n)} per substep, FP32 oracle (reference algorithm restated "
+                                   f"in C), OpenMP {cores} threads"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
@@ -670,7 +680,7 @@ def run_sweep(a):
         d0 = scenes[0]
         from oracle.oracle import Oracle, build_state
         o = Oracle("f32_omp")
-        st = build_state(o, d0.x, d0.vol, d0.args(), d0.dx, d0.minBounds, d0.gridDims, limit=a.cpu_sample)
+        st = build_state(o, d0.x, d0.vol, d0.args(), d0.dx, d0.minBounds, d0.gridDims, limit=(a.cpu_sample or None))
         k, el = _time_oracle(o, st, seconds=a.cpu_seconds)
         m = st.particle_x.shape[0]
         cores = os.cpu_count() or 1
@@ -853,7 +863,8 @@ def main():
     ap.add_argument("--workload", choices=["tunnel", "sweep"], default="tunnel",
                     help="tunnel: the 3,873,600-particle tunnel (replicas over ranks); sweep: the batched "
                          "64-scene parameter sweep (scenes sharded over ranks)")
-    ap.add_argument("--cpu-sample", type=int, default=250_000)
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="particles of the tunnel the CPU baseline steps (0: all, the GPU line's workload)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the plain-vs-learned return map comparison")
