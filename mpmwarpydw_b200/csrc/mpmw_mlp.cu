@@ -574,6 +574,303 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const unsigned char *_
     }
 }
 
+// ---------------------------------------------------------------------------
+// tensor-core training: the loss of a minibatch and its gradient
+// ---------------------------------------------------------------------------
+// One CTA of 128 threads holds 128 samples, one per thread (the rows of every
+// forward and propagation MMA, M = 128).  Forward as the inference kernel
+// (hi + lo activations, FP32 last layer).  Backward:
+//   * the last layer's gradient in FP32 on the CUDA cores;
+//   * dz_(l-1) = (dz_l W_l) * SiLU'(z_(l-1)) on the tensor cores: A = dz_l as
+//     hi + lo terms, B = W_l transposed (exact BF16), with z_(l-1) recomputed by
+//     the layer's forward MMA from the stored input tile;
+//   * dW_l = dz_l^T a_(l-1) and the bias gradient on the tensor cores with the
+//     samples as K: A = dz_l^T (hi + lo; rows 64..127 zero, so M = 128),
+//     B = a_(l-1)^T in BF16 plus a row of ones (its column of D is the bias
+//     gradient); each CTA adds its partial gradient into the global one.
+// The weights are the BF16 roundings of the FP32 parameters, as in the FP32
+// training kernel (straight-through).
+constexpr int kTrK = 128;   // samples per CTA: K of the weight-gradient MMAs
+constexpr int kTrNW = 80;   // N of the weight-gradient MMAs: 64 inputs, a row of ones, zero rows
+constexpr int kTrN1 = 16;   // the same for layer 1: 8 inputs, a row of ones, zero rows
+constexpr int kTrCols = 128;  // TMEM columns allocated
+
+struct TrainTcShared {
+    unsigned char w1f[H * 16 * 2];                  // forward B of layer 1: [j][k], k 8..15 repeat 0..7
+    unsigned char w2f[H * H * 2], w3f[H * H * 2];   // forward B: [j][k]
+    unsigned char w2b[H * H * 2], w3b[H * H * 2];   // propagation B: [k][j] (transposed)
+    unsigned char x[kTcRows * 16 * 2];              // layer-1 A: features hi | lo
+    unsigned char a1[kTcRows * H * 2], a1lo[kTcRows * H * 2];
+    unsigned char a2[kTcRows * H * 2], a2lo[kTcRows * H * 2];
+    unsigned char dz[kTcRows * H * 2], dzlo[kTcRows * H * 2];      // propagation A: [s][j]; first a3 (FP32)
+    unsigned char dzt[kTcRows * kTrK * 2], dztlo[kTcRows * kTrK * 2];  // weight-gradient A: [j][s]
+    unsigned char act[kTrNW * kTrK * 2];            // weight-gradient B: [k][s]
+    float b[3 * H + OUT];
+    float w4[OUT][H];
+    float g4[kTcRows][OUT];
+    float red[kTcRows / 32];
+    uint64_t bar;
+    uint32_t tmem;
+    int timeout;
+};
+static_assert(sizeof(float) * kTcRows * H <= 2 * kTcRows * H * 2, "a3 fits the propagation A tiles");
+
+__device__ __forceinline__ void put_bf16(unsigned char *tile, int r, int k, int K, float v)
+{
+    *reinterpret_cast<__nv_bfloat16 *>(tile + core_offset(r, k, K)) = __float2bfloat16_rn(v);
+}
+
+__device__ __forceinline__ float silu_d(float z)
+{
+    const float sg = 1.f / (1.f + expf(-z));
+    return sg * (1.f + z * (1.f - sg));
+}
+
+// this thread's row of 64 FP32 values back from its hi and lo tiles
+__device__ __forceinline__ void get_row64(const unsigned char *a, const unsigned char *alo, int r, float *h)
+{
+#pragma unroll
+    for (int k = 0; k < H; ++k)
+        h[k] = __bfloat162float(*reinterpret_cast<const __nv_bfloat16 *>(a + core_offset(r, k, H))) +
+               __bfloat162float(*reinterpret_cast<const __nv_bfloat16 *>(alo + core_offset(r, k, H)));
+}
+
+__global__ void __launch_bounds__(kTcRows) k_mlp_grad_tc(const float *__restrict__ P, const float *__restrict__ X,
+                                                         const float *__restrict__ Yt, int64_t n,
+                                                         float *__restrict__ G, float *__restrict__ loss,
+                                                         uint32_t *status)
+{
+    extern __shared__ __align__(1024) unsigned char smem_tr[];
+    TrainTcShared &S = *reinterpret_cast<TrainTcShared *>(smem_tr + ((1024u - (smem_addr(smem_tr) & 1023u)) & 1023u));
+    const int t = threadIdx.x, warp = t >> 5;
+    const int64_t row = (int64_t)blockIdx.x * kTcRows + t;
+    const bool valid = row < n;
+    // weights as BF16 operand tiles (forward and transposed), biases and W4 in FP32
+    for (int q = t; q < H * 16; q += kTcRows) put_bf16(S.w1f, q / 16, q % 16, 16, P[oW1 + (q / 16) * IN + (q % 16) % IN]);
+    for (int q = t; q < H * H; q += kTcRows) {
+        const int j = q / H, k = q % H;
+        put_bf16(S.w2f, j, k, H, P[oW2 + q]);
+        put_bf16(S.w3f, j, k, H, P[oW3 + q]);
+        put_bf16(S.w2b, k, j, H, P[oW2 + q]);
+        put_bf16(S.w3b, k, j, H, P[oW3 + q]);
+    }
+    for (int q = t; q < H; q += kTcRows) {
+        S.b[q] = P[oB1 + q];
+        S.b[H + q] = P[oB2 + q];
+        S.b[2 * H + q] = P[oB3 + q];
+    }
+    if (t < OUT) S.b[3 * H + t] = P[oB4 + t];
+    for (int q = t; q < OUT * H; q += kTcRows) S.w4[q / H][q % H] = P[oW4 + q];
+    // the weight-gradient tiles start at zero (their padding rows stay zero)
+    {
+        uint4 *z0 = reinterpret_cast<uint4 *>(S.dzt), *z1 = reinterpret_cast<uint4 *>(S.dztlo);
+        uint4 *z2 = reinterpret_cast<uint4 *>(S.act);
+        const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+        for (int q = t; q < (int)(sizeof(S.dzt) / 16); q += kTcRows) { z0[q] = zero; z1[q] = zero; }
+        for (int q = t; q < (int)(sizeof(S.act) / 16); q += kTcRows) z2[q] = zero;
+    }
+    // this row's features (hi | lo) and targets
+    float f[IN], yt[OUT];
+#pragma unroll
+    for (int k = 0; k < IN; ++k) f[k] = valid ? X[row * IN + k] : 0.f;
+#pragma unroll
+    for (int o = 0; o < OUT; ++o) yt[o] = valid ? Yt[row * OUT + o] : 0.f;
+    {
+        __nv_bfloat162 v[4], w[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) split_bf16(f[2 * c], f[2 * c + 1], v[c], w[c]);
+        *reinterpret_cast<uint4 *>(S.x + core_offset(t, 0, 16)) = *reinterpret_cast<uint4 *>(v);
+        *reinterpret_cast<uint4 *>(S.x + core_offset(t, 8, 16)) = *reinterpret_cast<uint4 *>(w);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&S.tmem)),
+                     "r"(kTrCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (t == 0) { mbar_init(&S.bar, 1); S.timeout = 0; }
+    unsigned phase = 0;
+    uint32_t tmem = 0;
+    // one MMA group: every thread's operand writes published, one elected thread
+    // issues the K loop over the A terms, every thread waits for the commit
+    auto gemm = [&](const unsigned char *a0, const unsigned char *a1p, const unsigned char *b, int K, int N) {
+        proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        tmem = S.tmem;
+        if (t == 0 && !S.timeout) {
+            tc_fence_after();
+            const uint32_t id = idesc_bf16(N);
+            const unsigned char *as[2] = {a0, a1p};
+            int acc = 0;
+            for (int term = 0; term < (a1p ? 2 : 1); ++term)
+                for (int kk = 0; kk < K / 16; ++kk) {
+                    const uint64_t ad = smem_desc(as[term] + kk * 256, 128, (K / 8) * 128);
+                    const uint64_t bd = smem_desc(b + kk * 256, 128, (K / 8) * 128);
+                    tc_mma(tmem, ad, bd, id, acc);
+                    acc = 1;
+                }
+            tc_commit(&S.bar);
+        }
+        if (!mbar_wait_bounded(&S.bar, phase)) {
+            S.timeout = 1;
+            raise_status(status, MPMW_ST_TIMEOUT);
+        }
+        phase ^= 1u;
+        tc_fence_after();
+    };
+    // this thread's row (a sample) of an M = 128 result: N columns
+    auto ld_row = [&](float *v, int N) {
+        const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
+        for (int c = 0; c < N; c += 16) tc_ld16(lane_addr + (uint32_t)c, v + c);
+        tc_wait_ld();
+    };
+    // the weight-gradient result: rows j = 0..63 (warps 0 and 1), N columns;
+    // columns < nin are dW[j][c], column nin the bias gradient
+    auto add_dw = [&](int oW, int oB, int nin, int N) {
+        if (warp < 2) {
+            float v[kTrNW];
+            const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
+            for (int c = 0; c < N; c += 16) tc_ld16(lane_addr + (uint32_t)c, v + c);
+            tc_wait_ld();
+            const int j = t;
+            for (int c = 0; c < nin; ++c) atomicAdd(&G[oW + j * nin + c], v[c]);
+            atomicAdd(&G[oB + j], v[nin]);
+        }
+    };
+    float h[H], d[H];
+    // ---- forward ----
+    gemm(S.x, nullptr, S.w1f, 16, H);
+    ld_row(h, H);
+#pragma unroll
+    for (int j = 0; j < H; ++j) { const float z = h[j] + S.b[j]; h[j] = z / (1.f + expf(-z)); }
+    put_row64(S.a1, S.a1lo, t, h);
+    gemm(S.a1, S.a1lo, S.w2f, H, H);
+    ld_row(h, H);
+#pragma unroll
+    for (int j = 0; j < H; ++j) { const float z = h[j] + S.b[H + j]; h[j] = z / (1.f + expf(-z)); }
+    put_row64(S.a2, S.a2lo, t, h);
+    gemm(S.a2, S.a2lo, S.w3f, H, H);
+    ld_row(h, H);
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+        const float z = h[j] + S.b[2 * H + j];
+        d[j] = silu_d(z);
+        h[j] = z / (1.f + expf(-z));   // a3
+    }
+    // ---- loss, last layer (FP32) ----
+    const float inv = 2.f / (float)((double)n * OUT);
+    float lsum = 0.f, g4[OUT];
+#pragma unroll
+    for (int o = 0; o < OUT; ++o) {
+        float z = S.b[3 * H + o];
+#pragma unroll
+        for (int k = 0; k < H; ++k) z = fmaf(h[k], S.w4[o][k], z);
+        const float r = valid ? z - yt[o] : 0.f;
+        lsum = fmaf(r, r, lsum);
+        g4[o] = inv * r;
+        S.g4[t][o] = g4[o];
+    }
+    float(*a3s)[H] = reinterpret_cast<float(*)[H]>(S.dz);
+#pragma unroll
+    for (int k = 0; k < H; ++k) a3s[t][k] = h[k];
+    // dz3 = (g4 W4) * SiLU'(z3)
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+        float g = 0.f;
+#pragma unroll
+        for (int o = 0; o < OUT; ++o) g = fmaf(g4[o], S.w4[o][j], g);
+        d[j] *= g;
+    }
+    __syncthreads();
+    for (int q = t; q < OUT * H; q += kTcRows) {
+        const int o = q / H, k = q % H;
+        float acc = 0.f;
+        for (int r = 0; r < kTcRows; ++r) acc = fmaf(S.g4[r][o], a3s[r][k], acc);
+        atomicAdd(&G[oW4 + q], acc);
+    }
+    if (t < OUT) {
+        float acc = 0.f;
+        for (int r = 0; r < kTcRows; ++r) acc += S.g4[r][t];
+        atomicAdd(&G[oB4 + t], acc);
+    }
+    // loss
+    {
+        float v = lsum;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((t & 31) == 0) S.red[warp] = v;
+    }
+    __syncthreads();   // a3s and g4 read, the loss partials written
+    if (t == 0) {
+        float v = 0.f;
+        for (int w = 0; w < kTcRows / 32; ++w) v += S.red[w];
+        atomicAdd(loss, v / (float)((double)n * OUT));
+    }
+    // the weight-gradient operands of one layer: dz^T (hi, lo) in column t,
+    // the layer's input (BF16) in column t, the ones row
+    auto put_dw_operands = [&](const float *dzv, const float *in, int nin) {
+#pragma unroll
+        for (int j = 0; j < H; ++j) {
+            const __nv_bfloat16 hi = __float2bfloat16_rn(dzv[j]);
+            *reinterpret_cast<__nv_bfloat16 *>(S.dzt + core_offset(j, t, kTrK)) = hi;
+            *reinterpret_cast<__nv_bfloat16 *>(S.dztlo + core_offset(j, t, kTrK)) =
+                __float2bfloat16_rn(dzv[j] - __bfloat162float(hi));
+        }
+        for (int k = 0; k < nin; ++k) put_bf16(S.act, k, t, kTrK, in[k]);
+        put_bf16(S.act, nin, t, kTrK, 1.f);
+    };
+    // ---- layer 3: dW3, db3; dz2 ----
+    get_row64(S.a2, S.a2lo, t, h);            // a2
+    put_dw_operands(d, h, H);
+    gemm(S.dzt, S.dztlo, S.act, kTrK, kTrNW);
+    add_dw(oW3, oB3, H, kTrNW);
+    put_row64(S.dz, S.dzlo, t, d);            // dz3 as propagation A
+    gemm(S.a1, S.a1lo, S.w2f, H, H);          // z2 again
+    ld_row(h, H);
+#pragma unroll
+    for (int k = 0; k < H; ++k) h[k] = silu_d(h[k] + S.b[H + k]);
+    gemm(S.dz, S.dzlo, S.w3b, H, H);          // dz3 W3
+    ld_row(d, H);
+#pragma unroll
+    for (int k = 0; k < H; ++k) d[k] *= h[k];  // dz2
+    // ---- layer 2: dW2, db2; dz1 ----
+    get_row64(S.a1, S.a1lo, t, h);            // a1
+    put_dw_operands(d, h, H);
+    gemm(S.dzt, S.dztlo, S.act, kTrK, kTrNW);
+    add_dw(oW2, oB2, H, kTrNW);
+    put_row64(S.dz, S.dzlo, t, d);            // dz2 as propagation A
+    gemm(S.x, nullptr, S.w1f, 16, H);         // z1 again
+    ld_row(h, H);
+#pragma unroll
+    for (int k = 0; k < H; ++k) h[k] = silu_d(h[k] + S.b[k]);
+    gemm(S.dz, S.dzlo, S.w2b, H, H);          // dz2 W2
+    ld_row(d, H);
+#pragma unroll
+    for (int k = 0; k < H; ++k) d[k] *= h[k];  // dz1
+    // ---- layer 1: dW1, db1 (inputs: the features, then ones, then zeros) ----
+    {
+        float in[kTrN1];
+#pragma unroll
+        for (int k = 0; k < kTrN1; ++k) in[k] = k < IN ? f[k] : 0.f;
+        put_dw_operands(d, in, kTrN1 - 1);     // rows 8..14 zero, row 15 ones
+    }
+    gemm(S.dzt, S.dztlo, S.act, kTrK, kTrN1);
+    if (warp < 2) {
+        float v[kTrN1];
+        const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
+        tc_ld16(lane_addr, v);
+        tc_wait_ld();
+        for (int c = 0; c < IN; ++c) atomicAdd(&G[oW1 + t * IN + c], v[c]);
+        atomicAdd(&G[oB1 + t], v[kTrN1 - 1]);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTrCols) : "memory");
+    }
+}
+
 }  // namespace mlp
 }  // namespace mpmw
 
@@ -588,8 +885,10 @@ static int set_smem_attrs()
     if (cudaGetDevice(&dev) != cudaSuccess) { set_error("mlp: no current device"); return MPMW_E_DEVICE; }
     if (dev >= 0 && dev < 64 && !g_mlp_attr[dev]) {
         const int ts = (int)sizeof(TrainShared), tc = (int)sizeof(TcShared) + 1024;
+        const int tr = (int)sizeof(TrainTcShared) + 1024;
         if (cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, ts) != cudaSuccess ||
             cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, ts) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mlp_grad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tr) != cudaSuccess ||
             cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc) != cudaSuccess) {
             set_error("mlp: cannot reserve shared memory");
             return MPMW_E_DEVICE;
@@ -635,6 +934,23 @@ int mpmw_mlp_grad(const float *params, const float *x, const float *y, int64_t n
     const unsigned g = (unsigned)((n + kTile - 1) / kTile);
     k_mlp_grad<<<g, kThreads, sizeof(TrainShared), s>>>(params, x, y, n, grad, loss);
     return check_launch("k_mlp_grad");
+}
+
+int mpmw_mlp_grad_tc(const float *params, const float *x, const float *y, int64_t n, float *grad, float *loss,
+                     uint32_t *status, mpmw_stream_t stream)
+{
+    if (!params || !grad || !loss || n <= 0 || !x || !y) { set_error("mlp_grad_tc: bad arguments"); return MPMW_E_ARG; }
+    if (count_too_large(n, "mlp_grad_tc")) return MPMW_E_ARG;
+    { int rc_ = set_smem_attrs(); if (rc_ != MPMW_OK) return rc_; }
+    cudaStream_t s = as_stream(stream);
+    if (cudaMemsetAsync(grad, 0, NP * sizeof(float), s) != cudaSuccess ||
+        cudaMemsetAsync(loss, 0, sizeof(float), s) != cudaSuccess) {
+        set_error("mlp_grad_tc: memset failed");
+        return MPMW_E_DEVICE;
+    }
+    const unsigned g = (unsigned)((n + kTcRows - 1) / kTcRows);
+    k_mlp_grad_tc<<<g, kTcRows, sizeof(TrainTcShared) + 1024, s>>>(params, x, y, n, grad, loss, status);
+    return check_launch("k_mlp_grad_tc");
 }
 
 int mpmw_mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr, mpmw_stream_t stream)
