@@ -74,6 +74,17 @@ int mpmw_mlp_forward(const float *params, const float *x, int64_t n, float *y, m
 int mpmw_mlp_grad(const float *params, const float *x, const float *y, int64_t n, float *grad, float *loss,
                   mpmw_stream_t stream);
 
+/* The same loss and gradient on the tensor cores (tcgen05.mma, FP32
+ * accumulators in tensor memory), 128 samples per CTA: the forward pass as
+ * mpmw_mlp_infer_tc; the back-propagated errors dz W with dz as hi + lo BF16
+ * terms against the BF16 weights; the weight and bias gradients dz^T a with
+ * the samples as the MMA's K (dz^T as hi + lo terms, a in BF16, a row of ones
+ * for the bias); the last layer in FP32 on the CUDA cores.  Pre-activations
+ * are recomputed by each layer's MMA instead of being stored.  Bounded waits
+ * report MPMW_ST_TIMEOUT in *status (may be NULL). */
+int mpmw_mlp_grad_tc(const float *params, const float *x, const float *y, int64_t n, float *grad, float *loss,
+                     uint32_t *status, mpmw_stream_t stream);
+
 /* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8), step counts from 1. */
 int mpmw_mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr, mpmw_stream_t stream);
 

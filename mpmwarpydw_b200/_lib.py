@@ -149,6 +149,7 @@ _SIGS = {
     "mpmw_dp_samples": (_I, [_I64, ctypes.c_uint64, _P, _P, _P]),
     "mpmw_mlp_forward": (_I, [_P, _P, _I64, _P, _P]),
     "mpmw_mlp_grad": (_I, [_P, _P, _P, _I64, _P, _P, _P]),
+    "mpmw_mlp_grad_tc": (_I, [_P, _P, _P, _I64, _P, _P, _P, _P]),
     "mpmw_mlp_adam": (_I, [_P, _P, _P, _P, _I, _F, _P]),
     "mpmw_mlp_pack": (_I, [_P, _P, _P]),
     "mpmw_mlp_infer_tc": (_I, [_P, _P, _P, _I64, _P, _P, _P]),

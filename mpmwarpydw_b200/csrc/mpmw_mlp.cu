@@ -729,13 +729,19 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_grad_tc(const float *__restrict
     // columns < nin are dW[j][c], column nin the bias gradient
     auto add_dw = [&](int oW, int oB, int nin, int N) {
         if (warp < 2) {
-            float v[kTrNW];
             const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
-            for (int c = 0; c < N; c += 16) tc_ld16(lane_addr + (uint32_t)c, v + c);
-            tc_wait_ld();
             const int j = t;
-            for (int c = 0; c < nin; ++c) atomicAdd(&G[oW + j * nin + c], v[c]);
-            atomicAdd(&G[oB + j], v[nin]);
+            for (int c0 = 0; c0 < N; c0 += 16) {
+                float v[16];
+                tc_ld16(lane_addr + (uint32_t)c0, v);
+                tc_wait_ld();
+#pragma unroll
+                for (int c = 0; c < 16; ++c) {
+                    const int col = c0 + c;
+                    if (col < nin) atomicAdd(&G[oW + j * nin + col], v[c]);
+                    else if (col == nin) atomicAdd(&G[oB + j], v[c]);
+                }
+            }
         }
     };
     float h[H], d[H];
@@ -860,6 +866,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_grad_tc(const float *__restrict
         const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
         tc_ld16(lane_addr, v);
         tc_wait_ld();
+#pragma unroll
         for (int c = 0; c < IN; ++c) atomicAdd(&G[oW1 + t * IN + c], v[c]);
         atomicAdd(&G[oB1 + t], v[kTrN1 - 1]);
     }

@@ -4,8 +4,9 @@ reference, whose return map is closed form: utils/mpmRoutines.py:314-453).
 An MLP 8 -> 64 -> 64 -> 64 -> 4 (SiLU) maps the features of a plastic trial
 state to its return (feature and target definitions in include/mpmw_mlp.h).
 It is trained on the GPU by the library's own kernels: labelled samples from
-the plain return map (``mpmw_dp_samples``), forward/backward in FP32 with the
-weights rounded to BF16 (``mpmw_mlp_grad``), Adam (``mpmw_mlp_adam``).
+the plain return map (``mpmw_dp_samples``), forward and backward on the
+tensor cores (``mpmw_mlp_grad_tc``; ``mpmw_mlp_grad`` is the FP32 CUDA-core
+version) with the hidden weights rounded to BF16, Adam (``mpmw_mlp_adam``).
 Inference runs on the tensor cores (``mpmw_mlp_infer_tc``: tcgen05.mma with
 BF16 weights, each hidden-layer input split into hi + lo BF16 terms, FP32
 accumulation in tensor memory; the last layer in FP32).
@@ -57,20 +58,32 @@ class ReturnMapSurrogate:
         _lib.check(_lib.lib().mpmw_dp_samples(n, seed, x.data_ptr(), y.data_ptr(), stream_handle()), "dp_samples")
         return x, y
 
-    def loss_and_grad(self, x, y):
-        _lib.check(_lib.lib().mpmw_mlp_grad(self.params.data_ptr(), x.data_ptr(), y.data_ptr(), x.shape[0],
-                                            self.grad.data_ptr(), self.loss.data_ptr(), stream_handle()), "mlp_grad")
+    def loss_and_grad(self, x, y, tensor_cores: bool = False):
+        """Loss and gradient of (x, y): FP32 CUDA-core kernel, or the
+        tensor-core kernel (mpmw_mlp_grad_tc)."""
+        L = _lib.lib()
+        if tensor_cores:
+            st = status_word(x.device)
+            _lib.check(L.mpmw_mlp_grad_tc(self.params.data_ptr(), x.data_ptr(), y.data_ptr(), x.shape[0],
+                                          self.grad.data_ptr(), self.loss.data_ptr(), st.data_ptr(),
+                                          stream_handle()), "mlp_grad_tc")
+        else:
+            _lib.check(L.mpmw_mlp_grad(self.params.data_ptr(), x.data_ptr(), y.data_ptr(), x.shape[0],
+                                       self.grad.data_ptr(), self.loss.data_ptr(), stream_handle()), "mlp_grad")
         return self.loss, self.grad
 
-    def train(self, x, y, steps: int, batch: int = 8192, lr: float = 2e-3, lr_end: float = 2e-5):
-        """Adam over contiguous mini-batches of (x, y); cosine learning-rate decay."""
+    def train(self, x, y, steps: int, batch: int = 8192, lr: float = 2e-3, lr_end: float = 2e-5,
+              tensor_cores: bool = True):
+        """Adam over contiguous mini-batches of (x, y); cosine learning-rate
+        decay.  The loss and gradient of each batch come from the tensor-core
+        kernel by default (``tensor_cores=False``: the FP32 CUDA-core one)."""
         n = x.shape[0]
         L = _lib.lib()
         losses = []
         for k in range(steps):
             i0 = (k * batch) % max(1, n - batch + 1)
             xb, yb = x[i0:i0 + batch], y[i0:i0 + batch]
-            self.loss_and_grad(xb, yb)
+            self.loss_and_grad(xb, yb, tensor_cores)
             self.step += 1
             lrk = lr_end + 0.5 * (lr - lr_end) * (1 + math.cos(math.pi * k / max(1, steps)))
             _lib.check(L.mpmw_mlp_adam(self.params.data_ptr(), self.grad.data_ptr(), self.m.data_ptr(),

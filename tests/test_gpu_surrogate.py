@@ -45,6 +45,48 @@ def test_gradient_matches_cpu():
         assert _rel(g[off:off + n], g_ref[off:off + n]) <= 1e-4, name
 
 
+def test_tensor_core_gradient_matches_cpu():
+    """The tensor-core training kernel (mpmw_mlp_grad_tc) against the FP64
+    restatement and the FP32 CUDA-core kernel on 700 samples (5 full 128-row
+    CTAs and a partial one): the loss to 1e-5 (the forward pass carries split
+    BF16 activations), every parameter block's gradient to 1e-2 norm-wise (the
+    weight gradients take the layer inputs in BF16)."""
+    import torch
+    net = _net(2)
+    x, y = net.samples(700, 12)
+    l_tc, g_tc = net.loss_and_grad(x, y, tensor_cores=True)
+    l_tc, g_tc = float(l_tc.item()), g_tc.clone().cpu().numpy()
+    l_32, g_32 = net.loss_and_grad(x, y, tensor_cores=False)
+    l_32, g_32 = float(l_32.item()), g_32.clone().cpu().numpy()
+    torch.cuda.synchronize()
+    from mpmwarpydw_b200.bind import read_status
+    assert read_status(x.device) == 0
+    l_ref, g_ref = M.loss_and_grad(net.params.cpu().numpy(), x.cpu().numpy(), y.cpu().numpy())
+    assert abs(l_tc - l_ref) <= 1e-5 * l_ref and abs(l_tc - l_32) <= 1e-5 * l_ref
+    for name, (off, shape) in M.OFFSETS.items():
+        n = int(np.prod(shape))
+        a, b, c = g_tc[off:off + n], g_ref[off:off + n], g_32[off:off + n]
+        err = float(np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-30))
+        assert err <= 1e-2, (name, err)
+        assert float(np.linalg.norm(a - c) / (np.linalg.norm(c) + 1e-30)) <= 1e-2, name
+
+
+def test_tensor_core_training_tracks_fp32_training():
+    """Training on the tensor cores reaches the loss the FP32 kernels reach
+    from the same start (3,000 Adam steps): within 1.5x, both below 1e-2."""
+    import torch
+    x, y = _net(7).samples(400_000, 18)
+    out = []
+    for tc in (True, False):
+        net = _net(7)
+        losses = net.train(x, y, steps=3000, batch=8192, tensor_cores=tc)
+        torch.cuda.synchronize()
+        out.append(float(np.mean(losses[-3:])))
+    print(f"training loss after 3,000 steps: tensor cores {out[0]:.3e}, FP32 kernels {out[1]:.3e}")
+    assert max(out) < 1e-2
+    assert out[0] <= 1.5 * out[1]
+
+
 def test_tensor_core_inference_matches_split_emulation():
     """tcgen05 MMA path (BF16 weights, every hidden-layer input fed as hi + lo
     BF16 terms, FP32 accumulate, FP32 last layer) against the same network
