@@ -59,7 +59,7 @@ def test_resorted_run_equals_unsorted_run():
     """A block sliding over the floor, stepped 300 substeps with a device re-sort every 50
     (every particle field gathered through the new order) equals the same run
     without re-sorting, once both are put back in input order: to the
-    atomic-order noise of the scatter (x 1e-5, v 1e-4, C 1e-4 of 1 /s)."""
+    atomic-order noise of the scatter (x 1e-5, v 1e-4, C 1e-4 of |v|/dx)."""
     import torch
 
     from mpmwarpydw_b200 import domains
@@ -85,6 +85,8 @@ def test_resorted_run_equals_unsorted_run():
     assert moved > 0.05                          # the block did move across cells
     assert np.array_equal(a["materialLabel"], b["materialLabel"])
     # C, the velocity gradient of a block sliding at a uniform velocity, is close
-    # to zero: its noise is held against 1 /s rather than against its own size
-    for k, tol, floor in (("particle_x", 1e-5, 0.0), ("particle_v", 1e-4, 0.0), ("particle_C", 1e-4, 1.0)):
+    # to zero: its noise is held against the velocity's own gradient scale
+    # |v| / dx (about 9 /s here) rather than against C's size
+    c_scale = float(np.abs(a["particle_v"]).max()) / 0.5
+    for k, tol, floor in (("particle_x", 1e-5, 0.0), ("particle_v", 1e-4, 0.0), ("particle_C", 1e-4, c_scale)):
         assert rel_err(a[k], b[k], floor) <= tol, (k, rel_err(a[k], b[k], floor))
