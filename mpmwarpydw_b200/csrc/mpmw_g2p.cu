@@ -100,31 +100,34 @@ __global__ void __launch_bounds__(kBlock) k_stress_p2g_list(mpmw_particles_t P, 
 // Shared memory of k_g2p: the grid tile, F of the CTA's particles (read ahead
 // by bulk copies) and the positions, parked while the gather runs so that fewer
 // registers stay live across it.
+template <int Cta>
 struct G2PShared {
     GatherShared g;
-    float F[9][kBlock];
-    float xpark[3][kBlock];
+    float F[9][Cta];
+    float xpark[3][Cta];
     uint64_t pbar;
 };
 
-// G2P of the CTA whose particles start at p0 (a multiple of kBlock).
-template <bool Fused>
+// G2P of the CTA of Cta particles (and threads) that starts at p0 (a multiple
+// of Cta).
+template <bool Fused, int Cta = kBlock>
 __device__ __forceinline__ void g2p_body(const mpmw_particles_t &P, const mpmw_grid_t &G, const mpmw_params_t &prm,
                                          uint32_t *status, int *svd_list, int *svd_count, const CUtensorMap *tmap,
                                          int use_tma, int use_ahead, int64_t p0)
 {
-    __shared__ __align__(128) G2PShared S;
+    static_assert(Cta % 32 == 0 && Cta / 32 <= kGatherMaxWarps, "whole warps, within the gather's box slots");
+    __shared__ __align__(128) G2PShared<Cta> S;
     const int64_t n = P.n;
     const int t = threadIdx.x;
     const int64_t p = p0 + t;
     // F read ahead into shared memory by bulk copies (full CTAs; the host checks
     // the 16-byte alignment they need), in flight while the CTA waits for its tile
-    const bool ahead = use_ahead && p0 + kBlock <= n;
+    const bool ahead = use_ahead && p0 + Cta <= n;
     if (ahead && t == 0) {
         mbar_init(&S.pbar, 1);
-        mbar_arrive_expect_tx(&S.pbar, 9u * kBlock * 4u);
+        mbar_arrive_expect_tx(&S.pbar, 9u * Cta * 4u);
 #pragma unroll 1
-        for (int f = 0; f < 9; ++f) bulk_load(&S.F[f][0], P.F + (int64_t)f * n + p0, kBlock * 4u, &S.pbar);
+        for (int f = 0; f < 9; ++f) bulk_load(&S.F[f][0], P.F + (int64_t)f * n + p0, Cta * 4u, &S.pbar);
     }
     // labels and x are loaded together (not behind the label test)
     int lab_a = 0, lab_m = 0;
@@ -771,16 +774,17 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g_batc
                             (int64_t)(R.pcta_base + blockIdx.x) * kScatterChunk);
 }
 
-__global__ void __launch_bounds__(kBlock, 3) k_g2p_batch(mpmw_particles_t P, const BatchRef R,
+// the batch's particle CTAs are the scatter's (kScatterChunk particles), so the
+// scene table's CTA entries serve every batched particle kernel
+__global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p_batch(mpmw_particles_t P, const BatchRef R,
                                                      const __grid_constant__ BatchMaps M, uint32_t *status,
                                                      int use_ahead)
 {
-    static_assert(kBlock == kScatterChunk, "particle CTAs of the batched G2P and P2G kernels coincide");
     __shared__ BatchScene B;
     const int s = stage_scene(R, B, status);
     if (s < 0) return;
-    g2p_body<false>(P, B.grid, B.prm, status, nullptr, nullptr, &M.tmap[s], R.use_tma, use_ahead,
-                    (int64_t)(R.pcta_base + blockIdx.x) * kBlock);
+    g2p_body<false, kScatterChunk>(P, B.grid, B.prm, status, nullptr, nullptr, &M.tmap[s], R.use_tma, use_ahead,
+                                   (int64_t)(R.pcta_base + blockIdx.x) * kScatterChunk);
 }
 
 __global__ void __launch_bounds__(kBlock) k_stress_p2g_list_batch(mpmw_particles_t P, const BatchRef R,
@@ -878,6 +882,7 @@ int prepare_batch(const mpmw_particles_t &p, const mpmw_grid_t *grids, const mpm
         if (!cached_grid_map(grids[k], &maps->tmap[k])) use_tma = 0;
         sc[k].grid = grids[k];
         sc[k].prm = prms[k];
+        static_assert(256 % kScatterChunk == 0, "scene offsets (multiples of 256) fall on particle-CTA boundaries");
         for (int64_t b = offsets[k] / kScatterChunk; b < offsets[k + 1] / kScatterChunk; ++b) pcta[b] = k;
         nfirst[k] = c;
         const int nc = (int)scene_node_ctas(grids[k]);
@@ -1010,7 +1015,7 @@ int launch_batch_substeps(const mpmw_particles_t &p, int first, int last, int ns
         } else {
             k_grid_update_batch<<<nctas, kBlock, 0, s>>>(R, 0, st);
             MPMW_TRY_LAUNCH("k_grid_update_batch");
-            k_g2p_batch<<<pctas, kBlock, 0, s>>>(p, R, *bp.maps, st, bp.use_ahead_g2p);
+            k_g2p_batch<<<pctas, kScatterChunk, 0, s>>>(p, R, *bp.maps, st, bp.use_ahead_g2p);
             MPMW_TRY_LAUNCH("k_g2p_batch");
         }
     }

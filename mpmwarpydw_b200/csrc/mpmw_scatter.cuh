@@ -43,9 +43,14 @@
 
 namespace mpmw {
 
-constexpr int kScatterChunk = 256;   // particles (and threads) per CTA
+// Particles (and threads) per CTA of the scattering kernels.  128 rather than
+// 256: the same 24 warps per SM (6 CTAs at 80 registers), but each CTA barrier
+// waits for 4 warps instead of 8; measured 3.7 % faster for the fused substep
+// on the tunnel.  The shared memory of 6 CTAs must fit an SM: hence 512
+// counting-sort bins (a 128-particle CTA spans far fewer base cells).
+constexpr int kScatterChunk = 128;
 constexpr int kScatterCtasPerSm = 768 / kScatterChunk;  // resident CTAs the launch bounds aim at (80 registers)
-constexpr int kScatterBins = 1024;   // base cells of a CTA's box that the counting sort handles
+constexpr int kScatterBins = 512;    // base cells of a CTA's box that the counting sort handles
 
 constexpr int kScatterRec = 8;       // float4 records per particle
 

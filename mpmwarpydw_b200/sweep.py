@@ -121,7 +121,7 @@ class SceneBatch:
         return out
 
 
-_CHUNK = 256  # particles per CTA: scene offsets are multiples of this
+_CHUNK = 256  # scene offsets are multiples of this (the batch entry points require it)
 _TUNED = {}   # (scenes, log2 particles) -> (group count, kernel options) chosen by ConcatBatch.tune
 
 
