@@ -799,6 +799,50 @@ def run_profile_xpbd(k):
                                        "status_word": read_status(dev)}}))
 
 
+def run_xpbd_study(a):
+    """The XPBD step (utils/simulationRoutines.py:295-526) in its two forms --
+    one persistent cooperative launch and one launch per pass -- on the caving
+    block (509,696 particles, 35 % of them seeded as XPBD particles, 4
+    iterations): CUDA-event time of each step, the forms alternating, median
+    of 20 steps each after 3 warm-up steps.  One JSON line."""
+    import torch
+
+    from mpmwarpydw_b200 import _lib, domains
+    from mpmwarpydw_b200.bind import read_status
+    from mpmwarpydw_b200.engine import sort_particles
+    from mpmwarpydw_b200.utils import simulationRoutines as S
+    dev = torch.device("cuda", 0)
+    L = _lib.lib()
+    sim, mpm, xpbd = domains.build(domains.caving_block(), device=dev)
+    sort_particles(sim, mpm, xpbd)
+    g = torch.Generator(device=dev).manual_seed(5)
+    xp = torch.rand(sim.nPoints, generator=g, device=dev) < 0.35
+    sim.materialLabel.copy_(torch.where(xp, 2, sim.materialLabel))
+    S.run_mpm_substeps(sim, mpm, xpbd, 5)
+    times = {1: [], 0: []}
+    stream = torch.cuda.current_stream(dev)
+    try:
+        for rep in range(23):
+            for form in (1, 0):
+                _lib.check(L.mpmw_xpbd_set_options(form), "xpbd options")
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                S.xpbdSimulationStep(sim, mpm, xpbd, dev)
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                if rep >= 3:
+                    times[form].append(e0.elapsed_time(e1))
+    finally:
+        _lib.check(L.mpmw_xpbd_set_options(1), "xpbd options")
+    med = {f: sorted(t)[len(t) // 2] for f, t in times.items()}
+    print(json.dumps({"study": "XPBD step: one persistent launch vs one launch per pass",
+                      "workload": "caving block, 509,696 particles, 35 % XPBD particles, 4 iterations",
+                      "unit": "ms per XPBD step (median of 20)", "persistent": med[1], "per_pass": med[0],
+                      "persistent_launches": int(L.mpmw_xpbd_persistent_launches()),
+                      "xpbd_particles": int((sim.materialLabel == 2).sum().item()),
+                      "status_word": read_status(dev)}))
+
+
 def run_profile_mlp(n):
     """Tensor-core inference of the surrogate network on n samples (after a
     short training), for ncu captures of k_mlp_infer_tc; prints one line."""
@@ -857,9 +901,10 @@ def main():
     ap.add_argument("--variant-steps", type=int, default=50,
                     help="substeps of the getArgs-default (VLC + covariance) variant")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--study", choices=["resort"], default=None,
+    ap.add_argument("--study", choices=["resort", "xpbd"], default=None,
                     help="resort: the fused kernel's time over 2,000 caving-block substeps with and without "
-                         "re-sorting (prints its own JSON line, not a bench line)")
+                         "re-sorting; xpbd: the XPBD step as one persistent launch and as one launch per pass "
+                         "(each prints its own JSON line, not a bench line)")
     ap.add_argument("--workload", choices=["tunnel", "sweep"], default="tunnel",
                     help="tunnel: the 3,873,600-particle tunnel (replicas over ranks); sweep: the batched "
                          "64-scene parameter sweep (scenes sharded over ranks)")
@@ -879,6 +924,8 @@ def main():
         run_profile_mlp(a.profile_mlp)
     elif a.study == "resort":
         run_resort_study(a)
+    elif a.study == "xpbd":
+        run_xpbd_study(a)
     elif a.impl == "reference":
         run_reference(a)
     elif a.workload == "sweep":

@@ -97,9 +97,23 @@ int mpmw_xpbd_kernel(int which, const mpmw_particles_t *p, const mpmw_xpbd_t *x,
 size_t mpmw_xpbd_step_workspace_bytes(int64_t n, const int32_t *dims);
 /* utils/simulationRoutines.py:295-526 xpbdSimulationStep (hash build, integrate,
  * label reset, iterations x (bound, particle contacts, apply), sleep,
- * impulses + commit, swelling). */
+ * impulses + commit, swelling).
+ * With a workspace of mpmw_xpbd_step_workspace_bytes(n, h->dims) (256-byte
+ * aligned) the whole step is ONE persistent kernel: a cooperative launch of
+ * at most one full wave of CTAs that runs the hash build, the iterations and
+ * the closing passes as phases separated by grid barriers.  Each barrier wait
+ * is bounded (1 s); a CTA that gives up sets MPMW_ST_TIMEOUT in *status (may
+ * be NULL) and the launch ends early.  With a smaller workspace, or after
+ * mpmw_xpbd_set_options(0), one kernel per pass (hash build included).  Both
+ * forms give the same bits. */
 int mpmw_xpbd_step(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_hash_t *h,
-                   const mpmw_xpbd_params_t *q, void *workspace, size_t ws_bytes, mpmw_stream_t stream);
+                   const mpmw_xpbd_params_t *q, uint32_t *status, void *workspace, size_t ws_bytes,
+                   mpmw_stream_t stream);
+/* Process-wide form of mpmw_xpbd_step: persistent (1, the default) or one
+ * launch per pass (0). */
+int mpmw_xpbd_set_options(int persistent);
+/* Persistent launches mpmw_xpbd_step has made in this process. */
+int64_t mpmw_xpbd_persistent_launches(void);
 
 /* ---- the big step on the device (runMPMYDW.py:633-844) ------------------ */
 /* Phase 1 with its XPBD steps and gravity pulse inside one CUDA graph: a while
@@ -134,7 +148,8 @@ int mpmw_phase_loop_create(const mpmw_particles_t *p, const mpmw_grid_t *g, cons
  * mpmw_loop_launch, destroy with mpmw_loop_destroy. */
 int mpmw_xpbd_loop_create(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_hash_t *h,
                           const mpmw_xpbd_params_t *q, int max_steps, double sleep_ratio, mpmw_loop_state_t *state,
-                          void *xpbd_workspace, size_t xpbd_ws_bytes, mpmw_loop_t **out, mpmw_stream_t stream);
+                          uint32_t *status, void *xpbd_workspace, size_t xpbd_ws_bytes, mpmw_loop_t **out,
+                          mpmw_stream_t stream);
 
 #ifdef __cplusplus
 }

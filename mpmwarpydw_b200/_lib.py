@@ -139,7 +139,7 @@ _SIGS = {
                                     _P, _P, _P, ctypes.c_size_t, _P, ctypes.c_size_t,
                                     ctypes.POINTER(ctypes.c_void_p), _P]),
     "mpmw_xpbd_loop_create": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(XPBD), ctypes.POINTER(Hash),
-                                   ctypes.POINTER(XPBDParams), _I, ctypes.c_double, _P, _P, ctypes.c_size_t,
+                                   ctypes.POINTER(XPBDParams), _I, ctypes.c_double, _P, _P, _P, ctypes.c_size_t,
                                    ctypes.POINTER(ctypes.c_void_p), _P]),
     "mpmw_loop_launch": (_I, [_P, _P]),
     "mpmw_loop_destroy": (None, [_P]),
@@ -166,7 +166,9 @@ _SIGS = {
     "mpmw_xpbd_kernel": (_I, [_I, ctypes.POINTER(Particles), ctypes.POINTER(XPBD), ctypes.POINTER(Hash),
                               ctypes.POINTER(XPBDParams), _I, _P]),
     "mpmw_xpbd_step": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(XPBD), ctypes.POINTER(Hash),
-                            ctypes.POINTER(XPBDParams), _P, ctypes.c_size_t, _P]),
+                            ctypes.POINTER(XPBDParams), _P, _P, ctypes.c_size_t, _P]),
+    "mpmw_xpbd_set_options": (_I, [_I]),
+    "mpmw_xpbd_persistent_launches": (_I64, []),
 }
 
 _LIB = None

@@ -358,8 +358,8 @@ int mpmw_phase_loop_create(const mpmw_particles_t *p, const mpmw_grid_t *g, cons
         int e = mpmw_run_substeps(p, g, prm_pulse, r, status, workspace, ws_bytes, stream);
         return e == MPMW_OK ? mpmw_run_substeps(p, g, prm, k - r, status, workspace, ws_bytes, stream) : e;
     });
-    branch(3, [&]() { return mpmw_xpbd_step(p, x, h, q_pulse, xpbd_workspace, xpbd_ws_bytes, stream); });
-    branch(4, [&]() { return mpmw_xpbd_step(p, x, h, q, xpbd_workspace, xpbd_ws_bytes, stream); });
+    branch(3, [&]() { return mpmw_xpbd_step(p, x, h, q_pulse, status, xpbd_workspace, xpbd_ws_bytes, stream); });
+    branch(4, [&]() { return mpmw_xpbd_step(p, x, h, q, status, xpbd_workspace, xpbd_ws_bytes, stream); });
     if (rc == MPMW_OK)
         rc = capture_into(body, &last, s, [&]() {
             int e = mpmw_stats(p, state->stats, stream);
@@ -372,7 +372,8 @@ int mpmw_phase_loop_create(const mpmw_particles_t *p, const mpmw_grid_t *g, cons
 
 int mpmw_xpbd_loop_create(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_hash_t *h,
                           const mpmw_xpbd_params_t *q, int max_steps, double sleep_ratio, mpmw_loop_state_t *state,
-                          void *xpbd_workspace, size_t xpbd_ws_bytes, mpmw_loop_t **out, mpmw_stream_t stream)
+                          uint32_t *status, void *xpbd_workspace, size_t xpbd_ws_bytes, mpmw_loop_t **out,
+                          mpmw_stream_t stream)
 {
     if (!out) { set_error("xpbd loop: out is NULL"); return MPMW_E_ARG; }
     *out = nullptr;
@@ -387,7 +388,7 @@ int mpmw_xpbd_loop_create(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const
     int rc = make_while_graph(&graph, &body, &hw);
     if (rc != MPMW_OK) return rc;
     rc = capture_into(body, nullptr, s, [&]() {
-        int e = mpmw_xpbd_step(p, x, h, q, xpbd_workspace, xpbd_ws_bytes, stream);
+        int e = mpmw_xpbd_step(p, x, h, q, status, xpbd_workspace, xpbd_ws_bytes, stream);
         if (e != MPMW_OK) return e;
         k_xpbd_phase_decide<<<1, 32, 0, s>>>(state, x->counts, max_steps, sleep_ratio, hw);
         return check_launch("k_xpbd_phase_decide");

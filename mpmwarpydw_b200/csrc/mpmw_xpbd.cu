@@ -13,9 +13,12 @@
 //   query            = cells from trunc((p - r)/w) to trunc((p + r)/w) per axis
 //                      (at most dims cells per axis), x fastest, then y, then z;
 //                      within a cell, sorted order
+#include <atomic>
+#include <cstring>
 #include "mpmw_common.cuh"
 #include "mpmw_math.cuh"
 #include "mpmw_scan.cuh"
+#include "mpmw_tma.cuh"
 #include "../../include/mpmw_xpbd.h"
 
 namespace mpmw {
@@ -36,11 +39,10 @@ __device__ __forceinline__ int hash_index(const int *hd, int x, int y, int z)
 
 struct HashDims { int d[3]; };
 
-__global__ void k_hash_cells(const float *__restrict__ x, int64_t n, float inv, HashDims hd, int *__restrict__ keys,
-                             int *__restrict__ ids, int *__restrict__ point_cells)
+__device__ __forceinline__ void hash_cell_at(const float *x, int64_t n, float inv, const HashDims &hd,
+                                             int *keys, int *ids,
+                                             int *point_cells, int64_t p)
 {
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
     int cx = (int)(x[p] * inv), cy = (int)(x[n + p] * inv), cz = (int)(x[2 * n + p] * inv);
     int h = hash_index(hd.d, cx, cy, cz);
     keys[p] = h;
@@ -48,16 +50,29 @@ __global__ void k_hash_cells(const float *__restrict__ x, int64_t n, float inv, 
     if (point_cells) point_cells[p] = h;
 }
 
+__global__ void k_hash_cells(const float *__restrict__ x, int64_t n, float inv, HashDims hd, int *__restrict__ keys,
+                             int *__restrict__ ids, int *__restrict__ point_cells)
+{
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) hash_cell_at(x, n, inv, hd, keys, ids, point_cells, p);
+}
+
 // one bit per hash cell: set where a particle labelled XPBD lies (its cell
 // from the same positions and formula as k_hash_cells)
-__global__ void k_mark_xpbd_cells(mpmw_particles_t P, float inv, HashDims hd, unsigned *__restrict__ bits)
+__device__ __forceinline__ void mark_xpbd_cell_at(const mpmw_particles_t &P, float inv, const HashDims &hd,
+                                                  unsigned *bits, int64_t p)
 {
     const int64_t n = P.n;
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n || P.material[p] != 2) return;
+    if (P.material[p] != 2) return;
     int cx = (int)(P.x[p] * inv), cy = (int)(P.x[n + p] * inv), cz = (int)(P.x[2 * n + p] * inv);
     int h = hash_index(hd.d, cx, cy, cz);
     atomicOr(&bits[h >> 5], 1u << (h & 31));
+}
+
+__global__ void k_mark_xpbd_cells(mpmw_particles_t P, float inv, HashDims hd, unsigned *__restrict__ bits)
+{
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < P.n) mark_xpbd_cell_at(P, inv, hd, bits, p);
 }
 
 // ---------------------------------------------------------------------------
@@ -69,39 +84,55 @@ constexpr int kSortThreads = 256;
 constexpr int kSortRounds = 16;
 constexpr int kSortTile = kSortThreads * kSortRounds;  // 4096 items per tile
 
-// per-tile digit histogram, stored digit-major: hist[d * ntiles + tile]
-__global__ void __launch_bounds__(kSortThreads) k_radix_hist(const int *__restrict__ keys, int64_t n, int shift,
-                                                            int ntiles, int *__restrict__ hist)
+// per-tile digit histogram, stored digit-major: hist[d * ntiles + tile].
+// Every thread of a kSortThreads CTA calls it (it synchronizes the block,
+// last of all so that the CTA can go on to another tile).
+__device__ __forceinline__ void radix_hist_tile(int *h, const int *keys, int64_t n, int shift, int ntiles,
+                                                int *hist, int tile)
 {
-    __shared__ int h[kRadix];
     for (int i = threadIdx.x; i < kRadix; i += blockDim.x) h[i] = 0;
     __syncthreads();
-    int64_t base = (int64_t)blockIdx.x * kSortTile;
+    int64_t base = (int64_t)tile * kSortTile;
     for (int r = 0; r < kSortRounds; ++r) {
         int64_t i = base + (int64_t)r * kSortThreads + threadIdx.x;
         if (i < n) atomicAdd(&h[(keys[i] >> shift) & (kRadix - 1)], 1);
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) hist[(int64_t)d * ntiles + blockIdx.x] = h[d];
+    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) hist[(int64_t)d * ntiles + tile] = h[d];
+    __syncthreads();
 }
 
-// stable scatter: offsets[d * ntiles + tile] is the exclusive prefix of hist
-__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const int *__restrict__ kin, const int *__restrict__ vin,
-                                                               int64_t n, int shift, int ntiles,
-                                                               const int *__restrict__ offsets, int *__restrict__ kout,
-                                                               int *__restrict__ vout)
+__global__ void __launch_bounds__(kSortThreads) k_radix_hist(const int *__restrict__ keys, int64_t n, int shift,
+                                                            int ntiles, int *__restrict__ hist)
 {
-    constexpr int kWarps = kSortThreads / 32;
-    __shared__ int run[kRadix];            // items of each digit placed by earlier rounds
-    __shared__ int wcnt[kWarps][kRadix];   // per-warp digit counts of the current round
-    __shared__ int tile_off[kRadix];
+    __shared__ int h[kRadix];
+    radix_hist_tile(h, keys, n, shift, ntiles, hist, blockIdx.x);
+}
+
+constexpr int kSortWarps = kSortThreads / 32;
+struct RadixScatterShared {
+    int run[kRadix];               // items of each digit placed by earlier rounds
+    int wcnt[kSortWarps][kRadix];  // per-warp digit counts of the current round
+    int tile_off[kRadix];
+};
+
+// stable scatter of one tile: offsets[d * ntiles + tile] is the exclusive
+// prefix of hist.  Every thread of a kSortThreads CTA calls it.
+__device__ __forceinline__ void radix_scatter_tile(RadixScatterShared &S, const int *kin,
+                                                   const int *vin, int64_t n, int shift, int ntiles,
+                                                   const int *offsets, int *kout,
+                                                   int *vout, int tile)
+{
+    constexpr int kWarps = kSortWarps;
+    int *run = S.run, *tile_off = S.tile_off;
+    auto &wcnt = S.wcnt;
     for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
         run[d] = 0;
-        tile_off[d] = offsets[(int64_t)d * ntiles + blockIdx.x];
+        tile_off[d] = offsets[(int64_t)d * ntiles + tile];
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    int64_t base = (int64_t)blockIdx.x * kSortTile;
+    int64_t base = (int64_t)tile * kSortTile;
     for (int r = 0; r < kSortRounds; ++r) {
         for (int d = threadIdx.x; d < kWarps * kRadix; d += blockDim.x) (&wcnt[0][0])[d] = 0;
         __syncthreads();
@@ -132,13 +163,27 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const int *__res
     }
 }
 
-__global__ void k_cell_ranges(const int *__restrict__ skeys, int64_t n, int *__restrict__ starts, int *__restrict__ ends)
+__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const int *__restrict__ kin, const int *__restrict__ vin,
+                                                               int64_t n, int shift, int ntiles,
+                                                               const int *__restrict__ offsets, int *__restrict__ kout,
+                                                               int *__restrict__ vout)
 {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    __shared__ RadixScatterShared S;
+    radix_scatter_tile(S, kin, vin, n, shift, ntiles, offsets, kout, vout, blockIdx.x);
+}
+
+__device__ __forceinline__ void cell_range_at(const int *skeys, int64_t n, int *starts,
+                                              int *ends, int64_t i)
+{
     int c = skeys[i];
     if (i == 0 || skeys[i - 1] != c) starts[c] = (int)i;
     if (i == n - 1 || skeys[i + 1] != c) ends[c] = (int)(i + 1);
+}
+
+__global__ void k_cell_ranges(const int *__restrict__ skeys, int64_t n, int *__restrict__ starts, int *__restrict__ ends)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) cell_range_at(skeys, n, starts, ends, i);
 }
 
 static int64_t sort_tiles(int64_t n) { return (n + kSortTile - 1) / kSortTile; }
@@ -297,11 +342,10 @@ int hash_build(const float *x, int64_t n, const mpmw_hash_t &h, void *ws, size_t
 // flag bit1: write every particle (the wp.copy), else only integrated ones.
 // xpbd_count (optional, zeroed by the caller): receives the number of
 // particles labelled XPBD, active or not.
-__global__ void k_xpbd_integrate(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int flag,
+__device__ __forceinline__ void xpbd_integrate_at(int64_t p, mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int flag,
                                  int *xpbd_count = nullptr)
 {
     const int64_t n = P.n;
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int mat = p < n ? P.material[p] : 0;
     const bool integ = p < n && P.active[p] == 1 && mat == 2;
     if (xpbd_count) {
@@ -325,19 +369,28 @@ __global__ void k_xpbd_integrate(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_pa
     }
 }
 
-// xpbdRoutines.py:3-21
-__global__ void k_reset_labels(mpmw_particles_t P)
+__global__ void k_xpbd_integrate(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int flag,
+                                 int *xpbd_count = nullptr)
 {
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    xpbd_integrate_at((int64_t)blockIdx.x * blockDim.x + threadIdx.x, P, X, q, flag, xpbd_count);
+}
+
+// xpbdRoutines.py:3-21
+__device__ __forceinline__ void reset_labels_at(int64_t p, mpmw_particles_t P)
+{
     if (p >= P.n) return;
     if (P.active[p] == 1 && P.material[p] == 0) P.material[p] = 1;
 }
 
+__global__ void k_reset_labels(mpmw_particles_t P)
+{
+    reset_labels_at((int64_t)blockIdx.x * blockDim.x + threadIdx.x, P);
+}
+
 // xpbdRoutines.py:49-136; writes delta (the reference zeroes it first, then adds)
-__global__ void k_bound_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int accumulate)
+__device__ __forceinline__ void bound_contacts_at(int64_t p, mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int accumulate)
 {
     const int64_t n = P.n;
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     float acc[3] = {0.f, 0.f, 0.f};
     if (accumulate) load3(X.delta, n, p, acc);
@@ -375,6 +428,11 @@ __global__ void k_bound_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_pa
     store3(X.delta, n, p, acc);
 }
 
+__global__ void k_bound_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int accumulate)
+{
+    bound_contacts_at((int64_t)blockIdx.x * blockDim.x + threadIdx.x, P, X, q, accumulate);
+}
+
 // xpbdRoutines.py:138-219.  One thread per sorted position tid; the outer
 // checks use tid, the work uses the sorted point i (reference behaviour).
 // Each deltas[i] is owned by exactly one thread, so it is read-modify-written
@@ -393,15 +451,14 @@ __global__ void k_bound_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_pa
 // The records hold the same values (labels as of the kernel's start, which the
 // tests here cannot tell from the live ones: the lock only writes 0 over <= 1).
 template <bool Rec>
-__global__ void k_particle_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash_t H, mpmw_xpbd_params_t q,
+__device__ __forceinline__ void particle_contacts_at(int64_t tid, mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash_t H, mpmw_xpbd_params_t q,
                                     const int *xpbd_count = nullptr, const unsigned *xpbd_cells = nullptr,
-                                    const float4 *__restrict__ recA = nullptr,
-                                    const float4 *__restrict__ recB = nullptr)
+                                    const float4 *recA = nullptr,
+                                    const float4 *recB = nullptr)
 {
     const int64_t n = P.n;
-    int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= n) return;
-    if (xpbd_count && __ldg(xpbd_count) == 0) return;
+    if (xpbd_count && *(xpbd_count) == 0) return;
     if (P.active[tid] != 1) return;
     if (!(P.material[tid] >= 0)) return;
     int i = H.point_ids[tid];
@@ -430,64 +487,93 @@ __global__ void k_particle_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash
             for (int cy = ys; cy <= ye && !any; ++cy)
                 for (int cx = xs; cx <= xe && !any; ++cx) {
                     const int c = hash_index(hd, cx, cy, cz);
-                    any = (__ldg(&xpbd_cells[c >> 5]) >> (c & 31)) & 1u;
+                    any = (xpbd_cells[c >> 5] >> (c & 31)) & 1u;
                 }
         if (!any) return;
     }
-    for (int cz = zs; cz <= ze; ++cz)
-        for (int cy = ys; cy <= ye; ++cy)
-            for (int cx = xs; cx <= xe; ++cx) {
-                int c = hash_index(hd, cx, cy, cz);
-                int b = H.cell_starts[c], e = H.cell_ends[c];
-                for (int s = b; s < e; ++s) {
-                    int index, mat_j;
-                    float xj[3], rad_j, mass_j;
-                    if constexpr (Rec) {
-                        const float4 ra = recA[s], rb = recB[s];
-                        index = __float_as_int(rb.w);
-                        mass_j = rb.x;
-                        if (!(__float_as_int(rb.y) == 1 && index != i && mass_j > 0.f)) continue;
-                        mat_j = __float_as_int(rb.z);
-                        if (mat_i <= 1 && mat_j <= 1) continue;
-                        xj[0] = ra.x; xj[1] = ra.y; xj[2] = ra.z;
-                        rad_j = ra.w;
-                    } else {
-                        index = H.point_ids[s];
-                        if (!(P.active[index] == 1 && index != i && P.mass[index] > 0.f)) continue;
-                        mat_j = P.material[index];
-                        if (mat_i <= 1 && mat_j <= 1) continue;
-                        load3(X.x_int, n, index, xj);
-                        rad_j = P.radius[index];
-                        mass_j = P.mass[index];
-                    }
-                    float nn[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
-                    float d = len3(nn);
-                    float err = (d - rad) - rad_j;
-                    float w2 = 1.f / mass_j;
-                    float denom = w1 + w2;
-                    if (err <= q.cohesion && denom > 0.f) {
-                        if (q.lock == 1) {
-                            if (mat_i <= 1 && mat_j == 2) P.material[i] = 0;
-                            if (mat_i == 2 && mat_j <= 1) P.material[index] = 0;
-                        }
-                        float nu[3] = {nn[0] / d, nn[1] / d, nn[2] / d};
-                        float vj[3];
-                        load3(X.v_int, n, index, vj);
-                        float vrel[3] = {vi[0] - vj[0], vi[1] - vj[1], vi[2] - vj[2]};
-                        float ln = err / (1.f + (alpha * q.dt) * q.dt);
-                        float dn[3] = {nu[0] * ln, nu[1] * ln, nu[2] * ln};
-                        float vn = dot3(nu, vrel);
-                        if (fabsf(vn) < q.static_thr * rad) k_mu = q.static_friction;
-                        float vt[3] = {vrel[0] - nu[0] * vn, vrel[1] - nu[1] * vn, vrel[2] - nu[2] * vn};
-                        float lf = rmax(k_mu * ln, -len3(vt) * q.dt);
-                        float nv[3];
-                        normalize3(vt, nv);
-                        float df[3] = {nv[0] * lf, nv[1] * lf, nv[2] * lf};
+    // one candidate pair (i, index) that passed the activity and label tests
+    auto pair = [&](int index, int mat_j, const float *xj, float rad_j, float mass_j) {
+        float nn[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
+        float d = len3(nn);
+        float err = (d - rad) - rad_j;
+        float w2 = 1.f / mass_j;
+        float denom = w1 + w2;
+        if (err <= q.cohesion && denom > 0.f) {
+            if (q.lock == 1) {
+                if (mat_i <= 1 && mat_j == 2) P.material[i] = 0;
+                if (mat_i == 2 && mat_j <= 1) P.material[index] = 0;
+            }
+            float nu[3] = {nn[0] / d, nn[1] / d, nn[2] / d};
+            float vj[3];
+            load3(X.v_int, n, index, vj);
+            float vrel[3] = {vi[0] - vj[0], vi[1] - vj[1], vi[2] - vj[2]};
+            float ln = err / (1.f + (alpha * q.dt) * q.dt);
+            float dn[3] = {nu[0] * ln, nu[1] * ln, nu[2] * ln};
+            float vn = dot3(nu, vrel);
+            if (fabsf(vn) < q.static_thr * rad) k_mu = q.static_friction;
+            float vt[3] = {vrel[0] - nu[0] * vn, vrel[1] - nu[1] * vn, vrel[2] - nu[2] * vn};
+            float lf = rmax(k_mu * ln, -len3(vt) * q.dt);
+            float nv[3];
+            normalize3(vt, nv);
+            float df[3] = {nv[0] * lf, nv[1] * lf, nv[2] * lf};
 #pragma unroll
-                        for (int a = 0; a < 3; ++a) dl[a] = dl[a] + ((df[a] - dn[a]) / denom) * w1;
+            for (int a = 0; a < 3; ++a) dl[a] = dl[a] + ((df[a] - dn[a]) / denom) * w1;
+        }
+    };
+    // The walk visits the query box's cells x fastest, then y, then z, and
+    // each cell's slots in sorted order.
+    if constexpr (Rec) {
+        // One item ahead: the next cell's slot range and the next record are
+        // loaded before the current record is used, so their latencies overlap.
+        const int nqx = xe - xs + 1, nqy = ye - ys + 1, nqz = ze - zs + 1;
+        const int nq = (nqx > 0 && nqy > 0 && nqz > 0) ? nqx * nqy * nqz : 0;
+        int qx = 0, qy = 0, qz = 0;  // the next cell of the walk (offsets in the box)
+        int nb = 0, ne = 0;          // its slot range
+        auto next_range = [&]() {
+            const int c = hash_index(hd, xs + qx, ys + qy, zs + qz);
+            nb = H.cell_starts[c];
+            ne = H.cell_ends[c];
+            if (++qx == nqx) { qx = 0; if (++qy == nqy) { qy = 0; ++qz; } }
+        };
+        float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa;
+        int pre = -1;  // slot whose record pa, pb hold
+        if (nq > 0) next_range();
+        for (int kq = 0; kq < nq; ++kq) {
+            const int b = nb, e = ne;
+            if (kq + 1 < nq) next_range();
+            else nb = ne = 0;
+            if (b < e && pre != b) { pa = recA[b]; pb = recB[b]; pre = b; }
+            for (int s = b; s < e; ++s) {
+                const float4 ra = pa, rb = pb;
+                // the following record: this cell's next slot, or the next cell's first
+                const int sn = s + 1 < e ? s + 1 : (nb < ne ? nb : -1);
+                if (sn >= 0) { pa = recA[sn]; pb = recB[sn]; pre = sn; }
+                const int index = __float_as_int(rb.w);
+                const float mass_j = rb.x;
+                if (!(__float_as_int(rb.y) == 1 && index != i && mass_j > 0.f)) continue;
+                const int mat_j = __float_as_int(rb.z);
+                if (mat_i <= 1 && mat_j <= 1) continue;
+                const float xj[3] = {ra.x, ra.y, ra.z};
+                pair(index, mat_j, xj, ra.w, mass_j);
+            }
+        }
+    } else {
+        for (int cz = zs; cz <= ze; ++cz)
+            for (int cy = ys; cy <= ye; ++cy)
+                for (int cx = xs; cx <= xe; ++cx) {
+                    const int c = hash_index(hd, cx, cy, cz);
+                    const int b = H.cell_starts[c], e = H.cell_ends[c];
+                    for (int s = b; s < e; ++s) {
+                        const int index = H.point_ids[s];
+                        if (!(P.active[index] == 1 && index != i && P.mass[index] > 0.f)) continue;
+                        const int mat_j = P.material[index];
+                        if (mat_i <= 1 && mat_j <= 1) continue;
+                        float xj[3];
+                        load3(X.x_int, n, index, xj);
+                        pair(index, mat_j, xj, P.radius[index], P.mass[index]);
                     }
                 }
-            }
+    }
     float cur[3];
     load3(X.delta, n, i, cur);
 #pragma unroll
@@ -495,18 +581,26 @@ __global__ void k_particle_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash
     store3(X.delta, n, i, cur);
 }
 
+template <bool Rec>
+__global__ void __launch_bounds__(kBlock, 4) k_particle_contacts(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash_t H, mpmw_xpbd_params_t q,
+                                    const int *xpbd_count = nullptr, const unsigned *xpbd_cells = nullptr,
+                                    const float4 *__restrict__ recA = nullptr,
+                                    const float4 *__restrict__ recB = nullptr)
+{
+    particle_contacts_at<Rec>((int64_t)blockIdx.x * blockDim.x + threadIdx.x, P, X, H, q, xpbd_count, xpbd_cells, recA, recB);
+}
+
 // The fields the contact pass reads of its neighbours, one record per sorted
 // hash slot s (point i = point_ids[s]): (x_int, radius) and (mass, active,
 // material, i), so a neighbour walk reads contiguous memory in hash order.
 // Nothing to write when the step has no XPBD-labelled particle (xpbd_count):
 // the contact pass then reads no record.
-__global__ void k_contact_records(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash_t H, float4 *__restrict__ recA,
-                                  float4 *__restrict__ recB, const int *xpbd_count)
+__device__ __forceinline__ void contact_records_at(int64_t s, mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash_t H, float4 *recA,
+                                  float4 *recB, const int *xpbd_count)
 {
     const int64_t n = P.n;
-    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
-    if (xpbd_count && __ldg(xpbd_count) == 0) return;
+    if (xpbd_count && *(xpbd_count) == 0) return;
     const int i = H.point_ids[s];
     if (i < 0 || i >= n) {
         recA[s] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -519,16 +613,21 @@ __global__ void k_contact_records(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash_t
     recB[s] = make_float4(P.mass[i], __int_as_float(P.active[i]), __int_as_float(P.material[i]), __int_as_float(i));
 }
 
+__global__ void k_contact_records(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_hash_t H, float4 *__restrict__ recA,
+                                  float4 *__restrict__ recB, const int *xpbd_count)
+{
+    contact_records_at((int64_t)blockIdx.x * blockDim.x + threadIdx.x, P, X, H, recA, recB, xpbd_count);
+}
+
 // xpbdRoutines.py:221-257 my_apply_particle_deltas.  x_orig = particle x,
 // x_pred = x_int.  flag 0/1 (substep): the surrounding copies
 // (simulationRoutines.py:398-421) are folded in -- x_int/v_int are updated in
 // place, and with flag 1 the deltaInt buffers receive the same values for every
 // particle.  flag 2 (the kernel alone): results go to x_dI/v_dI for active
 // particles only, x_int/v_int are left untouched.
-__global__ void k_apply_deltas(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int flag)
+__device__ __forceinline__ void apply_deltas_at(int64_t p, mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int flag)
 {
     const int64_t n = P.n;
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     float xn[3], vn[3];
     load3(X.x_int, n, p, xn);
@@ -555,11 +654,15 @@ __global__ void k_apply_deltas(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_para
     }
 }
 
+__global__ void k_apply_deltas(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int flag)
+{
+    apply_deltas_at((int64_t)blockIdx.x * blockDim.x + threadIdx.x, P, X, q, flag);
+}
+
 // xpbdRoutines.py:312-334 sleepParticles (counts[0] total, counts[1] sleeping)
-__global__ void k_sleep(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q)
+__device__ __forceinline__ void sleep_at(int64_t p, mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q)
 {
     const int64_t n = P.n;
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool is = p < n && P.active[p] == 1 && P.material[p] == 2;
     bool slept = false;
     if (is) {
@@ -582,14 +685,18 @@ __global__ void k_sleep(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q)
     }
 }
 
+__global__ void k_sleep(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q)
+{
+    sleep_at((int64_t)blockIdx.x * blockDim.x + threadIdx.x, P, X, q);
+}
+
 // apply_mpm_contact_impulses (xpbdRoutines.py:259-310): x_orig/v_orig = particle
 // x/v, x_final = x_int, v_out = v_int.  With commit (the substep,
 // simulationRoutines.py:444-470) v_before_contact <- v first and x <- x_int,
 // v <- v_int after.
-__global__ void k_impulses_commit(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int commit)
+__device__ __forceinline__ void impulses_commit_at(int64_t p, mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int commit)
 {
     const int64_t n = P.n;
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     float x0[3], v0[3], xf[3], vf[3];
     load3(P.x, n, p, x0);
@@ -617,11 +724,15 @@ __global__ void k_impulses_commit(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_p
     }
 }
 
+__global__ void k_impulses_commit(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q, int commit)
+{
+    impulses_commit_at((int64_t)blockIdx.x * blockDim.x + threadIdx.x, P, X, q, commit);
+}
+
 // xpbdRoutines.py:354-375 swellParticlesType2
-__global__ void k_swell(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q)
+__device__ __forceinline__ void swell_at(int64_t p, mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q)
 {
     const int64_t n = P.n;
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     if (P.active[p] != 1 || P.material[p] != 2) return;
     float x[3], x0[3];
@@ -637,6 +748,198 @@ __global__ void k_swell(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q)
         float nr = br + ((sr - br) * (dxv - factor)) / (fmax - factor);
         nr = rmin(rmax(nr, P.radius[p]), sr);
         P.radius[p] = nr;
+    }
+}
+
+__global__ void k_swell(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q)
+{
+    swell_at((int64_t)blockIdx.x * blockDim.x + threadIdx.x, P, X, q);
+}
+
+
+// ---------------------------------------------------------------------------
+// The XPBD step as one persistent kernel (cooperative launch: every CTA of the
+// grid is resident at once).  Phases are separated by grid barriers; within a
+// phase each CTA takes elements (or sort tiles) strided by the grid, and each
+// element runs the same device function as the multi-launch step, so the two
+// forms give the same bits.
+// ---------------------------------------------------------------------------
+constexpr int kPersistThreads = kSortThreads;                     // 256
+constexpr uint64_t kGridSyncWaitNs = 1000ull * 1000ull * 1000ull;  // 1 s per barrier at most
+constexpr unsigned kGridSyncMaxPolls = 1u << 24;
+constexpr int kPersistMaxCtas = 4000;                              // chunk sums of the in-kernel scan
+constexpr size_t kPersistHeaderBytes = 16384;                      // arrival counter, XPBD count, tile tickets, chunk sums
+
+// Grid-wide barrier on a monotonically increasing arrival counter (zeroed
+// before the launch): each CTA adds one and waits until the count reaches the
+// next multiple of gridDim.x.  The wait is bounded (kGridSyncWaitNs of
+// %globaltimer and kGridSyncMaxPolls polls); a CTA that gives up reports
+// MPMW_ST_TIMEOUT and the call returns false in all its threads, after which
+// the kernel returns (the other CTAs then give up at their next barrier).
+__device__ __forceinline__ bool grid_sync(unsigned *arrive, uint32_t *status, int *s_ok)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned old = atomicAdd(arrive, 1u);
+        const unsigned target = (old / gridDim.x + 1u) * gridDim.x;
+        int ok = 1;
+        const uint64_t t0 = globaltimer_ns();
+        unsigned polls = 0;
+        for (;;) {
+            unsigned now;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(now) : "l"(arrive) : "memory");
+            if ((int)(now - target) >= 0) break;
+            if (++polls > kGridSyncMaxPolls || globaltimer_ns() - t0 > kGridSyncWaitNs) {
+                ok = 0;
+                raise_status(status, MPMW_ST_TIMEOUT);
+                break;
+            }
+            if (polls > 32) __nanosleep(64);
+        }
+        __threadfence();
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+struct PersistArgs {
+    mpmw_particles_t P;
+    mpmw_xpbd_t X;
+    mpmw_hash_t H;
+    mpmw_xpbd_params_t q, qi;  // step parameters; those of the iterations (no lock in XPBD-only steps)
+    HashDims hd;
+    float inv;                 // 1 / cell width
+    int64_t ncell;
+    int64_t bit_words;         // words of the per-cell XPBD bits (0: no bits)
+    int passes, ntiles;        // radix passes (7 bits each), sort tiles
+    int64_t hist_n;            // kRadix * ntiles
+    int *keys_a, *keys_b, *ids_scratch, *hist, *offs;
+    int *chunk_sums;           // one per CTA
+    unsigned *arrive;
+    int *tickets;              // contact-pass tiles drawn so far (all iterations)
+    int *xpbd_count;
+    unsigned *xpbd_cells;
+    float4 *recA, *recB;
+    uint32_t *status;
+    int reset_labels;
+};
+
+union PersistShared {
+    int h[kRadix];
+    RadixScatterShared sc;
+};
+
+// The next tile of a dynamically scheduled phase for this CTA: one ticket
+// per draw from a counter that only grows, `base` tickets drawn by earlier
+// such phases (each phase draws its tiles plus one final ticket per CTA).
+__device__ __forceinline__ int draw_tile(int *tickets, int base, int *s_tile)
+{
+    if (threadIdx.x == 0) *s_tile = atomicAdd(tickets, 1) - base;
+    __syncthreads();
+    const int t = *s_tile;
+    __syncthreads();
+    return t;
+}
+
+// Exclusive scan of hist[0, hist_n) into offs inside the persistent kernel:
+// each CTA sums a contiguous chunk, then (after a barrier) scans its chunk on
+// top of the earlier chunks' sums.  Every thread of every CTA calls it.
+__device__ __forceinline__ bool persist_scan(const PersistArgs &A, int *s_ok)
+{
+    const int64_t L = (A.hist_n + gridDim.x - 1) / gridDim.x;
+    const int64_t c0 = (int64_t)blockIdx.x * L;
+    const int64_t c1 = c0 + L < A.hist_n ? c0 + L : A.hist_n;
+    int part = 0, total = 0;
+    for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) part += A.hist[i];
+    block_excl_scan<kPersistThreads>(part, &total);
+    if (threadIdx.x == 0) A.chunk_sums[blockIdx.x] = total;
+    if (!grid_sync(A.arrive, A.status, s_ok)) return false;
+    part = 0;
+    for (int k = threadIdx.x; k < (int)blockIdx.x; k += blockDim.x) part += A.chunk_sums[k];
+    int prefix = 0;
+    block_excl_scan<kPersistThreads>(part, &prefix);
+    for (int64_t b = c0; b < c1; b += blockDim.x) {
+        const int64_t i = b + threadIdx.x;
+        const int v = i < c1 ? A.hist[i] : 0;
+        int tot = 0;
+        const int ex = block_excl_scan<kPersistThreads>(v, &tot);
+        if (i < c1) A.offs[i] = prefix + ex;
+        prefix += tot;
+    }
+    return grid_sync(A.arrive, A.status, s_ok);
+}
+
+// utils/simulationRoutines.py:295-526 in one launch: hash build (keys, radix
+// passes, cell ranges), XPBD cell bits, integration, label reset, the Jacobi
+// iterations (bound contacts and contact records; particle contacts; apply),
+// then sleeping, impulses with the commit, and swelling.
+__global__ void __launch_bounds__(kPersistThreads) k_xpbd_step_persistent(const __grid_constant__ PersistArgs A)
+{
+    __shared__ PersistShared sh;
+    __shared__ int s_ok, s_tile;
+    const int64_t n = A.P.n;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t b0 = (int64_t)blockIdx.x * blockDim.x;  // a CTA-uniform loop start, so warp votes see full warps
+    // the sorted ids end in point_ids after the last pass
+    int *ids0 = (A.passes & 1) ? A.ids_scratch : A.H.point_ids;
+    {
+        const int64_t m0 = n > A.ncell ? n : A.ncell;
+        const int64_t m = m0 > A.bit_words ? m0 : A.bit_words;
+        for (int64_t b = b0; b < m; b += stride) {
+            const int64_t e = b + threadIdx.x;
+            if (e < A.ncell) { A.H.cell_starts[e] = 0; A.H.cell_ends[e] = 0; }
+            if (e < A.bit_words) A.xpbd_cells[e] = 0u;
+            if (e < n) hash_cell_at(A.P.x, n, A.inv, A.hd, A.keys_a, ids0, A.H.point_cells, e);
+        }
+    }
+    if (!grid_sync(A.arrive, A.status, &s_ok)) return;
+    int *ki = A.keys_a, *vi = ids0, *ko = A.keys_b, *vo = (A.passes & 1) ? A.H.point_ids : A.ids_scratch;
+    for (int pass = 0; pass < A.passes; ++pass) {
+        const int shift = pass * kRadixBits;
+        for (int t = blockIdx.x; t < A.ntiles; t += gridDim.x) radix_hist_tile(sh.h, ki, n, shift, A.ntiles, A.hist, t);
+        if (!grid_sync(A.arrive, A.status, &s_ok)) return;
+        if (!persist_scan(A, &s_ok)) return;
+        for (int t = blockIdx.x; t < A.ntiles; t += gridDim.x)
+            radix_scatter_tile(sh.sc, ki, vi, n, shift, A.ntiles, A.offs, ko, vo, t);
+        if (!grid_sync(A.arrive, A.status, &s_ok)) return;
+        int *tk = ki; ki = ko; ko = tk;
+        int *tv = vi; vi = vo; vo = tv;
+    }
+    for (int64_t b = b0; b < n; b += stride) {
+        const int64_t p = b + threadIdx.x;
+        if (p < n) {
+            cell_range_at(ki, n, A.H.cell_starts, A.H.cell_ends, p);
+            if (A.bit_words) mark_xpbd_cell_at(A.P, A.inv, A.hd, A.xpbd_cells, p);
+        }
+        xpbd_integrate_at(p, A.P, A.X, A.q, 3, A.xpbd_count);
+        if (A.reset_labels) reset_labels_at(p, A.P);
+    }
+    if (!grid_sync(A.arrive, A.status, &s_ok)) return;
+    const int iters = A.qi.iterations;
+    for (int it = 0; it < iters; ++it) {
+        for (int64_t p = b0 + threadIdx.x; p < n; p += stride) {
+            bound_contacts_at(p, A.P, A.X, A.qi, 0);
+            contact_records_at(p, A.P, A.X, A.H, A.recA, A.recB, A.xpbd_count);
+        }
+        if (!grid_sync(A.arrive, A.status, &s_ok)) return;
+        // the neighbour walks vary in length: tiles are handed out as CTAs free up
+        const int ctiles = (int)((n + blockDim.x - 1) / blockDim.x);
+        for (int t = draw_tile(A.tickets, it * (ctiles + (int)gridDim.x), &s_tile); t < ctiles;
+             t = draw_tile(A.tickets, it * (ctiles + (int)gridDim.x), &s_tile))
+            particle_contacts_at<true>((int64_t)t * blockDim.x + threadIdx.x, A.P, A.X, A.H, A.qi, A.xpbd_count,
+                                       A.xpbd_cells, A.recA, A.recB);
+        if (!grid_sync(A.arrive, A.status, &s_ok)) return;
+        for (int64_t p = b0 + threadIdx.x; p < n; p += stride) apply_deltas_at(p, A.P, A.X, A.qi, it == iters - 1);
+        if (it < iters - 1 && !grid_sync(A.arrive, A.status, &s_ok)) return;
+    }
+    // each particle's own values only from here on (its thread applied its deltas)
+    for (int64_t b = b0; b < n; b += stride) {
+        const int64_t p = b + threadIdx.x;
+        sleep_at(p, A.P, A.X, A.q);
+        impulses_commit_at(p, A.P, A.X, A.q, 1);
+        if (A.q.swelling_ratio > 0.f) swell_at(p, A.P, A.X, A.q);
     }
 }
 
@@ -702,13 +1005,32 @@ static size_t xpbd_bits_bytes(const int32_t *dims)
 }
 static size_t xpbd_records_offset(const int32_t *dims) { return (256 + xpbd_bits_bytes(dims) + 255) / 256 * 256; }
 
+// Workspace of the persistent step: a header (arrival counter, XPBD count, tile tickets,
+// chunk sums of the in-kernel scan), the per-cell XPBD bits, then one area
+// that holds the sort's buffers until the cell ranges are built and the
+// contact records after that.
+static size_t al256(size_t b) { return (b + 255) / 256 * 256; }
+static size_t persist_area_offset(const int32_t *dims) { return al256(kPersistHeaderBytes + xpbd_bits_bytes(dims)); }
+static size_t persist_sort_bytes(int64_t n)
+{
+    const int64_t hist_n = (int64_t)kRadix * sort_tiles(n);
+    return al256(4 * (size_t)n) * 3 + al256(4 * (size_t)hist_n) * 2;
+}
+static size_t persist_workspace_bytes(int64_t n, const int32_t *dims)
+{
+    const size_t sort = persist_sort_bytes(n), rec = 2 * (size_t)n * sizeof(float4);
+    return persist_area_offset(dims) + (sort > rec ? sort : rec);
+}
+
 size_t mpmw_xpbd_step_workspace_bytes(int64_t n, const int32_t *dims)
 {
     if (n < 0) n = 0;
     const size_t hash = mpmw::hash_workspace_bytes(n);
     if (!dims) return hash;
     const size_t step = xpbd_records_offset(dims) + 2 * (size_t)n * sizeof(float4);
-    return hash > step ? hash : step;
+    const size_t pers = persist_workspace_bytes(n, dims);
+    const size_t m = hash > step ? hash : step;
+    return m > pers ? m : pers;
 }
 
 int mpmw_hash_build(const float *x, int64_t n, const mpmw_hash_t *h, void *workspace, size_t ws_bytes,
@@ -753,13 +1075,121 @@ int mpmw_xpbd_kernel(int which, const mpmw_particles_t *p, const mpmw_xpbd_t *x,
     return check_launch("xpbd kernel");
 }
 
+// process-wide choice of the step's form (1: one persistent launch where the
+// workspace and the device allow it; 0: one launch per pass)
+static std::atomic<int> g_xpbd_persistent{1};
+static std::atomic<int64_t> g_xpbd_persistent_launches{0};
+
+int64_t mpmw_xpbd_persistent_launches(void) { return g_xpbd_persistent_launches.load(); }
+
+int mpmw_xpbd_set_options(int persistent)
+{
+    g_xpbd_persistent.store(persistent ? 1 : 0);
+    return MPMW_OK;
+}
+
+// CTAs of the persistent step's cooperative grid on the current device (0: the
+// device cannot launch it)
+static int persist_grid_capacity()
+{
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 0;
+    if (dev < 64) {
+        const int c = cache[dev].load();
+        if (c != 0) return c > 0 ? c : 0;
+    }
+    int coop = 0, sms = 0, per_sm = 0;
+    int cap = -1;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && coop &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_xpbd_step_persistent, kPersistThreads, 0) ==
+            cudaSuccess &&
+        per_sm > 0) {
+        cap = per_sm * sms;
+        if (cap > kPersistMaxCtas) cap = kPersistMaxCtas;
+    }
+    cudaGetLastError();
+    if (dev < 64) cache[dev].store(cap);
+    return cap > 0 ? cap : 0;
+}
+
+// The whole step as one cooperative launch of k_xpbd_step_persistent.
+static int xpbd_step_persistent(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_hash_t *h,
+                                const mpmw_xpbd_params_t *q, uint32_t *status, void *workspace, int grid,
+                                cudaStream_t s)
+{
+    const int64_t n = p->n;
+    if (!x->cum_dist) { set_error("sleep: cum_dist is required"); return MPMW_E_ARG; }
+    if (q->swelling_ratio > 0.f && (!x->base_radius || !x->max_radius || !p->x_pc)) {
+        set_error("swell: radii and x_pc are required");
+        return MPMW_E_ARG;
+    }
+    PersistArgs A;
+    memset(&A, 0, sizeof(A));
+    A.P = *p;
+    A.X = *x;
+    A.H = *h;
+    A.q = *q;
+    A.qi = *q;
+    if (q->xpbd_only) A.qi.lock = 0;
+    A.reset_labels = q->lock && !q->xpbd_only;
+    A.hd = HashDims{{h->dims[0], h->dims[1], h->dims[2]}};
+    A.inv = 1.0f / h->cell_width;
+    A.ncell = (int64_t)h->dims[0] * h->dims[1] * h->dims[2];
+    A.bit_words = (A.ncell + 31) / 32;
+    int bits = 0;
+    for (int64_t c = A.ncell - 1; c > 0; c >>= 1) ++bits;
+    A.passes = (bits + kRadixBits - 1) / kRadixBits;
+    A.ntiles = (int)sort_tiles(n);
+    A.hist_n = (int64_t)kRadix * A.ntiles;
+    char *w = static_cast<char *>(workspace);
+    A.arrive = reinterpret_cast<unsigned *>(w);
+    A.xpbd_count = reinterpret_cast<int *>(w) + 1;
+    A.tickets = reinterpret_cast<int *>(w) + 2;
+    A.chunk_sums = reinterpret_cast<int *>(w) + 64;
+    A.xpbd_cells = reinterpret_cast<unsigned *>(w + kPersistHeaderBytes);
+    char *area = w + persist_area_offset(h->dims);
+    A.keys_a = reinterpret_cast<int *>(area);
+    A.keys_b = reinterpret_cast<int *>(area + al256(4 * (size_t)n));
+    A.ids_scratch = reinterpret_cast<int *>(area + 2 * al256(4 * (size_t)n));
+    A.hist = reinterpret_cast<int *>(area + 3 * al256(4 * (size_t)n));
+    A.offs = reinterpret_cast<int *>(area + 3 * al256(4 * (size_t)n) + al256(4 * (size_t)A.hist_n));
+    A.recA = reinterpret_cast<float4 *>(area);
+    A.recB = A.recA + n;
+    A.status = status;
+    if (cudaMemsetAsync(w, 0, 3 * sizeof(int), s) != cudaSuccess ||
+        (x->counts && cudaMemsetAsync(x->counts, 0, 2 * sizeof(int), s) != cudaSuccess)) {
+        set_error("xpbd_step: memset failed");
+        return MPMW_E_DEVICE;
+    }
+    void *args[] = {&A};
+    if (cudaLaunchCooperativeKernel((const void *)k_xpbd_step_persistent, dim3((unsigned)grid), dim3(kPersistThreads),
+                                    args, 0, s) != cudaSuccess) {
+        set_error("xpbd_step: cooperative launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+        return MPMW_E_DEVICE;
+    }
+    g_xpbd_persistent_launches.fetch_add(1);
+    return MPMW_OK;
+}
+
 int mpmw_xpbd_step(const mpmw_particles_t *p, const mpmw_xpbd_t *x, const mpmw_hash_t *h,
-                   const mpmw_xpbd_params_t *q, void *workspace, size_t ws_bytes, mpmw_stream_t stream)
+                   const mpmw_xpbd_params_t *q, uint32_t *status, void *workspace, size_t ws_bytes,
+                   mpmw_stream_t stream)
 {
     TRY(check_xpbd_args(p, x, q));
     TRY(check_hash(h, p->n));
     if (p->n == 0) return MPMW_OK;
     cudaStream_t s = as_stream(stream);
+    if (g_xpbd_persistent.load() && workspace && ws_bytes >= persist_workspace_bytes(p->n, h->dims) &&
+        (reinterpret_cast<uintptr_t>(workspace) & 255u) == 0) {
+        const int cap = persist_grid_capacity();
+        if (cap > 0) {
+            const int64_t work = (p->n + kPersistThreads - 1) / kPersistThreads;
+            const int grid = (int)(work < cap ? (work > 0 ? work : 1) : cap);
+            return xpbd_step_persistent(p, x, h, q, status, workspace, grid, s);
+        }
+    }
     TRY(mpmw_hash_build(p->x, p->n, h, workspace, ws_bytes, stream));
     // The hash build's scratch is free again: its first int counts the
     // particles labelled XPBD, which lets the contact passes skip a step

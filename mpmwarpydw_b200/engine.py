@@ -338,8 +338,9 @@ class XPBDLoop(DeviceLoop):
         self.handle = ctypes.c_void_p()
         _lib.check(_lib.lib().mpmw_xpbd_loop_create(ctypes.byref(P), ctypes.byref(X), ctypes.byref(H),
                                                     ctypes.byref(Q), int(max_steps), float(sleep_ratio),
-                                                    self.state.data_ptr(), xw.data_ptr(), xw.numel(),
-                                                    ctypes.byref(self.handle), stream_handle(self.stream)),
+                                                    self.state.data_ptr(), status_word(sim.device).data_ptr(),
+                                                    xw.data_ptr(), xw.numel(), ctypes.byref(self.handle),
+                                                    stream_handle(self.stream)),
                    "xpbd_loop_create")
 
     def run_steps(self, done, budget):

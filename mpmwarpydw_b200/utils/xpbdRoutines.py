@@ -14,7 +14,7 @@ import ctypes
 import torch
 
 from .. import _lib
-from ..bind import Marshal, particles_from_states, particles_struct, ptr, stream_handle
+from ..bind import Marshal, particles_from_states, particles_struct, ptr, status_word, stream_handle
 from ..state import F32, I32
 
 __all__ = ["HashGrid", "reset_mpm_contact_labels", "integrateParticlesXPBD", "my_solve_particle_bound_contacts",
@@ -290,5 +290,6 @@ def xpbd_step(sim, mpm, xpbd, xpbd_only=False):
     hg._ensure(sim.nPoints)
     hg.n = sim.nPoints
     ws = hg.workspace()
-    _lib.check(_lib.lib().mpmw_xpbd_step(P, X, hg.struct(), q, ws.data_ptr(), ws.numel(), stream_handle()),
+    _lib.check(_lib.lib().mpmw_xpbd_step(P, X, hg.struct(), q, status_word(sim.device).data_ptr(), ws.data_ptr(),
+                                         ws.numel(), stream_handle()),
                "xpbdSimulationStep")

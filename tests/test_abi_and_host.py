@@ -53,7 +53,7 @@ def test_particle_counts_beyond_32_bits_are_rejected():
     for i in range(3):
         H.dims[i] = 8
     H.cell_width = 1.0
-    rc = L.mpmw_xpbd_step(ctypes.byref(P), ctypes.byref(X), ctypes.byref(H), ctypes.byref(q), None, 0, None)
+    rc = L.mpmw_xpbd_step(ctypes.byref(P), ctypes.byref(X), ctypes.byref(H), ctypes.byref(q), None, None, 0, None)
     assert rc == 1 and b"2147483647" in L.mpmw_last_error()
     rc = L.mpmw_hash_build(None, big, ctypes.byref(H), None, 0, None)
     assert rc == 1 and b"2147483647" in L.mpmw_last_error()
