@@ -657,11 +657,16 @@ def run_sweep(a):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded sweep scenes)",
         "config": {"workload": "batched sweep: 64 Drucker-Prager block collapses (10 m cubes, 20,000-500,000 "
                                "particles, friction angle U(20,45) deg, cohesion log-uniform [0.1,5] MPa, seed 4), "
-                               "scenes sharded over ranks by particle count, one launch per kernel over a rank's "
-                               "scenes, K substeps of every scene per timed call",
+                               "scenes sharded over ranks by particle count, a rank's scenes in the tuned form (one "
+                               "persistent launch, or one launch per kernel per scene group), K substeps of every "
+                               "scene per timed call",
                    "particles_total": int(sum(counts)), "particles_rank0": N, "scenes_rank0": len(mine),
                    "grid_nodes_rank0": G, "tuned": {"groups": b.groups, "gather_tile": b.options[0],
-                                                    "read_ahead": b.options[1]},
+                                                    "read_ahead": b.options[1],
+                                                    "form": "one persistent launch for the fused substeps"
+                                                    if b.groups == 0 else "one launch per kernel per scene group",
+                                                    "candidates": {f"groups={g},tile={o[0]},ahead={o[1]}": r
+                                                                   for (g, o), r in b.tuning.items()}},
                    "l2": "working set > 126 MB L2, no flush", "parallelism": f"scene shards x{world}"},
         "roofline": {"bound": "hbm", "kernel": "whole batched substep (fused G2P/return map/P2G + grid pass)",
                      "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "traffic": None,

@@ -222,6 +222,20 @@ int mpmw_batch_run_substeps(const mpmw_particles_t *p, int nsteps, uint32_t *sta
  * measured by sweep.ConcatBatch.tune). */
 int mpmw_batch_run_range(const mpmw_particles_t *p, int first_scene, int last_scene, int nsteps, uint32_t *status,
                          void *workspace, size_t ws_bytes, mpmw_stream_t stream);
+/* The same nsteps substeps of every scene with the fused substeps of all
+ * scenes in ONE persistent kernel: a cooperative launch of at most one full
+ * wave that runs, per substep, the grid update of every scene's grid, the
+ * fused G2P -> return map -> P2G of every scene's particles (particle tiles
+ * handed out as CTAs free up) and the SVD worklist, separated by grid
+ * barriers.  Before it, the prologue (grids cleared, the first return map and
+ * P2G); after it, the last grid update and G2P.  Same results as
+ * mpmw_batch_run_substeps.  Each barrier wait is bounded (1 s): a CTA that
+ * gives up sets MPMW_ST_TIMEOUT and the launch ends early.  Not to be run
+ * concurrently with another persistent launch. */
+int mpmw_batch_run_persistent(const mpmw_particles_t *p, int nsteps, uint32_t *status, void *workspace,
+                              size_t ws_bytes, mpmw_stream_t stream);
+/* Persistent batch launches made in this process. */
+int64_t mpmw_batch_persistent_launches(void);
 
 /* ---- particle order ------------------------------------------------------ */
 /* No counterpart in the reference (its kernels do not depend on particle

@@ -168,6 +168,8 @@ _SIGS = {
     "mpmw_xpbd_step": (_I, [ctypes.POINTER(Particles), ctypes.POINTER(XPBD), ctypes.POINTER(Hash),
                             ctypes.POINTER(XPBDParams), _P, _P, ctypes.c_size_t, _P]),
     "mpmw_xpbd_set_options": (_I, [_I]),
+    "mpmw_batch_run_persistent": (_I, [ctypes.POINTER(Particles), _I, _P, _P, ctypes.c_size_t, _P]),
+    "mpmw_batch_persistent_launches": (_I64, []),
     "mpmw_xpbd_persistent_launches": (_I64, []),
 }
 

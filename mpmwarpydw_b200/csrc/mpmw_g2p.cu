@@ -18,6 +18,7 @@
 //   particles go to the same worklist and k_stress_p2g_list.
 // The worklists live in the caller's workspace (mpmw_workspace_bytes).
 #include <atomic>
+#include <cstring>
 #include <memory>
 #include <mutex>
 #include <unordered_map>
@@ -25,6 +26,7 @@
 
 #include "mpmw_common.cuh"
 #include "mpmw_gather.cuh"
+#include "mpmw_gridsync.cuh"
 #include "mpmw_grid.cuh"
 #include "mpmw_internal.cuh"
 #include "mpmw_math.cuh"
@@ -246,7 +248,7 @@ __device__ __forceinline__ const float *ahead_src(const mpmw_particles_t &P, int
 template <bool StoreStress>
 __device__ __forceinline__ void g2p2g_body(const mpmw_particles_t &P, const mpmw_grid_t &G, const mpmw_params_t &prm,
                                            uint32_t *status, int *svd_list, int *svd_count, const CUtensorMap *tmap,
-                                           int use_tma, int use_ahead, int64_t p0)
+                                           int use_tma, int use_ahead, int64_t p0, bool store_rt = false)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     // the TMA destination (S.g.tile) must be 128-byte aligned: round the base up
@@ -339,7 +341,7 @@ __device__ __forceinline__ void g2p2g_body(const mpmw_particles_t &P, const mpmw
             add_viscous(T, nC, eta_s, eta_b, out);
             store9(P.F, n, p, Fo);
             st6[0] = out[0]; st6[1] = out[4]; st6[2] = out[8]; st6[3] = out[1]; st6[4] = out[2]; st6[5] = out[5];
-            if (StoreStress || rm == 2) store_sym6(P.stress, n, p, out);
+            if (StoreStress || store_rt || rm == 2) store_sym6(P.stress, n, p, out);
             if (rm == 2) {
                 // became an XPBD particle: it leaves the MPM path with this G2P's v and C
                 store3(P.v, n, p, nv);
@@ -697,9 +699,9 @@ __device__ __forceinline__ bool bad_scene(int s, const BatchRef &R, uint32_t *st
 // scene's record copied into `rec` (published by the barrier); -1 (for the
 // whole CTA, before any barrier, reported in *status) if the table holds no
 // valid scene index.
-__device__ __forceinline__ int stage_scene(const BatchRef &R, BatchScene &rec, uint32_t *status)
+__device__ __forceinline__ int stage_scene_at(const BatchRef &R, int pcta, BatchScene &rec, uint32_t *status)
 {
-    const int s = R.pcta_scene[R.pcta_base + blockIdx.x];
+    const int s = R.pcta_scene[pcta];
     if (bad_scene(s, R, status)) return -1;  // uniform: every thread read the same entry
     constexpr int kWords = (int)(sizeof(BatchScene) / 4);
     if (threadIdx.x < kWords)
@@ -708,49 +710,69 @@ __device__ __forceinline__ int stage_scene(const BatchRef &R, BatchScene &rec, u
     return s;
 }
 
+__device__ __forceinline__ int stage_scene(const BatchRef &R, BatchScene &rec, uint32_t *status)
+{
+    return stage_scene_at(R, R.pcta_base + blockIdx.x, rec, status);
+}
+
 // Grid-node CTAs of the batch cover kBatchNodesPerCta nodes of one scene each
 // (kBatchNodesPerThread per thread, kBlock apart), so the scene lookup is paid
 // once per 2048 nodes.
 constexpr int kBatchNodesPerThread = 8;
 constexpr int kBatchNodesPerCta = kBlock * kBatchNodesPerThread;
 
-__global__ void __launch_bounds__(kBlock) k_zero_grid_batch(const BatchRef R, uint32_t *status)
+// One grid-node entry b of the table (kBatchNodesPerCta nodes of one scene),
+// by the blockDim.x threads of a CTA (kBatchNodesPerCta / blockDim.x nodes
+// each, blockDim.x apart).
+__device__ __forceinline__ void zero_grid_entry(const BatchRef &R, int b, uint32_t *status)
 {
-    const int b = R.ncta_base + blockIdx.x;
     const int s = R.ncta_scene[b];
     if (bad_scene(s, R, status)) return;
     const mpmw_grid_t G = R.scene[s].grid;
     const int64_t total = (int64_t)G.dims[0] * G.dims[1] * G.dims[2];
     const int64_t g0 = (int64_t)(b - R.ncta_first[s]) * kBatchNodesPerCta + threadIdx.x;
-#pragma unroll
-    for (int u = 0; u < kBatchNodesPerThread; ++u) {
-        const int64_t g = g0 + (int64_t)u * kBlock;
+    const int per = kBatchNodesPerCta / (int)blockDim.x;
+    for (int u = 0; u < per; ++u) {
+        const int64_t g = g0 + (int64_t)u * blockDim.x;
         if (g < total) reinterpret_cast<float4 *>(G.mv)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
 }
 
-__global__ void __launch_bounds__(kBlock) k_grid_update_batch(const BatchRef R, int zero_mv, uint32_t *status)
+template <int kGroup = kBatchNodesPerThread>
+__device__ __forceinline__ void grid_update_entry(const BatchRef &R, int b, int zero_mv, uint32_t *status)
 {
-    const int b = R.ncta_base + blockIdx.x;
     const int s = R.ncta_scene[b];
     if (bad_scene(s, R, status)) return;
     const BatchScene B = R.scene[s];
     const int64_t g0 = (int64_t)(b - R.ncta_first[s]) * kBatchNodesPerCta + threadIdx.x;
     const int64_t total = (int64_t)B.grid.dims[0] * B.grid.dims[1] * B.grid.dims[2];
-    // every node's accumulators are loaded before any store: the stores go
-    // through pointers the compiler cannot tell apart from the loads, so
-    // interleaving them would pay one memory latency per node
-    float4 a[kBatchNodesPerThread];
+    const int per = kBatchNodesPerCta / (int)blockDim.x;
+    for (int u0 = 0; u0 < per; u0 += kGroup) {
+        // a group of nodes' accumulators is loaded before any store: the stores
+        // go through pointers the compiler cannot tell apart from the loads, so
+        // interleaving them would pay one memory latency per node
+        float4 a[kGroup];
 #pragma unroll
-    for (int u = 0; u < kBatchNodesPerThread; ++u) {
-        const int64_t g = g0 + (int64_t)u * kBlock;
-        a[u] = g < total ? reinterpret_cast<const float4 *>(B.grid.mv)[g] : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
+        for (int u = 0; u < kGroup; ++u) {
+            const int64_t g = g0 + (int64_t)(u0 + u) * blockDim.x;
+            a[u] = g < total ? reinterpret_cast<const float4 *>(B.grid.mv)[g] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
 #pragma unroll
-    for (int u = 0; u < kBatchNodesPerThread; ++u) {
-        const int64_t g = g0 + (int64_t)u * kBlock;
-        if (g < total) grid_update_apply(B.grid, B.prm, zero_mv, g, a[u]);
+        for (int u = 0; u < kGroup; ++u) {
+            const int64_t g = g0 + (int64_t)(u0 + u) * blockDim.x;
+            if (g < total) grid_update_apply(B.grid, B.prm, zero_mv, g, a[u]);
+        }
     }
+}
+
+__global__ void __launch_bounds__(kBlock) k_zero_grid_batch(const BatchRef R, uint32_t *status)
+{
+    zero_grid_entry(R, R.ncta_base + blockIdx.x, status);
+}
+
+__global__ void __launch_bounds__(kBlock) k_grid_update_batch(const BatchRef R, int zero_mv, uint32_t *status)
+{
+    grid_update_entry(R, R.ncta_base + blockIdx.x, zero_mv, status);
 }
 
 __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_stress_p2g_batch(
@@ -787,9 +809,9 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p_batch(
                                    (int64_t)(R.pcta_base + blockIdx.x) * kScatterChunk);
 }
 
-__global__ void __launch_bounds__(kBlock) k_stress_p2g_list_batch(mpmw_particles_t P, const BatchRef R,
-                                                                 uint32_t *status, const int *__restrict__ list,
-                                                                 const int *__restrict__ count)
+// the listed (SVD-path) particles, by all threads of the grid
+__device__ __forceinline__ void stress_p2g_list_batch_all(const mpmw_particles_t &P, const BatchRef &R,
+                                                          uint32_t *status, const int *list, const int *count)
 {
     const int cnt = *count;
     uint32_t bad = 0;
@@ -804,13 +826,100 @@ __global__ void __launch_bounds__(kBlock) k_stress_p2g_list_batch(mpmw_particles
     if (bad) raise_status(status, bad);
 }
 
+__global__ void __launch_bounds__(kBlock) k_stress_p2g_list_batch(mpmw_particles_t P, const BatchRef R,
+                                                                 uint32_t *status, const int *__restrict__ list,
+                                                                 const int *__restrict__ count)
+{
+    stress_p2g_list_batch_all(P, R, status, list, count);
+}
+
+
+// ---------------------------------------------------------------------------
+// The batch's fused substeps as one persistent kernel (cooperative launch):
+// every fused substep (grid update, G2P -> return map -> P2G, the SVD
+// worklist) of all scenes, phases separated by bounded grid barriers.  The
+// prologue before it (grids cleared, the first return map and P2G) and the
+// last grid update and G2P after it are the per-kernel launches.  Particle CTAs of the
+// scene table are handed out as tiles from a ticket counter as CTAs free up
+// (the scenes differ in size and in plastic work); grid-node entries are
+// split evenly.  Each tile runs the body the per-kernel launches run.
+// ---------------------------------------------------------------------------
+struct BatchPersistArgs {
+    mpmw_particles_t P;
+    BatchRef R;
+    uint32_t *status;
+    int *list, *count;   // SVD worklist of the whole batch
+    unsigned *arrive;    // grid-barrier arrivals
+    unsigned *tickets;   // particle tiles drawn so far
+    int nsteps;          // the run's substeps: its nsteps - 1 fused ones run here
+    int pctas, nctas;    // particle tiles, grid-node entries
+    int use_ahead;
+};
+
+// after every particle tile: the tile's shared-memory writes (generic proxy)
+// are ordered before the next tile's bulk and TMA copies into the same bytes
+// (async proxy), and no thread is still in the tile.  Returns false (for the
+// whole CTA) once the launch has reported a copy timeout that was not set
+// when it started: a copy may still be in flight, so the CTA stops.
+__device__ __forceinline__ bool batch_tile_done(uint32_t *status, uint32_t st0, int *s_stop)
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t now = status ? *reinterpret_cast<volatile uint32_t *>(status) : 0u;
+        *s_stop = (now & MPMW_ST_TIMEOUT) && !(st0 & MPMW_ST_TIMEOUT);
+    }
+    __syncthreads();
+    return *s_stop == 0;
+}
+
+__global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_batch_persistent(
+    const __grid_constant__ BatchPersistArgs A, const __grid_constant__ BatchMaps M)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ BatchScene B;
+    __shared__ int s_ok, s_tile, s_stop;
+    // the fused body's shared layout (as g2p2g_body places it), for its barriers
+    G2P2GShared &S = *reinterpret_cast<G2P2GShared *>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
+    const uint32_t st0 = A.status ? *reinterpret_cast<volatile uint32_t *>(A.status) : 0u;
+    const int64_t n = A.P.n;
+    unsigned tick = 0;  // tickets drawn by the earlier tiled phases
+    const unsigned per_phase = (unsigned)A.pctas + gridDim.x;
+    for (int step = 0; step + 1 < A.nsteps; ++step) {
+        for (int b = blockIdx.x; b < A.nctas; b += gridDim.x) grid_update_entry<4>(A.R, b, 1, A.status);
+        if (blockIdx.x == 0 && threadIdx.x == 0) *A.count = 0;  // the list phase that read it is over
+        if (!grid_sync(A.arrive, A.status, &s_ok)) return;
+        const bool store = step + 2 == A.nsteps;  // the last fused substep writes the stress
+        for (int t = draw_tile(A.tickets, tick, &s_tile); t < A.pctas; t = draw_tile(A.tickets, tick, &s_tile)) {
+            const int sc = stage_scene_at(A.R, t, B, A.status);
+            const int64_t p0 = (int64_t)t * kScatterChunk;
+            // one body, the stress store chosen at run time (a uniform branch)
+            if (sc >= 0)
+                g2p2g_body<false>(A.P, B.grid, B.prm, A.status, A.list, A.count, &M.tmap[sc], A.R.use_tma,
+                                  A.use_ahead, p0, store);
+            __syncthreads();
+            if (sc >= 0 && threadIdx.x == 0) {
+                // the body initialised these barriers; their bytes are reused
+                mbar_inval(&S.g.bar);
+                if (A.use_ahead && p0 + kScatterChunk <= n) mbar_inval(&S.pbar);
+            }
+            if (!batch_tile_done(A.status, st0, &s_stop)) return;
+        }
+        tick += per_phase;
+        if (!grid_sync(A.arrive, A.status, &s_ok)) return;
+        stress_p2g_list_batch_all(A.P, A.R, A.status, A.list, A.count);
+        if (!grid_sync(A.arrive, A.status, &s_ok)) return;
+    }
+}
+
 namespace {
 // Workspace layout of a batch: the SVD worklist (n ints; a range of scenes
 // lists its particles in its own part, from the range's first particle on),
 // one worklist count per scene (a range uses its first scene's), the scene
-// records, then the three CTA tables.
+// records, the three CTA tables, then the persistent form's barrier and
+// ticket counters.
 struct BatchLayout {
-    size_t list, counts, scenes, pcta, ncta, nfirst, total;
+    size_t list, counts, scenes, pcta, ncta, nfirst, sync, total;
 };
 size_t round256(size_t b) { return (b + 255) / 256 * 256; }
 BatchLayout batch_layout(int64_t n, int nscenes, int64_t nctas)
@@ -822,7 +931,8 @@ BatchLayout batch_layout(int64_t n, int nscenes, int64_t nctas)
     L.pcta = L.scenes + round256((size_t)nscenes * sizeof(BatchScene));
     L.ncta = L.pcta + round256((size_t)(n / kScatterChunk) * sizeof(int));
     L.nfirst = L.ncta + round256((size_t)nctas * sizeof(int));
-    L.total = L.nfirst + round256((size_t)(nscenes + 1) * sizeof(int));
+    L.sync = L.nfirst + round256((size_t)(nscenes + 1) * sizeof(int));  // the persistent form's counters
+    L.total = L.sync + 256;
     return L;
 }
 int64_t scene_node_ctas(const mpmw_grid_t &g)
@@ -936,6 +1046,8 @@ bool set_batch_options(const void *ws, int gather_tile, int read_ahead)
 // per device: the batched kernels' shared-memory attribute is set (several host
 // threads may launch batches at once; setting it twice is harmless)
 static std::atomic<bool> g_batch_attr[64];
+std::atomic<int64_t> g_batch_persistent_launches{0};
+int64_t batch_persistent_launches() { return g_batch_persistent_launches.load(); }
 
 // The fused schedule of mpmw_run_substeps over the scenes [first, last) of a
 // batch that prepare_batch wrote into this workspace (last < 0: to the end).
@@ -1019,6 +1131,99 @@ int launch_batch_substeps(const mpmw_particles_t &p, int first, int last, int ns
             MPMW_TRY_LAUNCH("k_g2p_batch");
         }
     }
+    return MPMW_OK;
+}
+
+// CTAs of the persistent batch kernel's cooperative grid on the current
+// device (0: it cannot be launched there)
+static int batch_persist_capacity(size_t smem)
+{
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 0;
+    if (dev < 64) {
+        const int c = cache[dev].load();
+        if (c != 0) return c > 0 ? c : 0;
+    }
+    int coop = 0, sms = 0, per_sm = 0, cap = -1;
+    if (cudaFuncSetAttribute(k_batch_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && coop &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent, kScatterChunk, smem) ==
+            cudaSuccess &&
+        per_sm > 0)
+        cap = per_sm * sms;
+    cudaGetLastError();
+    if (dev < 64) cache[dev].store(cap);
+    return cap > 0 ? cap : 0;
+}
+
+// All scenes of a prepared batch, nsteps substeps: the prologue, the fused
+// substeps in one persistent launch, then the last grid update and G2P.
+int launch_batch_persistent(const mpmw_particles_t &p, int nsteps, uint32_t *st, void *ws, size_t ws_bytes,
+                            cudaStream_t s)
+{
+    BatchPrepared bp;
+    {
+        std::lock_guard<std::mutex> lk(g_batch_mu);
+        auto it = g_batches.find(ws);
+        if (it == g_batches.end()) { set_error("batch: the workspace was not prepared (mpmw_batch_prepare)"); return MPMW_E_ARG; }
+        bp = it->second;
+    }
+    if (bp.n != p.n || ws_bytes < bp.L.total) {
+        set_error("batch: the workspace was prepared for %lld particles in %zu bytes", (long long)bp.n, bp.L.total);
+        return MPMW_E_ARG;
+    }
+    if (nsteps == 0 || p.n == 0) return MPMW_OK;
+    const size_t smem = sizeof(G2P2GShared) + 128;
+    static_assert(sizeof(G2P2GShared) + 128 >= sizeof(ScatterShared), "the stress + P2G phase fits the same buffer");
+    const int cap = batch_persist_capacity(smem);
+    if (cap <= 0) { set_error("batch: the device cannot run the persistent batch kernel"); return MPMW_E_DEVICE; }
+    unsigned char *base = static_cast<unsigned char *>(ws);
+    BatchPersistArgs A;
+    memset(&A, 0, sizeof(A));
+    A.P = p;
+    A.R.scene = reinterpret_cast<const BatchScene *>(base + bp.L.scenes);
+    A.R.pcta_scene = reinterpret_cast<const int *>(base + bp.L.pcta);
+    A.R.ncta_scene = reinterpret_cast<const int *>(base + bp.L.ncta);
+    A.R.ncta_first = reinterpret_cast<const int *>(base + bp.L.nfirst);
+    A.R.pcta_base = 0;
+    A.R.ncta_base = 0;
+    A.R.nscenes = bp.nscenes;
+    A.R.use_tma = bp.use_tma;
+    A.status = st;
+    A.list = reinterpret_cast<int *>(base + bp.L.list);
+    A.count = reinterpret_cast<int *>(base + bp.L.counts);
+    A.arrive = reinterpret_cast<unsigned *>(base + bp.L.sync);
+    A.tickets = A.arrive + 1;
+    A.nsteps = nsteps;
+    A.pctas = bp.pctas;
+    A.nctas = bp.nctas;
+    A.use_ahead = bp.use_ahead;
+    if (cudaMemsetAsync(base + bp.L.sync, 0, 2 * sizeof(unsigned), s) != cudaSuccess ||
+        cudaMemsetAsync(A.count, 0, sizeof(int), s) != cudaSuccess) {
+        set_error("batch: memset failed");
+        return MPMW_E_DEVICE;
+    }
+    BatchRef R = A.R;
+    k_zero_grid_batch<<<(unsigned)bp.nctas, kBlock, 0, s>>>(R, st);
+    MPMW_TRY_LAUNCH("k_zero_grid_batch");
+    k_stress_p2g_batch<<<(unsigned)bp.pctas, kScatterChunk, sizeof(ScatterShared), s>>>(p, R, st, A.list, A.count);
+    MPMW_TRY_LAUNCH("k_stress_p2g_batch");
+    k_stress_p2g_list_batch<<<148 * 4, kBlock, 0, s>>>(p, R, st, A.list, A.count);
+    MPMW_TRY_LAUNCH("k_stress_p2g_list_batch");
+    const int grid = bp.pctas < cap ? (bp.pctas > 0 ? bp.pctas : 1) : cap;
+    void *args[] = {&A, bp.maps.get()};
+    if (cudaLaunchCooperativeKernel((const void *)k_batch_persistent, dim3((unsigned)grid), dim3(kScatterChunk), args,
+                                    smem, s) != cudaSuccess) {
+        set_error("batch: cooperative launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+        return MPMW_E_DEVICE;
+    }
+    g_batch_persistent_launches.fetch_add(1);
+    k_grid_update_batch<<<(unsigned)bp.nctas, kBlock, 0, s>>>(R, 0, st);
+    MPMW_TRY_LAUNCH("k_grid_update_batch");
+    k_g2p_batch<<<(unsigned)bp.pctas, kScatterChunk, 0, s>>>(p, R, *bp.maps, st, bp.use_ahead_g2p);
+    MPMW_TRY_LAUNCH("k_g2p_batch");
     return MPMW_OK;
 }
 

@@ -28,5 +28,9 @@ int prepare_batch(const mpmw_particles_t &p, const mpmw_grid_t *grids, const mpm
 bool set_batch_options(const void *ws, int gather_tile, int read_ahead);
 int launch_batch_substeps(const mpmw_particles_t &p, int first, int last, int nsteps, uint32_t *st, void *ws,
                           size_t ws_bytes, cudaStream_t s);
+// the fused substeps of all scenes in one persistent (cooperative) launch
+int launch_batch_persistent(const mpmw_particles_t &p, int nsteps, uint32_t *st, void *ws, size_t ws_bytes,
+                            cudaStream_t s);
+int64_t batch_persistent_launches();
 
 }  // namespace mpmw

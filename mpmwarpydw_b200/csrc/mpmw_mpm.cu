@@ -617,6 +617,17 @@ int mpmw_batch_run_range(const mpmw_particles_t *p, int first_scene, int last_sc
                                  as_stream(stream));
 }
 
+int mpmw_batch_run_persistent(const mpmw_particles_t *p, int nsteps, uint32_t *status, void *workspace,
+                              size_t ws_bytes, mpmw_stream_t stream)
+{
+    MPMW_TRY(check_particles(p, kNeedLabels | kNeedXV | kNeedCF | kNeedStress));
+    if (nsteps < 0) { set_error("nsteps must be >= 0"); return MPMW_E_ARG; }
+    if (!workspace) { set_error("batch: workspace is NULL"); return MPMW_E_WORKSPACE; }
+    return launch_batch_persistent(*p, nsteps, status, workspace, ws_bytes, as_stream(stream));
+}
+
+int64_t mpmw_batch_persistent_launches(void) { return batch_persistent_launches(); }
+
 int mpmw_batch_set_options(const void *workspace, int gather_tile, int read_ahead)
 {
     if (!workspace) { set_error("batch: workspace is NULL"); return MPMW_E_ARG; }

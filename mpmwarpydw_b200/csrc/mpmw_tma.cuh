@@ -28,6 +28,13 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// invalidate before the barrier's shared memory is used again (another
+// mbarrier.init included)
+__device__ __forceinline__ void mbar_inval(uint64_t *bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)

@@ -18,7 +18,7 @@
 #include "mpmw_common.cuh"
 #include "mpmw_math.cuh"
 #include "mpmw_scan.cuh"
-#include "mpmw_tma.cuh"
+#include "mpmw_gridsync.cuh"
 #include "../../include/mpmw_xpbd.h"
 
 namespace mpmw {
@@ -765,44 +765,8 @@ __global__ void k_swell(mpmw_particles_t P, mpmw_xpbd_t X, mpmw_xpbd_params_t q)
 // forms give the same bits.
 // ---------------------------------------------------------------------------
 constexpr int kPersistThreads = kSortThreads;                     // 256
-constexpr uint64_t kGridSyncWaitNs = 1000ull * 1000ull * 1000ull;  // 1 s per barrier at most
-constexpr unsigned kGridSyncMaxPolls = 1u << 24;
 constexpr int kPersistMaxCtas = 4000;                              // chunk sums of the in-kernel scan
 constexpr size_t kPersistHeaderBytes = 16384;                      // arrival counter, XPBD count, tile tickets, chunk sums
-
-// Grid-wide barrier on a monotonically increasing arrival counter (zeroed
-// before the launch): each CTA adds one and waits until the count reaches the
-// next multiple of gridDim.x.  The wait is bounded (kGridSyncWaitNs of
-// %globaltimer and kGridSyncMaxPolls polls); a CTA that gives up reports
-// MPMW_ST_TIMEOUT and the call returns false in all its threads, after which
-// the kernel returns (the other CTAs then give up at their next barrier).
-__device__ __forceinline__ bool grid_sync(unsigned *arrive, uint32_t *status, int *s_ok)
-{
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned old = atomicAdd(arrive, 1u);
-        const unsigned target = (old / gridDim.x + 1u) * gridDim.x;
-        int ok = 1;
-        const uint64_t t0 = globaltimer_ns();
-        unsigned polls = 0;
-        for (;;) {
-            unsigned now;
-            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(now) : "l"(arrive) : "memory");
-            if ((int)(now - target) >= 0) break;
-            if (++polls > kGridSyncMaxPolls || globaltimer_ns() - t0 > kGridSyncWaitNs) {
-                ok = 0;
-                raise_status(status, MPMW_ST_TIMEOUT);
-                break;
-            }
-            if (polls > 32) __nanosleep(64);
-        }
-        __threadfence();
-        *s_ok = ok;
-    }
-    __syncthreads();
-    return *s_ok != 0;
-}
 
 struct PersistArgs {
     mpmw_particles_t P;
@@ -818,7 +782,7 @@ struct PersistArgs {
     int *keys_a, *keys_b, *ids_scratch, *hist, *offs;
     int *chunk_sums;           // one per CTA
     unsigned *arrive;
-    int *tickets;              // contact-pass tiles drawn so far (all iterations)
+    unsigned *tickets;         // contact-pass tiles drawn so far (all iterations)
     int *xpbd_count;
     unsigned *xpbd_cells;
     float4 *recA, *recB;
@@ -831,21 +795,6 @@ union PersistShared {
     RadixScatterShared sc;
 };
 
-// The next tile of a dynamically scheduled phase for this CTA: one ticket
-// per draw from a counter that only grows, `base` tickets drawn by earlier
-// such phases (each phase draws its tiles plus one final ticket per CTA).
-__device__ __forceinline__ int draw_tile(int *tickets, int base, int *s_tile)
-{
-    if (threadIdx.x == 0) *s_tile = atomicAdd(tickets, 1) - base;
-    __syncthreads();
-    const int t = *s_tile;
-    __syncthreads();
-    return t;
-}
-
-// Exclusive scan of hist[0, hist_n) into offs inside the persistent kernel:
-// each CTA sums a contiguous chunk, then (after a barrier) scans its chunk on
-// top of the earlier chunks' sums.  Every thread of every CTA calls it.
 __device__ __forceinline__ bool persist_scan(const PersistArgs &A, int *s_ok)
 {
     const int64_t L = (A.hist_n + gridDim.x - 1) / gridDim.x;
@@ -926,8 +875,8 @@ __global__ void __launch_bounds__(kPersistThreads) k_xpbd_step_persistent(const 
         if (!grid_sync(A.arrive, A.status, &s_ok)) return;
         // the neighbour walks vary in length: tiles are handed out as CTAs free up
         const int ctiles = (int)((n + blockDim.x - 1) / blockDim.x);
-        for (int t = draw_tile(A.tickets, it * (ctiles + (int)gridDim.x), &s_tile); t < ctiles;
-             t = draw_tile(A.tickets, it * (ctiles + (int)gridDim.x), &s_tile))
+        const unsigned base = (unsigned)it * (unsigned)(ctiles + (int)gridDim.x);
+        for (int t = draw_tile(A.tickets, base, &s_tile); t < ctiles; t = draw_tile(A.tickets, base, &s_tile))
             particle_contacts_at<true>((int64_t)t * blockDim.x + threadIdx.x, A.P, A.X, A.H, A.qi, A.xpbd_count,
                                        A.xpbd_cells, A.recA, A.recB);
         if (!grid_sync(A.arrive, A.status, &s_ok)) return;
@@ -1146,7 +1095,7 @@ static int xpbd_step_persistent(const mpmw_particles_t *p, const mpmw_xpbd_t *x,
     char *w = static_cast<char *>(workspace);
     A.arrive = reinterpret_cast<unsigned *>(w);
     A.xpbd_count = reinterpret_cast<int *>(w) + 1;
-    A.tickets = reinterpret_cast<int *>(w) + 2;
+    A.tickets = reinterpret_cast<unsigned *>(w) + 2;
     A.chunk_sums = reinterpret_cast<int *>(w) + 64;
     A.xpbd_cells = reinterpret_cast<unsigned *>(w + kPersistHeaderBytes);
     char *area = w + persist_area_offset(h->dims);

@@ -233,14 +233,22 @@ class ConcatBatch:
     def step(self, k: int, groups=None):
         """k substeps of every scene.  The scenes run as ``groups`` contiguous
         ranges (default: ``self.groups``), each range one launch per kernel
-        on its own stream; 1 group is a single launch per kernel."""
+        on its own stream; 1 group is a single launch per kernel; 0 runs the
+        fused substeps of all scenes in one persistent launch
+        (mpmw_batch_run_persistent)."""
         import ctypes
 
         from . import _lib
         from .bind import stream_handle
         L = _lib.lib()
-        ranges = scene_groups(self.counts, self.groups if groups is None else groups)
+        groups = self.groups if groups is None else groups
         cur = torch.cuda.current_stream(self.device)
+        if groups == 0:
+            _lib.check(L.mpmw_batch_run_persistent(ctypes.byref(self.P), int(k), self.status.data_ptr(),
+                                                   self.ws.data_ptr(), self.ws.numel(), stream_handle(cur)),
+                       "batch_run_persistent")
+            return
+        ranges = scene_groups(self.counts, groups)
         if len(ranges) == 1:
             _lib.check(L.mpmw_batch_run_substeps(ctypes.byref(self.P), int(k), self.status.data_ptr(),
                                                  self.ws.data_ptr(), self.ws.numel(), stream_handle(cur)),
@@ -279,7 +287,8 @@ class ConcatBatch:
         """Pick the launch configuration that steps this batch fastest: first
         the kernels' options (grid tile by TMA or L1 gathers, bulk read-ahead
         or plain loads) with one group, then the number of scene groups
-        (streams) with the best options.  Each candidate runs k substeps to
+        (streams) with the best options, and the one persistent launch for
+        all scenes (groups = 0).  Each candidate runs k substeps to
         warm up and k timed, so the tuning advances every scene by 2 k
         substeps per candidate.  The choice is kept in ``self.groups`` /
         ``self.options`` and, per batch shape, for later batches."""
@@ -297,7 +306,7 @@ class ConcatBatch:
             self.tuning[(1, opts)] = self._rate(k, 1)
         best_opts = max(((o, r) for (g, o), r in self.tuning.items()), key=lambda t: t[1])[0]
         self.set_options(*best_opts)
-        cands = sorted({c for c in (candidates or (1, 2, 4, 8, 16, 32, n)) if 1 < c <= n})
+        cands = sorted({c for c in (candidates or (0, 1, 2, 4, 8, 16, 32, n)) if c == 0 or 1 < c <= n})
         for g in cands:
             self.tuning[(g, best_opts)] = self._rate(k, g)
         (self.groups, opts) = max(self.tuning, key=self.tuning.get)
