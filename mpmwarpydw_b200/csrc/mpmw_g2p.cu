@@ -606,6 +606,8 @@ static bool g2p2g_ahead_ok(const mpmw_particles_t &p)
     return true;
 }
 
+constexpr bool kFusedReadAhead = false;
+
 int launch_g2p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st,
                  bool store_stress, void *ws, size_t ws_bytes, cudaStream_t s)
 {
@@ -623,7 +625,12 @@ int launch_g2p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_par
     int *count = static_cast<int *>(ws);
     int *list = reinterpret_cast<int *>(static_cast<char *>(ws) + 256);
     if (cudaMemsetAsync(count, 0, sizeof(int), s) != cudaSuccess) { set_error("g2p2g: memset failed"); return MPMW_E_DEVICE; }
-    const int use_ahead = g2p2g_ahead_ok(p) ? 1 : 0;
+    // The bulk read-ahead of the particle fields is off here: with 128-particle
+    // CTAs its 18 copies of 512 B per CTA cost more than the plain loads (the
+    // fused launch on the 3.87 M-particle tunnel: 0.5277 ms without, 0.5372 ms
+    // with; an L2 prefetch of the fields at the CTA's start was slower still).
+    // The batched kernels keep it as an option their tuner measures.
+    const int use_ahead = kFusedReadAhead && g2p2g_ahead_ok(p) ? 1 : 0;
     const unsigned grid = grid_for(p.n, kScatterChunk);
     if (store_stress) k_g2p2g<true><<<grid, kScatterChunk, smem, s>>>(p, g, prm, st, list, count, map, use_tma, use_ahead);
     else k_g2p2g<false><<<grid, kScatterChunk, smem, s>>>(p, g, prm, st, list, count, map, use_tma, use_ahead);
