@@ -128,7 +128,7 @@ VLC_COV_EXTRA_BYTES_P = 48 + 152
 # DRAM bytes of one k_g2p2g launch on the 3,873,600-particle tunnel, measured by
 # ncu (dram__bytes_read.sum + dram__bytes_write.sum, one launch, separate run);
 # not measured by this script.  Update it with the kernel.
-TRAFFIC_NCU = {"g2p2g": 629_962_240}
+TRAFFIC_NCU = {"g2p2g": 629_440_256}
 TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_g2p2g launch in a separate run " \
                  "(profiles/traffic_tunnel_full.md), not measured by this run"
 
