@@ -45,6 +45,35 @@ __device__ __forceinline__ void raise_status(uint32_t *status, uint32_t bits)
     if (status) atomicOr(status, bits);
 }
 
+// Programmatic dependent launch.  A kernel launched with the programmatic
+// stream-serialization attribute may begin while the kernel before it in the
+// stream is still running; pdl_wait() blocks until that kernel has completed
+// and its memory operations are visible, so it comes before any read of the
+// predecessor's results.  pdl_trigger() lets the next such kernel's CTAs be
+// scheduled once every CTA of this grid has issued it (they then wait in
+// their own pdl_wait).  Both are no-ops in a kernel launched the usual way.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
+// A kernel launch with the programmatic stream-serialization attribute (the
+// kernel must call pdl_wait() before it reads what the previous kernel wrote).
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                              Args &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<Args &&>(args)...);
+}
+
 // SoA accessors
 __device__ __forceinline__ void load3(const float *__restrict__ a, int64_t n, int64_t p, float *o)
 {

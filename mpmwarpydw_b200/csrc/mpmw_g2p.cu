@@ -92,6 +92,8 @@ __global__ void __launch_bounds__(kBlock) k_stress_p2g_list(mpmw_particles_t P, 
                                                            uint32_t *status, const int *__restrict__ list,
                                                            const int *__restrict__ count)
 {
+    pdl_wait();
+    pdl_trigger();
     const int cnt = *count;
     uint32_t bad = 0;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += gridDim.x * blockDim.x)
@@ -383,6 +385,8 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g(mpmw
                                                         const __grid_constant__ CUtensorMap tmap, int use_tma,
                                                         int use_ahead)
 {
+    pdl_wait();
+    pdl_trigger();
     g2p2g_body<StoreStress>(P, G, prm, status, svd_list, svd_count, &tmap, use_tma, use_ahead,
                             (int64_t)blockIdx.x * blockDim.x);
 }
@@ -609,7 +613,7 @@ static bool g2p2g_ahead_ok(const mpmw_particles_t &p)
 constexpr bool kFusedReadAhead = false;
 
 int launch_g2p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st,
-                 bool store_stress, void *ws, size_t ws_bytes, cudaStream_t s)
+                 bool store_stress, void *ws, size_t ws_bytes, cudaStream_t s, bool chained)
 {
     if (p.n == 0) return MPMW_OK;
     if (!ws || ws_bytes < g2p_workspace_bytes(p.n)) {
@@ -624,7 +628,10 @@ int launch_g2p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_par
     if (!use_tma) memset(&map, 0, sizeof(map));
     int *count = static_cast<int *>(ws);
     int *list = reinterpret_cast<int *>(static_cast<char *>(ws) + 256);
-    if (cudaMemsetAsync(count, 0, sizeof(int), s) != cudaSuccess) { set_error("g2p2g: memset failed"); return MPMW_E_DEVICE; }
+    if (!chained && cudaMemsetAsync(count, 0, sizeof(int), s) != cudaSuccess) {
+        set_error("g2p2g: memset failed");
+        return MPMW_E_DEVICE;
+    }
     // The bulk read-ahead of the particle fields is off here: with 128-particle
     // CTAs its 18 copies of 512 B per CTA cost more than the plain loads (the
     // fused launch on the 3.87 M-particle tunnel: 0.5277 ms without, 0.5372 ms
@@ -632,6 +639,17 @@ int launch_g2p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_par
     // The batched kernels keep it as an option their tuner measures.
     const int use_ahead = kFusedReadAhead && g2p2g_ahead_ok(p) ? 1 : 0;
     const unsigned grid = grid_for(p.n, kScatterChunk);
+    if (chained) {
+        const cudaError_t e = store_stress
+            ? launch_pdl(k_g2p2g<true>, grid, kScatterChunk, smem, s, p, g, prm, st, list, count, map, use_tma, use_ahead)
+            : launch_pdl(k_g2p2g<false>, grid, kScatterChunk, smem, s, p, g, prm, st, list, count, map, use_tma, use_ahead);
+        if (e != cudaSuccess ||
+            launch_pdl(k_stress_p2g_list, 148 * 4, kBlock, 0, s, p, g, prm, st, list, (const int *)count) != cudaSuccess) {
+            set_error("g2p2g: launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+            return MPMW_E_DEVICE;
+        }
+        return MPMW_OK;
+    }
     if (store_stress) k_g2p2g<true><<<grid, kScatterChunk, smem, s>>>(p, g, prm, st, list, count, map, use_tma, use_ahead);
     else k_g2p2g<false><<<grid, kScatterChunk, smem, s>>>(p, g, prm, st, list, count, map, use_tma, use_ahead);
     MPMW_TRY_LAUNCH("k_g2p2g");

@@ -12,8 +12,10 @@ int launch_stress(const mpmw_particles_t &p, const mpmw_params_t &prm, cudaStrea
 int launch_p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, cudaStream_t s);
 int launch_g2p(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, bool fused,
                void *ws, size_t ws_bytes, cudaStream_t s);
+// chained: launched as the fused schedule's programmatic dependent launches,
+// with the worklist count already reset by the grid pass before it
 int launch_g2p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st,
-                 bool store_stress, void *ws, size_t ws_bytes, cudaStream_t s);
+                 bool store_stress, void *ws, size_t ws_bytes, cudaStream_t s, bool chained = false);
 size_t g2p_workspace_bytes(int64_t n);
 int launch_stress_p2g(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st,
                       void *ws, size_t ws_bytes, cudaStream_t s);

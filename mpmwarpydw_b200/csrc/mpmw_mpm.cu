@@ -35,9 +35,13 @@ int check_launch(const char *what)
 }
 
 // zero_mv: also clear the accumulators after reading them (for the fused
-// G2P->P2G kernel, which scatters the next substep into them)
-__global__ void __launch_bounds__(kBlock) k_grid_update(mpmw_grid_t G, mpmw_params_t prm, int zero_mv)
+// G2P->P2G kernel, which scatters the next substep into them).
+// reset (may be NULL): set to 0 once, for the fused kernel's worklist count.
+__global__ void __launch_bounds__(kBlock) k_grid_update(mpmw_grid_t G, mpmw_params_t prm, int zero_mv, int *reset)
 {
+    pdl_wait();
+    pdl_trigger();
+    if (reset && blockIdx.x == 0 && threadIdx.x == 0) *reset = 0;
     grid_update_node(G, prm, zero_mv, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
@@ -350,10 +354,20 @@ static int check_params(const mpmw_params_t *prm)
     } while (0)
 
 // host-side launchers (also used by the multi-step driver)
-int launch_grid(const mpmw_grid_t &g, const mpmw_params_t &prm, cudaStream_t s, bool zero_mv = false)
+// pdl: a programmatic dependent launch (the fused schedule's chain);
+// reset: a worklist count the kernel sets to 0
+int launch_grid(const mpmw_grid_t &g, const mpmw_params_t &prm, cudaStream_t s, bool zero_mv = false,
+                int *reset = nullptr, bool pdl = false)
 {
     int64_t G = (int64_t)g.dims[0] * g.dims[1] * g.dims[2];
-    k_grid_update<<<grid_for(G), kBlock, 0, s>>>(g, prm, zero_mv ? 1 : 0);
+    if (pdl) {
+        if (launch_pdl(k_grid_update, grid_for(G), kBlock, 0, s, g, prm, zero_mv ? 1 : 0, reset) != cudaSuccess) {
+            set_error("k_grid_update: launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+            return MPMW_E_DEVICE;
+        }
+        return MPMW_OK;
+    }
+    k_grid_update<<<grid_for(G), kBlock, 0, s>>>(g, prm, zero_mv ? 1 : 0, reset);
     return check_launch("k_grid_update");
 }
 int launch_vlc(const mpmw_particles_t &p, const mpmw_grid_t &g, const mpmw_params_t &prm, uint32_t *st, cudaStream_t s)
@@ -553,8 +567,13 @@ int mpmw_run_substeps(const mpmw_particles_t *p, const mpmw_grid_t *g, const mpm
     for (int step = 0; step < nsteps; ++step) {
         const bool last = step == nsteps - 1;
         if (!last && fuse) {
-            MPMW_TRY(launch_grid(*g, *prm, s, true));
-            MPMW_TRY(launch_g2p2g(*p, *g, *prm, status, step + 1 == nsteps - 1, workspace, ws_bytes, s));
+            // grid update -> fused kernel -> worklist as one chain of
+            // programmatic dependent launches: each kernel's CTAs are
+            // scheduled during its predecessor's last wave and wait for it to
+            // finish, which hides the launch gaps.  The grid pass also resets
+            // the fused kernel's worklist count.
+            MPMW_TRY(launch_grid(*g, *prm, s, true, static_cast<int *>(workspace), true));
+            MPMW_TRY(launch_g2p2g(*p, *g, *prm, status, step + 1 == nsteps - 1, workspace, ws_bytes, s, true));
         } else {
             MPMW_TRY(launch_grid(*g, *prm, s));
             MPMW_TRY(launch_g2p(*p, *g, *prm, status, false, nullptr, 0, s));
