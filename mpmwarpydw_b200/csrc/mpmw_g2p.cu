@@ -795,8 +795,13 @@ __global__ void __launch_bounds__(kBlock) k_zero_grid_batch(const BatchRef R, ui
     zero_grid_entry(R, R.ncta_base + blockIdx.x, status);
 }
 
-__global__ void __launch_bounds__(kBlock) k_grid_update_batch(const BatchRef R, int zero_mv, uint32_t *status)
+// reset (may be NULL): the range's worklist count, set to 0 once
+__global__ void __launch_bounds__(kBlock) k_grid_update_batch(const BatchRef R, int zero_mv, uint32_t *status,
+                                                             int *reset)
 {
+    pdl_wait();
+    pdl_trigger();
+    if (reset && blockIdx.x == 0 && threadIdx.x == 0) *reset = 0;
     grid_update_entry(R, R.ncta_base + blockIdx.x, zero_mv, status);
 }
 
@@ -814,6 +819,8 @@ __global__ void __launch_bounds__(kScatterChunk, kScatterCtasPerSm) k_g2p2g_batc
     mpmw_particles_t P, const BatchRef R, const __grid_constant__ BatchMaps M, uint32_t *status, int *svd_list,
     int *svd_count, int use_ahead)
 {
+    pdl_wait();
+    pdl_trigger();
     __shared__ BatchScene B;
     const int s = stage_scene(R, B, status);
     if (s < 0) return;
@@ -855,6 +862,8 @@ __global__ void __launch_bounds__(kBlock) k_stress_p2g_list_batch(mpmw_particles
                                                                  uint32_t *status, const int *__restrict__ list,
                                                                  const int *__restrict__ count)
 {
+    pdl_wait();
+    pdl_trigger();
     stress_p2g_list_batch_all(P, R, status, list, count);
 }
 
@@ -1139,18 +1148,25 @@ int launch_batch_substeps(const mpmw_particles_t &p, int first, int last, int ns
     MPMW_TRY_LAUNCH("k_stress_p2g_list_batch");
     for (int step = 0; step < nsteps; ++step) {
         if (step < nsteps - 1) {
-            k_grid_update_batch<<<nctas, kBlock, 0, s>>>(R, 1, st);
-            MPMW_TRY_LAUNCH("k_grid_update_batch");
-            if (reset_count() != MPMW_OK) return MPMW_E_DEVICE;
-            if (step + 1 == nsteps - 1)
-                k_g2p2g_batch<true><<<pctas, kScatterChunk, smem, s>>>(p, R, *bp.maps, st, list, count, bp.use_ahead);
-            else
-                k_g2p2g_batch<false><<<pctas, kScatterChunk, smem, s>>>(p, R, *bp.maps, st, list, count, bp.use_ahead);
-            MPMW_TRY_LAUNCH("k_g2p2g_batch");
-            k_stress_p2g_list_batch<<<148 * 4, kBlock, 0, s>>>(p, R, st, list, count);
-            MPMW_TRY_LAUNCH("k_stress_p2g_list_batch");
+            // grid pass (which also resets the worklist count) -> fused kernel
+            // -> worklist, as programmatic dependent launches (each waits for
+            // its predecessor before it reads anything)
+            cudaError_t e = launch_pdl(k_grid_update_batch, nctas, kBlock, 0, s, R, 1, st, count);
+            if (e == cudaSuccess)
+                e = step + 1 == nsteps - 1
+                        ? launch_pdl(k_g2p2g_batch<true>, pctas, kScatterChunk, smem, s, p, R, *bp.maps, st, list,
+                                     count, bp.use_ahead)
+                        : launch_pdl(k_g2p2g_batch<false>, pctas, kScatterChunk, smem, s, p, R, *bp.maps, st, list,
+                                     count, bp.use_ahead);
+            if (e == cudaSuccess)
+                e = launch_pdl(k_stress_p2g_list_batch, 148 * 4, kBlock, 0, s, p, R, st, (const int *)list,
+                               (const int *)count);
+            if (e != cudaSuccess) {
+                set_error("batch: launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+                return MPMW_E_DEVICE;
+            }
         } else {
-            k_grid_update_batch<<<nctas, kBlock, 0, s>>>(R, 0, st);
+            k_grid_update_batch<<<nctas, kBlock, 0, s>>>(R, 0, st, nullptr);
             MPMW_TRY_LAUNCH("k_grid_update_batch");
             k_g2p_batch<<<pctas, kScatterChunk, 0, s>>>(p, R, *bp.maps, st, bp.use_ahead_g2p);
             MPMW_TRY_LAUNCH("k_g2p_batch");
@@ -1245,7 +1261,7 @@ int launch_batch_persistent(const mpmw_particles_t &p, int nsteps, uint32_t *st,
         return MPMW_E_DEVICE;
     }
     g_batch_persistent_launches.fetch_add(1);
-    k_grid_update_batch<<<(unsigned)bp.nctas, kBlock, 0, s>>>(R, 0, st);
+    k_grid_update_batch<<<(unsigned)bp.nctas, kBlock, 0, s>>>(R, 0, st, nullptr);
     MPMW_TRY_LAUNCH("k_grid_update_batch");
     k_g2p_batch<<<(unsigned)bp.pctas, kScatterChunk, 0, s>>>(p, R, *bp.maps, st, bp.use_ahead_g2p);
     MPMW_TRY_LAUNCH("k_g2p_batch");
