@@ -368,9 +368,10 @@ def surrogate_comparison(sim, mpm, xpbd, dev, reps=10):
     random directions and frames, friction angle U(20, 45) deg, cohesion
     log-uniform in [0.1, 5] MPa, damage U(0, 1): domains.seed_plastic_trials),
     so that the stress phase has plastic trials to return; each stress phase
-    runs `reps` times from that restored state, timed with CUDA events, with
-    every surrogate return audited against the exact one.  The scene state is
-    restored afterwards."""
+    runs `reps` times from that restored state, timed with CUDA events.  The
+    timed surrogate phase audits 1 % of its returns against the exact one (the
+    production setting); one more untimed pass audits every return, for the
+    accuracy statistics.  The scene state is restored afterwards."""
     import torch
 
     from mpmwarpydw_b200 import _lib, domains
@@ -419,11 +420,13 @@ def surrogate_comparison(sim, mpm, xpbd, dev, reps=10):
     plastic = (acc > snap[acc_idx]) & (lab <= 1)
     stats = torch.zeros(_lib.SURR_NSTATS, dtype=torch.int32, device=dev)
 
-    def surr():
+    def surr(audit):
         stats.zero_()
-        compute_stress(sim, mpm, xpbd, net, gate_tol=1e-3, audit=1.0, audit_seed=7, stats=stats)
+        compute_stress(sim, mpm, xpbd, net, gate_tol=1e-3, audit=audit, audit_seed=7, stats=stats)
 
-    ms_surr = timed(surr)
+    ms_surr_full = timed(lambda: surr(1.0))
+    summ_full = stats_summary(stats)
+    ms_surr = timed(lambda: surr(0.01))
     flipped = lab != lab_plain
     keep = plastic & ~flipped
     d = (stress - s_plain)[:, keep]
@@ -431,13 +434,20 @@ def surrogate_comparison(sim, mpm, xpbd, dev, reps=10):
     err = float(torch.linalg.norm(d.double()) / torch.linalg.norm(ref.double()).clamp_min(1e-30)) if ref.numel() else 0.0
     n = sim.nPoints
     summ = stats_summary(stats)
+    # the accuracy statistics come from the pass that audits every return; the
+    # gate's counts are the same in both passes
+    for k in ("audited", "audit_max_rel_err", "audit_mean_rel_err", "audit_within_1e-3", "audited_accepted",
+              "accepted_audit_max_rel_err"):
+        if k in summ_full:
+            summ[k] = summ_full[k]
     restore(orig)
     return {"stress_phase_plain": n / (ms_plain * 1e-3), "stress_phase_surrogate": n / (ms_surr * 1e-3),
             "unit": "particle-updates/s", "speedup": ms_plain / ms_surr, "ms_plain": ms_plain, "ms_surrogate": ms_surr,
             "state": "tunnel particles with seeded plastic trials (|e| log-uniform [1e-6, 1e-1], friction angle "
                      "U(20,45) deg, cohesion log-uniform [0.1,5] MPa, damage U(0,1))",
             "particles": n, "plastic_particles": int(plastic.sum().item()), "label_differences": int(flipped.sum().item()),
-            **summ, "stress_err_vs_plain_over_plastic": err, "gate_tol": 1e-3, "audit_fraction": 1.0,
+            "ms_surrogate_full_audit": ms_surr_full, "audit_fraction_timed": 0.01,
+            **summ, "stress_err_vs_plain_over_plastic": err, "gate_tol": 1e-3, "audit_fraction_stats": 1.0,
             "train_seconds": train_s, "train_loss_first_last": [losses[0], losses[-1]],
             "network": "8-64-64-64-4 SiLU; hidden layers tcgen05 BF16 weights with hi+lo BF16 activations, "
                        "FP32 accumulate; last layer FP32"}
