@@ -211,3 +211,22 @@ def test_device_segments_stop_before_host_events():
         nxt_ok = (a + k <= n_steps and not (pulse and a < pulse < a + k)
                   and not any(m % ratio == 0 for m in range(max(a, 1), a + k)))
         assert not nxt_ok
+
+
+def test_xpbd_step_workspace_covers_the_persistent_form():
+    """mpmw_xpbd_step runs as one persistent launch only with a workspace of
+    mpmw_xpbd_step_workspace_bytes(n, dims): a 16 KB header (barrier
+    arrivals, XPBD count, tile tickets, scan chunk sums), one bit per hash
+    cell, then an area that holds the radix sort's buffers and, after the
+    build, 32 B of contact records per point.  Host-side size query only."""
+    import ctypes
+
+    from mpmwarpydw_b200 import _lib
+    L = _lib.lib()
+    for n, d in ((1, (1, 1, 1)), (1000, (128, 128, 128)), (3_873_600, (120, 70, 120))):
+        dims = (ctypes.c_int32 * 3)(*d)
+        need = int(L.mpmw_xpbd_step_workspace_bytes(n, dims))
+        ncell = d[0] * d[1] * d[2]
+        bits = (ncell + 31) // 32 * 4
+        assert need >= 16384 + bits + 32 * n
+        assert need >= int(L.mpmw_hash_workspace_bytes(n))
