@@ -213,9 +213,11 @@ struct G2P2GShared {
     uint64_t pbar;  // particle-field read-ahead
 };
 
-// Particle fields read ahead by k_g2p2g (bulk copies into the scatter's record
-// area, which is free until the scatter): F (9), mu, lam, ys, alpha, damage,
-// eta_shear, eta_bulk, mass, vol.
+// Particle fields the fused body can read ahead (bulk copies into the
+// scatter's record area, which is free until the scatter) when its caller asks
+// for it -- the batched kernels' tuner option; the single-scene launch loads
+// them plainly: F (9), mu, lam, ys, alpha, damage, eta_shear, eta_bulk, mass,
+// vol.
 constexpr int kAheadFields = 18;
 struct AheadFields {
     float f[kAheadFields][kScatterChunk];
@@ -259,8 +261,8 @@ __device__ __forceinline__ void g2p2g_body(const mpmw_particles_t &P, const mpmw
     const int64_t n = P.n;
     const int t = threadIdx.x;
     const int64_t p = p0 + t;
-    // read-ahead of the particle fields used after the gather (full CTAs only;
-    // the host checks the 16-byte alignment the bulk copies need)
+    // optional read-ahead of the particle fields used after the gather (full
+    // CTAs only; the host checks the 16-byte alignment the bulk copies need)
     const bool ahead = use_ahead && p0 + kScatterChunk <= n;
     AheadFields &AF = *reinterpret_cast<AheadFields *>(&S.s.rec[0][0]);
     if (ahead && t == 0) {
