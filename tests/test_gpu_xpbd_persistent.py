@@ -141,3 +141,24 @@ def test_persistent_step_tunnel():
     assert made == 1
     assert a["counts"][0] > 1000
     _assert_same(a, b)
+
+
+@pytest.mark.parametrize("over", [{"xpbd_iterations": 0}, {"xpbd_iterations": 1, "swellingRatio": 0.0}])
+def test_persistent_step_edge_parameters(over):
+    """No Jacobi iteration at all (the step is hash, integrate, sleep and
+    impulses only), and one iteration without swelling: both forms and the
+    oracle agree bit for bit."""
+    import torch
+
+    from mpmwarpydw_b200.utils import simulationRoutines as S
+    a, b, made = _run_both(lambda: xpbd_scene(seed=8, lock=1, **over), 1)
+    assert made == 1
+    _assert_same(a, b)
+    sim, mpm, xpbd = xpbd_scene(seed=8, lock=1, **over)
+    s = to_oracle(sim, mpm, xpbd)
+    S.xpbdSimulationStep(sim, mpm, xpbd, "cuda:0")
+    torch.cuda.synchronize()
+    orc.xpbd_step(oracle("f32"), s)
+    g = gpu_fields(sim, mpm, xpbd)
+    for k in KEYS:
+        assert np.array_equal(g[k], getattr(s, k)), (k, rel_err(g[k], getattr(s, k)))
