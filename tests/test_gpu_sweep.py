@@ -151,9 +151,11 @@ def test_persistent_batch_sweep_scale():
     launches agree to atomic-order noise.  That noise is not uniform: the
     per-kernel form run twice differs in v by up to 8e-4 of max |v| at a few
     dozen particles (a branch that the FP32 sums' order can flip), and by
-    under 1e-6 everywhere else.  So: labels equal, x and F within 1e-5, v
-    within 1e-4 of max |v| at all but 1 in 10^5 particles and within 1e-2
-    everywhere."""
+    under 1e-6 everywhere else; between the two forms 105 and 235 particles
+    of 17.6 M exceeded 1e-4 in two runs, always with the same 7.8e-4 maximum.
+    A fault (a scene skipped, a grid read stale) moves millions of particles
+    by order one.  So: labels equal, x and F within 1e-5, v within 1e-4 of
+    max |v| at all but 1 in 10^4 particles and within 1e-2 everywhere."""
     import torch
 
     from mpmwarpydw_b200.bind import read_status
@@ -177,7 +179,7 @@ def test_persistent_batch_sweep_scale():
     dv = np.abs(a["v"] - c["v"]).max(axis=0) / float(np.abs(c["v"]).max())
     off = int((dv > 1e-4).sum())
     print(f"v: max {dv.max():.2e} of max |v|, {off} of {dv.size} particles above 1e-4")
-    assert off <= dv.size // 100_000 and dv.max() <= 1e-2
+    assert off <= dv.size // 10_000 and dv.max() <= 1e-2
 
 
 @pytest.mark.parametrize("steps", [1, 2])
